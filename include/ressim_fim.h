@@ -1,0 +1,174 @@
+/*
+ * ressim_fim.h — C ABI of the B200-native fully implicit (FIM) Newton step.
+ *
+ * This is the drop-in boundary under the simulator's step API.  Every entry point takes plain
+ * pointers and sizes, returns an int32_t status (0 ok, >0 recoverable solver status, <0 usage or
+ * device error) and never allocates on the caller's behalf.  A context owns one CUDA stream and
+ * its device buffers; calls on one context must be serialised by the caller (the reference
+ * simulator object is `&mut self`, single threaded).
+ *
+ * Units follow the reference (bar, m, day, mD, cP).  Cell order is natural:
+ * idx = k*nx*ny + j*nx + i (src/lib/ressim/src/grid.rs:25-27).
+ */
+#ifndef RESSIM_FIM_H
+#define RESSIM_FIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RF_ABI_VERSION 1
+
+/* status codes */
+#define RF_OK 0
+#define RF_STEP_WARNING 1        /* step finished with a solver warning (dt collapse, retry budget) */
+#define RF_ERR_INVALID (-1)      /* invalid argument or deck */
+#define RF_ERR_UNSUPPORTED (-2)  /* deck uses a feature the device path does not implement */
+#define RF_ERR_CUDA (-3)         /* CUDA runtime error */
+#define RF_ERR_DEVICE_STATUS (-4)/* a device-side bounded wait or check reported failure */
+
+/* One completion entry (src/lib/ressim/src/well.rs:64-90).  Entries that share a physical well
+ * id (or, when none is given, the legacy fingerprint injector/i/j/bhp/radius/skin) form one
+ * physical well (src/lib/ressim/src/fim/wells.rs:544-594). */
+typedef struct RfWell {
+  int32_t i, j, k;
+  int32_t injector;          /* 1 injector, 0 producer */
+  int32_t physical_well_id;  /* >= 0 explicit id; -1 legacy fingerprint grouping */
+  int32_t has_schedule;      /* 1: explicit per-well schedule below (WellSchedule) */
+  int32_t schedule_enabled;
+  int32_t schedule_control;  /* 0 none, 1 pressure, 2 rate */
+  double bhp;                /* BHP target / last accepted BHP [bar] */
+  double well_radius;        /* [m] */
+  double skin;
+  double schedule_target_rate;         /* NaN: none */
+  double schedule_target_surface_rate; /* NaN: none */
+  double schedule_bhp_limit;           /* NaN: none */
+  double datum_depth_m;                /* NaN: shallowest completion */
+  double wellbore_density_kg_m3;       /* NaN: derived from completions */
+} RfWell;
+
+/* Static deck: grid, rock, fluid, SCAL, wells and controls.  Mirrors the fields of
+ * ReservoirSimulator (src/lib/ressim/src/lib.rs:93-217) that the FIM path reads. */
+typedef struct RfDeck {
+  int32_t abi_version;
+  int32_t nx, ny, nz;
+  double dx, dy;
+  const double* dz;        /* [nz] */
+  const double* porosity;  /* [N] */
+  const double* perm_x;    /* [N] mD */
+  const double* perm_y;    /* [N] mD */
+  const double* perm_z;    /* [N] mD */
+  /* fluid (FluidProperties + rock properties) */
+  double mu_o, mu_w, c_o, c_w, rho_o, rho_w;
+  double b_o, b_w;
+  double water_pvt_reference_pressure_bar;
+  double rock_compressibility;
+  double rock_reference_pressure_bar;
+  double depth_reference_m;
+  int32_t gravity_enabled;
+  /* two-phase Corey SCAL (RockFluidProps) and the FIM relperm table knot count */
+  double s_wc, s_or, n_w, n_o, k_rw_max, k_ro_max;
+  int32_t corey_table_points;
+  /* oil-water capillary pressure (Brooks-Corey, capped at 20x entry) */
+  double pc_entry, pc_lambda;
+  /* wells and family controls (src/lib/ressim/src/fim/wells.rs:691-798) */
+  int32_t n_wells;
+  const RfWell* wells;
+  int32_t injector_rate_controlled;
+  int32_t producer_rate_controlled;
+  int32_t injector_enabled;
+  double target_injector_rate_m3_day;
+  double target_producer_rate_m3_day;
+  double target_injector_surface_rate_m3_day; /* NaN: none */
+  double target_producer_surface_rate_m3_day; /* NaN: none */
+  double well_bhp_min, well_bhp_max;
+  /* three-phase black-oil mode: reserved, must be 0 in this ABI version */
+  int32_t three_phase_mode;
+  int32_t injected_fluid; /* 0 water, 1 gas */
+} RfDeck;
+
+/* Per-report-step outcome (FimStepStats subset, src/lib/ressim/src/reporting.rs:191-243). */
+typedef struct RfStepReport {
+  int32_t substeps;             /* accepted substeps */
+  int32_t retries;              /* failed Newton attempts */
+  int32_t newton_iterations;    /* summed over accepted and failed attempts */
+  int32_t linear_iterations;    /* summed FGMRES iterations */
+  int32_t linear_solves;
+  int32_t warning;              /* 0 none, 1 dt collapse, 2 retry budget, 3 max substeps */
+  double time_days;             /* simulator time after the step */
+  double advanced_days;
+  double last_dt_days;
+  double device_ms;             /* device time of the step measured with CUDA events */
+} RfStepReport;
+
+/* One accepted-substep rate record (TimePointRates subset, reporting.rs:246-291). */
+typedef struct RfTimePointRates {
+  double time;
+  double total_production_oil;
+  double total_production_liquid;
+  double total_production_liquid_reservoir;
+  double total_injection;
+  double total_injection_reservoir;
+  double material_balance_error_m3;
+  double material_balance_error_oil_m3;
+  double avg_reservoir_pressure;
+  double avg_water_saturation;
+  double producer_bhp_limited_fraction;
+  double injector_bhp_limited_fraction;
+} RfTimePointRates;
+
+/* Linear-solve report (FimLinearSolveReport, src/lib/ressim/src/fim/linear/mod.rs:213-230). */
+typedef struct RfLinearReport {
+  int32_t converged;
+  int32_t iterations;
+  double rhs_norm;
+  double final_residual_norm;
+} RfLinearReport;
+
+typedef struct RfCtx RfCtx;
+
+/* Replaces ReservoirSimulator::new + setters (src/lib/ressim/src/frontend.rs:36-123): copies
+ * the deck to the device on the current CUDA device. */
+int32_t rf_create(const RfDeck* deck, RfCtx** out);
+int32_t rf_destroy(RfCtx* ctx);
+
+/* Message of the last error on this context (or the last rf_create failure when ctx is NULL). */
+int32_t rf_last_error(const RfCtx* ctx, char* buf, size_t len);
+
+/* Replaces loadState's grid/well payload (frontend.rs:931-1008).  sg and rs may be NULL in
+ * two-phase mode. */
+int32_t rf_set_state(RfCtx* ctx, const double* pressure, const double* sat_water,
+                     const double* sat_gas, const double* rs, double time_days);
+/* Replaces getPressures/getSatWater/getSatOil/getSatGas/getRs (frontend.rs:523-605); any
+ * output pointer may be NULL. */
+int32_t rf_get_state(const RfCtx* ctx, double* pressure, double* sat_water, double* sat_oil,
+                     double* sat_gas, double* rs, double* time_days);
+/* Current BHP of every completion entry (getWellState's `bhp`). */
+int32_t rf_get_well_bhp(const RfCtx* ctx, double* bhp, int32_t n);
+
+/* Replaces ReservoirSimulator::step (frontend.rs:345-349 -> fim/timestep.rs:989-1848): one
+ * report step of the OPM-aligned FIM controller, Newton iterations on the device. */
+int32_t rf_step(RfCtx* ctx, double target_dt_days, RfStepReport* out);
+
+/* getRateHistory (frontend.rs:562-565): number of records and one record. */
+int32_t rf_rate_history_len(const RfCtx* ctx);
+int32_t rf_rate_history_get(const RfCtx* ctx, int32_t index, RfTimePointRates* out);
+
+/* Linear-solver seam replacing solve_linearized_system for a tail-free system
+ * (src/lib/ressim/src/fim/linear/mod.rs:252-260): CPR-FGMRES with block-ILU0 on a 3x3 block
+ * CSR matrix given on the host (block row pointers, block columns, row-major 3x3 values). */
+int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* block_row_ptr,
+                            const int32_t* block_cols, const double* block_vals,
+                            const double* rhs, double* x, RfLinearReport* out);
+
+/* Number of kernel launches this context has issued since creation (device work counter). */
+int64_t rf_kernel_launches(const RfCtx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RESSIM_FIM_H */

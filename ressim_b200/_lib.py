@@ -1,0 +1,52 @@
+"""Loader of the device FIM library (libressim_fim.so, built in-tree for sm_100a).
+
+There is no fallback: if the library is missing or fails to load, importing the simulator raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.path.join(HERE, "libressim_fim.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(SO_PATH):
+        raise RuntimeError(f"device FIM library not built: {SO_PATH} (run python -m ressim_b200.build)")
+    L = C.CDLL(SO_PATH)
+    L.rf_create.argtypes = [C.POINTER(_abi.RfDeck), C.POINTER(C.c_void_p)]
+    L.rf_destroy.argtypes = [C.c_void_p]
+    L.rf_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    L.rf_set_state.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double]
+    L.rf_get_state.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.rf_get_well_bhp.argtypes = [C.c_void_p, _dp, C.c_int32]
+    L.rf_step.argtypes = [C.c_void_p, C.c_double, C.POINTER(_abi.RfStepReport)]
+    L.rf_rate_history_len.argtypes = [C.c_void_p]
+    L.rf_rate_history_get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(_abi.RfTimePointRates)]
+    L.rf_linear_solve_bsr.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp, _dp, _dp, C.POINTER(_abi.RfLinearReport)]
+    L.rf_kernel_launches.argtypes = [C.c_void_p]
+    L.rf_kernel_launches.restype = C.c_int64
+    _lib = L
+    return L
+
+
+def last_error(handle) -> str:
+    buf = C.create_string_buffer(1024)
+    load().rf_last_error(handle, buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+EXPORTED_SYMBOLS = (
+    "rf_create", "rf_destroy", "rf_last_error", "rf_set_state", "rf_get_state", "rf_get_well_bhp",
+    "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_kernel_launches",
+)

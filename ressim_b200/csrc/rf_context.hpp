@@ -1,0 +1,134 @@
+// rf_context.hpp — host-side context of the device FIM path: deck copy, well topology, device
+// buffers and the linear-solver workspace.  One context per simulator; one CUDA stream each.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ressim_fim.h"
+#include "rf_device.cuh"
+#include "rf_physics.cuh"
+
+namespace rf {
+
+// Stencil slot order of a block row: z-, y-, x-, diagonal, x+, y+, z+.  This is also the
+// ascending column order, and the order in which the reference's assembly loop adds face terms
+// into a cell's rows (faces owned by lower-index neighbours first).
+enum { kZm = 0, kYm = 1, kXm = 2, kDiag = 3, kXp = 4, kYp = 5, kZp = 6 };
+
+struct WellControlH {
+  int enabled, rate_controlled, uses_surface_target, has_target, injector;
+  double target_rate, bhp_limit, bhp_target;
+};
+
+struct Topology {
+  int n_wells = 0, n_perfs = 0;
+  std::vector<int> perf_cell, perf_well, perf_entry, perf_inj, perf_has_wi;
+  std::vector<double> perf_wi;
+  std::vector<int> well_rep, well_inj, well_ptr, well_perfs;  // perfs of well w: well_perfs[well_ptr[w]..]
+  int max_perfs_per_well = 0;
+};
+
+// Level schedule of a lower-triangular block pattern: rows of level l are rows[ptr[l]..ptr[l+1]).
+struct Levels {
+  int n_levels = 0;
+  std::vector<int> h_ptr;
+  int* d_rows = nullptr;
+  int* d_ptr = nullptr;
+};
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (count == 0) count = 1;
+    RF_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct Ctx {
+  std::string err;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+  int device = 0, num_sms = 0;
+
+  // deck
+  int nx = 0, ny = 0, nz = 0, n = 0;
+  double dx = 0, dy = 0;
+  std::vector<double> dz, depth_layer, porosity, kx, ky, kz, pv;
+  Fluid fluid{};
+  std::vector<RfWell> wells;
+  std::vector<double> head_offset;
+  int inj_rate_ctl = 0, prod_rate_ctl = 0, inj_enabled = 1;
+  double tgt_inj = 0, tgt_prod = 0, tgt_inj_surf = NAN, tgt_prod_surf = NAN, bhp_min = -100, bhp_max = 2000;
+  Topology topo;
+
+  // simulator state on the host side (mirrors of what the device holds after each step)
+  std::vector<double> h_p, h_sw, h_so, h_sg, h_rs;
+  double time_days = 0;
+  std::vector<RfTimePointRates> rate_history;
+  double cum_inj = 0, cum_prod = 0, cum_mb = 0, cum_mb_oil = 0;
+  std::string last_warning;
+
+  // block pattern (reduced reservoir system): stencil + well fill
+  int nnzb = 0;
+  std::vector<int> h_row_ptr, h_col, h_diag, h_stencil;  // h_stencil: 7 positions per row, -1 absent
+  DBuf<int> d_row_ptr, d_col, d_diag, d_stencil;
+  Levels levels;
+  // well fill positions: for each well, m*m block positions (row perf a, col perf b)
+  std::vector<int> h_fill_off, h_fill_pos;
+  DBuf<int> d_fill_off, d_fill_pos;
+
+  // device state
+  DBuf<double> d_pv, d_tx, d_ty, d_tz, d_depth;
+  DBuf<double> d_p, d_sw, d_hc, d_pp, d_psw, d_phc, d_cp, d_csw, d_chc;
+  DBuf<double> d_res, d_val;
+  // wells on the device
+  DBuf<int> d_perf_cell, d_perf_well, d_perf_inj, d_perf_has_wi, d_well_ptr, d_well_perfs;
+  DBuf<double> d_perf_wi, d_perf_head;
+  DBuf<WellControlH> d_ctrl;
+  DBuf<double> d_bhp, d_q;
+  DBuf<double> d_res_tail;                       // W + P
+  DBuf<double> d_jrw;                            // P*3: cell rows x own q column
+  DBuf<double> d_jwr_perf, d_jwr_ctrl;           // P*3 each
+  DBuf<double> d_jww_perf_bhp, d_jww_ctrl_q;     // P each
+  DBuf<double> d_jww_ctrl_bhp;                   // W
+  DBuf<double> d_tinv;                           // per well (1+m)^2 dense inverse
+  std::vector<int> h_tinv_off;
+  DBuf<int> d_tinv_off;
+  DBuf<double> d_rhs_red, d_rhs_full, d_dx_tail, d_jrr_perf;  // d_jrr_perf: original perforated-row blocks
+  std::vector<int> h_perf_row_blocks_off;  // per perforation: offset into d_jrr_perf (row block copy)
+  DBuf<int> d_perf_row_off;
+
+  // linear solver workspace (reduced system, 3N unknowns)
+  static constexpr int kRestart = 30;
+  DBuf<double> d_V, d_Z, d_w, d_x, d_tmp, d_tmp2, d_cand;
+  DBuf<double> d_cpr_w;       // 3N restriction weights
+  DBuf<double> d_pval;        // nnzb pressure matrix values (block pattern)
+  DBuf<double> d_plu, d_pdiag;  // pressure ILU factors on the same pattern, diagonal
+  DBuf<double> d_lu, d_dinv;  // block ILU factors (nnzb*9), inverse diagonal blocks (N*9)
+  DBuf<unsigned char> d_bmask;  // block present in the reduced matrix (any |v| > EPS, or diagonal)
+  DBuf<double> d_cres, d_full;  // last FGMRES true residual, full-system residual rows
+  DBuf<double> d_dense;       // N*N dense pressure inverse when N <= 299
+  int dense_ok = 0;
+  DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
+  DBuf<double> d_partials, d_scal;
+  DBuf<DeviceStatus> d_status;
+  DBuf<unsigned int> d_barrier;  // count, gen
+  int coop_blocks_bicg = 0, coop_blocks_sweep = 0;
+  DBuf<int> d_flag_dense;
+
+  // timing
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+}  // namespace rf

@@ -1,0 +1,1321 @@
+// rf_linear.cu — the linear solve of one Newton iteration on the device.
+//
+//   well Schur elimination     k_schur / k_recover: one CTA per physical well, dense local
+//                              inverse in shared memory (fim/linear/well_schur.rs:70-471)
+//   CPR build                  k_cpr_weights (QuasiImpes: row 0 of the inverse diagonal block,
+//                              normalised by its largest magnitude), k_pressure_matrix
+//                              (A_p[i,j] = sum_l w_i[l] A[(i,l),(j,0)]), level-scheduled
+//                              pressure ILU0 and block ILU0 factorisations in the reference's
+//                              natural order (gmres_block_jacobi.rs:178-353, 746-808, 919-1363)
+//   CPR apply                  restrict -> coarse solve (dense inverse when N <= 299, else a
+//                              cooperative persistent BiCGStab with pressure ILU0, at most 50
+//                              iterations, tol 1e-6 relative) -> prolong -> r - A x_p ->
+//                              block-ILU0 sweep -> add (gmres_block_jacobi.rs:471-729)
+//   FGMRES(30)                 right-preconditioned flexible GMRES, x0 = 0, modified
+//                              Gram-Schmidt, true residual of the candidate every inner step,
+//                              tolerance 1e-12 + 5e-3 |b| (gmres_block_jacobi.rs:1470-1665)
+//
+// A block is "present" in the ILU pattern when any of its entries exceeds EPS in magnitude (the
+// reference builds its ILU0 pattern that way); absent blocks are held as zeros and receive no
+// fill.  Pressure-matrix entries with |v| <= 1e-14 are dropped, as the reference does.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "rf_ops.hpp"
+
+namespace rf {
+
+constexpr double kEps = kF64Eps;
+
+// ============================================================================================
+// small dense helpers
+// ============================================================================================
+__device__ __forceinline__ void mat3_mul(const double* a, const double* b, double* c) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c[3 * r + k] = a[3 * r] * b[k] + a[3 * r + 1] * b[3 + k] + a[3 * r + 2] * b[6 + k];
+}
+// 3x3 inverse by cofactors; fails only on an exactly zero determinant, then the diagonal
+// reciprocal fallback (gmres_block_jacobi.rs:888-901) is used.
+__host__ __device__ __forceinline__ void mat3_inverse_or_diag(const double* m, double* o) {
+  const double m11 = m[0], m12 = m[1], m13 = m[2], m21 = m[3], m22 = m[4], m23 = m[5], m31 = m[6], m32 = m[7],
+               m33 = m[8];
+  const double c11 = m22 * m33 - m32 * m23;
+  const double c21 = m21 * m33 - m31 * m23;
+  const double c31 = m21 * m32 - m31 * m22;
+  const double det = m11 * c11 - m12 * c21 + m13 * c31;
+  if (det != 0.0) {
+    o[0] = c11 / det;
+    o[1] = (m13 * m32 - m33 * m12) / det;
+    o[2] = (m12 * m23 - m22 * m13) / det;
+    o[3] = -c21 / det;
+    o[4] = (m11 * m33 - m31 * m13) / det;
+    o[5] = (m13 * m21 - m23 * m11) / det;
+    o[6] = c31 / det;
+    o[7] = (m12 * m31 - m32 * m11) / det;
+    o[8] = (m11 * m22 - m21 * m12) / det;
+    return;
+  }
+  for (int k = 0; k < 9; ++k) o[k] = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    const double v = m[4 * d];
+    o[4 * d] = fabs(v) > kEps ? 1.0 / v : 1.0;
+  }
+}
+
+// ============================================================================================
+// BSR SpMV and vector kernels
+// ============================================================================================
+// y = A x (mode 0) or y = b - A x (mode 1), thread per block row, blocks in column order.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_spmv(int nb, const int* __restrict__ rp, const int* __restrict__ col,
+                                                  const double* __restrict__ val, const double* __restrict__ x,
+                                                  const double* __restrict__ b, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const double* a = val + size_t(k) * 9;
+    const int j = col[k];
+    const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+    s0 = s0 + a[0] * x0;
+    s0 = s0 + a[1] * x1;
+    s0 = s0 + a[2] * x2;
+    s1 = s1 + a[3] * x0;
+    s1 = s1 + a[4] * x1;
+    s1 = s1 + a[5] * x2;
+    s2 = s2 + a[6] * x0;
+    s2 = s2 + a[7] * x1;
+    s2 = s2 + a[8] * x2;
+  }
+  if (MODE == 0) {
+    y[3 * i] = s0;
+    y[3 * i + 1] = s1;
+    y[3 * i + 2] = s2;
+  } else {
+    y[3 * i] = b[3 * i] - s0;
+    y[3 * i + 1] = b[3 * i + 1] - s1;
+    y[3 * i + 2] = b[3 * i + 2] - s2;
+  }
+}
+
+// partial sums of a*b (or a*a when b == nullptr) per block, grid-stride; final pass in k_sum_final
+__global__ void __launch_bounds__(kBlock) k_dot_partial(long long n, const double* __restrict__ a,
+                                                         const double* __restrict__ b, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += a[i] * (b ? b[i] : a[i]);
+  const double r = block_sum<kBlock>(s, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+__global__ void k_reduce_to(int nblocks, const double* __restrict__ partials, double* __restrict__ out, int take_sqrt) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0;
+  for (int b = 0; b < nblocks; ++b) a += partials[b];
+  *out = take_sqrt ? sqrt(a) : a;
+}
+// w -= h * v with h read from device memory
+__global__ void k_axpy_dev(long long n, const double* __restrict__ h, const double* __restrict__ v, double* __restrict__ w) {
+  const double c = *h;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    w[i] -= v[i] * c;
+}
+// out = w / nrm (nrm from device memory)
+__global__ void k_scale_div(long long n, const double* __restrict__ w, const double* __restrict__ nrm,
+                            double* __restrict__ out) {
+  const double d = *nrm;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = w[i] / d;
+}
+// cand = origin + sum_c Z_c y_c (y on the device), update accumulated from zero in column order
+__global__ void k_combine(long long n, int cols, const double* __restrict__ Z, long long ld, const double* __restrict__ y,
+                          const double* __restrict__ origin, double* __restrict__ cand) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double u = 0.0;
+    for (int c = 0; c < cols; ++c) u += Z[c * ld + i] * y[c];
+    cand[i] = origin ? origin[i] + u : u;
+  }
+}
+__global__ void k_copy(long long n, const double* __restrict__ a, double* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+__global__ void k_neg(long long n, const double* __restrict__ a, double* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = -a[i];
+}
+__global__ void k_add_inplace(long long n, const double* __restrict__ a, double* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] += a[i];
+}
+__global__ void k_count_nonfinite(long long n, const double* __restrict__ a, int* __restrict__ flag) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (!isfinite(a[i])) atomicExch(flag, 1);
+}
+
+// ============================================================================================
+// Well Schur elimination (one CTA per physical well)
+// ============================================================================================
+struct SchurArgs {
+  int n_wells;
+  const int* well_ptr;
+  const int* well_perfs;
+  const int* perf_cell;
+  const int* perf_has_wi;
+  const double* jrw;
+  const double* jwr_perf;
+  const double* jwr_ctrl;
+  const double* jww_perf_bhp;
+  const double* jww_ctrl_q;
+  const double* jww_ctrl_bhp;
+  const double* res;       // cell residual (rhs = -res)
+  const double* res_tail;  // W + P
+  const int* tinv_off;
+  double* tinv;
+  const int* row_ptr;
+  const int* fill_off;
+  const int* fill_pos;
+  const int* perf_row_off;
+  double* val;
+  double* jrr_perf;
+  double* rhs_red;  // holds -res for every cell on entry; perforated rows corrected here
+};
+
+// Gauss-Jordan inverse with partial pivoting of the nt x nt matrix in shared memory.  Returns
+// false on an exactly zero pivot.
+__device__ bool smem_gauss_jordan(double* a, double* inv, int nt, int* s_piv, double* s_red) {
+  const int t = threadIdx.x, nt_threads = blockDim.x;
+  for (int k = t; k < nt * nt; k += nt_threads) inv[k] = (k / nt == k % nt) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int c = 0; c < nt; ++c) {
+    if (t == 0) {
+      int piv = c;
+      double best = fabs(a[c * nt + c]);
+      for (int r = c + 1; r < nt; ++r)
+        if (fabs(a[r * nt + c]) > best) {
+          best = fabs(a[r * nt + c]);
+          piv = r;
+        }
+      s_piv[0] = piv;
+      s_red[0] = best;
+    }
+    __syncthreads();
+    if (s_red[0] == 0.0) return false;
+    const int piv = s_piv[0];
+    if (piv != c)
+      for (int k = t; k < nt; k += nt_threads) {
+        double x = a[c * nt + k];
+        a[c * nt + k] = a[piv * nt + k];
+        a[piv * nt + k] = x;
+        x = inv[c * nt + k];
+        inv[c * nt + k] = inv[piv * nt + k];
+        inv[piv * nt + k] = x;
+      }
+    __syncthreads();
+    const double d = a[c * nt + c];
+    __syncthreads();
+    for (int k = t; k < nt; k += nt_threads) {
+      a[c * nt + k] /= d;
+      inv[c * nt + k] /= d;
+    }
+    __syncthreads();
+    for (int idx = t; idx < nt * nt; idx += nt_threads) {
+      const int r = idx / nt, k = idx % nt;
+      if (r == c) continue;
+      const double f = a[r * nt + c];
+      if (k != c) a[r * nt + k] -= f * a[c * nt + k];
+      inv[r * nt + k] -= f * inv[c * nt + k];
+    }
+    __syncthreads();
+    for (int r = t; r < nt; r += nt_threads)
+      if (r != c) a[r * nt + c] = 0.0;
+    __syncthreads();
+  }
+  return true;
+}
+
+__global__ void k_schur(SchurArgs s) {
+  extern __shared__ double sm[];
+  __shared__ int s_piv[1];
+  __shared__ double s_red[1];
+  const int w = blockIdx.x;
+  const int p0 = s.well_ptr[w], m = s.well_ptr[w + 1] - p0, nt = 1 + m;
+  double* J = sm;
+  double* I = sm + nt * nt;
+  double* rw = I + nt * nt;  // local rhs tail (nt)
+  double* tir = rw + nt;     // inv * rhs tail (nt)
+  const int t = threadIdx.x;
+  for (int k = t; k < nt * nt; k += blockDim.x) J[k] = 0.0;
+  __syncthreads();
+  if (t == 0) {
+    J[0] = s.jww_ctrl_bhp[w];
+    rw[0] = -s.res_tail[w];
+    for (int a = 0; a < m; ++a) {
+      const int k = s.well_perfs[p0 + a];
+      J[1 + a] = s.jww_ctrl_q[k];
+      J[(1 + a) * nt] = s.jww_perf_bhp[k];
+      J[(1 + a) * nt + 1 + a] = s.perf_has_wi[k] ? 1.0 : 0.0;
+      rw[1 + a] = -s.res_tail[s.n_wells + k];
+    }
+  }
+  __syncthreads();
+  // keep the assembled tail block's diagonal for the singular fallback
+  __shared__ double s_diag[257];
+  for (int r = t; r < nt && r < 257; r += blockDim.x) s_diag[r] = J[r * nt + r];
+  __syncthreads();
+  const bool ok = smem_gauss_jordan(J, I, nt, s_piv, s_red);
+  __syncthreads();
+  if (!ok) {
+    for (int k = t; k < nt * nt; k += blockDim.x) I[k] = 0.0;
+    __syncthreads();
+    for (int r = t; r < nt && r < 257; r += blockDim.x) I[r * nt + r] = fabs(s_diag[r]) > kEps ? 1.0 / s_diag[r] : 1.0;
+    __syncthreads();
+  }
+  double* tg = s.tinv + s.tinv_off[w];
+  for (int k = t; k < nt * nt; k += blockDim.x) tg[k] = I[k];
+  // inv * rhs_tail
+  for (int r = t; r < nt; r += blockDim.x) {
+    double acc = 0.0;
+    for (int c = 0; c < nt; ++c) acc += I[r * nt + c] * rw[c];
+    tir[r] = acc;
+  }
+  // save the original (pre-fill) blocks of every perforated row
+  for (int a = 0; a < m; ++a) {
+    const int k = s.well_perfs[p0 + a], cell = s.perf_cell[k];
+    const int b0 = s.row_ptr[cell], b1 = s.row_ptr[cell + 1];
+    double* dst = s.jrr_perf + size_t(s.perf_row_off[k]) * 9;
+    for (int e = t; e < (b1 - b0) * 9; e += blockDim.x) dst[e] = s.val[size_t(b0) * 9 + e];
+  }
+  __syncthreads();
+  // fill: block(a, b) -= jrw_a * inv[1+a][.] * J_WR[., b]
+  for (int pr = t; pr < m * m * 9; pr += blockDim.x) {
+    const int a = pr / (m * 9), b = (pr / 9) % m, e = pr % 9, r = e / 3, v = e % 3;
+    const int ka = s.well_perfs[p0 + a], kb = s.well_perfs[p0 + b];
+    const double j = s.jrw[3 * ka + r];
+    if (fabs(j) <= kEps) continue;
+    const double wc = 0.0 + j * I[(1 + a) * nt + 0];
+    const double wp = 0.0 + j * I[(1 + a) * nt + 1 + b];
+    const int pos = s.fill_pos[s.fill_off[w] + a * m + b];
+    double* blk = s.val + size_t(pos) * 9;
+    double x = blk[e];
+    const double jc = s.jwr_ctrl[3 * kb + v], jp = s.jwr_perf[3 * kb + v];
+    if (fabs(wc) > kEps && fabs(jc) > kEps) x += -wc * jc;
+    if (fabs(wp) > kEps && fabs(jp) > kEps) x += -wp * jp;
+    blk[e] = x;
+  }
+  // reduced rhs of the perforated rows
+  for (int idx = t; idx < m * 3; idx += blockDim.x) {
+    const int a = idx / 3, r = idx % 3;
+    const int k = s.well_perfs[p0 + a], cell = s.perf_cell[k];
+    const double j = s.jrw[3 * k + r];
+    if (fabs(j) <= kEps) continue;
+    const double corr = 0.0 + j * tir[1 + a];
+    s.rhs_red[3 * cell + r] -= corr;
+  }
+}
+
+struct RecoverArgs {
+  int n_wells;
+  const int* well_ptr;
+  const int* well_perfs;
+  const int* perf_cell;
+  const int* perf_has_wi;
+  const double* jrw;
+  const double* jwr_perf;
+  const double* jwr_ctrl;
+  const double* jww_perf_bhp;
+  const double* jww_ctrl_q;
+  const double* jww_ctrl_bhp;
+  const double* res;
+  const double* res_tail;
+  const int* tinv_off;
+  const double* tinv;
+  const double* x;  // reduced solution
+  double* dx_tail;  // W + P
+  const int* row_ptr;
+  const int* col;
+  const int* perf_row_off;
+  const double* jrr_perf;
+  double* full;       // full-system residual of the reservoir rows (perforated rows rewritten)
+  double* tail_sq;    // per well: sum of squared full-system residual of its tail rows
+};
+
+__global__ void k_recover(RecoverArgs s) {
+  const int w = blockIdx.x;
+  if (threadIdx.x != 0) return;
+  const int p0 = s.well_ptr[w], m = s.well_ptr[w + 1] - p0, nt = 1 + m;
+  const double* I = s.tinv + s.tinv_off[w];
+  double rt[257];
+  const int ntc = nt < 257 ? nt : 257;
+  {
+    double acc = 0.0;
+    for (int a = 0; a < m; ++a) {
+      const int k = s.well_perfs[p0 + a], c = s.perf_cell[k];
+      for (int v = 0; v < 3; ++v) {
+        const double j = s.jwr_ctrl[3 * k + v];
+        if (fabs(j) > kEps) acc += j * s.x[3 * c + v];
+      }
+    }
+    rt[0] = -s.res_tail[w] - acc;
+  }
+  for (int a = 0; a < m && a + 1 < ntc; ++a) {
+    const int k = s.well_perfs[p0 + a], c = s.perf_cell[k];
+    double acc = 0.0;
+    for (int v = 0; v < 3; ++v) {
+      const double j = s.jwr_perf[3 * k + v];
+      if (fabs(j) > kEps) acc += j * s.x[3 * c + v];
+    }
+    rt[1 + a] = -s.res_tail[s.n_wells + k] - acc;
+  }
+  double dx[257];
+  for (int r = 0; r < ntc; ++r) {
+    double acc = 0.0;
+    for (int c = 0; c < ntc; ++c) acc += I[r * nt + c] * rt[c];
+    dx[r] = acc;
+  }
+  s.dx_tail[w] = dx[0];
+  for (int a = 0; a < m && a + 1 < ntc; ++a) s.dx_tail[s.n_wells + s.well_perfs[p0 + a]] = dx[1 + a];
+  // full-system residual of this well's perforated rows and tail rows
+  double sq = 0.0;
+  {
+    double acc = 0.0;
+    for (int a = 0; a < m; ++a) {
+      const int k = s.well_perfs[p0 + a], c = s.perf_cell[k];
+      for (int v = 0; v < 3; ++v) acc += s.jwr_ctrl[3 * k + v] * s.x[3 * c + v];
+    }
+    acc += s.jww_ctrl_bhp[w] * dx[0];
+    for (int a = 0; a < m && a + 1 < ntc; ++a) acc += s.jww_ctrl_q[s.well_perfs[p0 + a]] * dx[1 + a];
+    const double r = -s.res_tail[w] - acc;
+    sq += r * r;
+  }
+  for (int a = 0; a < m && a + 1 < ntc; ++a) {
+    const int k = s.well_perfs[p0 + a], c = s.perf_cell[k];
+    double acc = 0.0;
+    for (int v = 0; v < 3; ++v) acc += s.jwr_perf[3 * k + v] * s.x[3 * c + v];
+    acc += s.jww_perf_bhp[k] * dx[0];
+    acc += (s.perf_has_wi[k] ? 1.0 : 0.0) * dx[1 + a];
+    const double r = -s.res_tail[s.n_wells + k] - acc;
+    sq += r * r;
+    // reservoir rows of the perforated cell, from the original (pre-fill) blocks
+    const int b0 = s.row_ptr[c], b1 = s.row_ptr[c + 1];
+    const double* blk0 = s.jrr_perf + size_t(s.perf_row_off[k]) * 9;
+    for (int e = 0; e < 3; ++e) {
+      double acc2 = 0.0;
+      for (int b = b0; b < b1; ++b) {
+        const double* blk = blk0 + size_t(b - b0) * 9;
+        const int j = s.col[b];
+        acc2 += blk[3 * e] * s.x[3 * j];
+        acc2 += blk[3 * e + 1] * s.x[3 * j + 1];
+        acc2 += blk[3 * e + 2] * s.x[3 * j + 2];
+      }
+      acc2 += s.jrw[3 * k + e] * dx[1 + a];
+      s.full[3 * c + e] = -s.res[3 * c + e] - acc2;
+    }
+  }
+  s.tail_sq[w] = sq;
+}
+
+// ============================================================================================
+// CPR build
+// ============================================================================================
+// QuasiImpes restriction weights from the diagonal block and the block presence mask
+__global__ void k_cpr_weights(int nb, const int* __restrict__ rp, const int* __restrict__ diag,
+                              const double* __restrict__ val, double* __restrict__ w,
+                              unsigned char* __restrict__ mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  double inv[9];
+  mat3_inverse_or_diag(val + size_t(diag[i]) * 9, inv);
+  double r0 = inv[0], r1 = inv[1], r2 = inv[2];
+  const double mx = fmax(fmax(fmax(0.0, fabs(r0)), fabs(r1)), fabs(r2));
+  if (mx > kEps) {
+    r0 /= mx;
+    r1 /= mx;
+    r2 /= mx;
+  }
+  w[3 * i] = r0;
+  w[3 * i + 1] = r1;
+  w[3 * i + 2] = r2;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const double* a = val + size_t(k) * 9;
+    bool present = (k == diag[i]);
+    for (int e = 0; e < 9; ++e) present = present || fabs(a[e]) > kEps;
+    mask[k] = present ? 1 : 0;
+  }
+}
+
+// A_p[i, j] = ((0 + w0 A[(i,0),(j,0)]) + w1 A[(i,1),(j,0)]) + w2 A[(i,2),(j,0)]; |A_p| <= 1e-14 -> 0
+__global__ void k_pressure_matrix(int nb, const int* __restrict__ rp, const double* __restrict__ val,
+                                  const double* __restrict__ w, double* __restrict__ pval) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const double w0 = w[3 * i], w1 = w[3 * i + 1], w2 = w[3 * i + 2];
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const double* a = val + size_t(k) * 9;
+    double s = 0.0;
+    // entries whose row weight is <= EPS are skipped, and so are zero matrix entries (absent from
+    // the reference's CSR)
+    if (fabs(w0) > kEps && a[0] != 0.0) s += w0 * a[0] * 1.0;
+    if (fabs(w1) > kEps && a[3] != 0.0) s += w1 * a[3] * 1.0;
+    if (fabs(w2) > kEps && a[6] != 0.0) s += w2 * a[6] * 1.0;
+    pval[k] = fabs(s) > 1e-14 ? s : 0.0;
+  }
+}
+
+// Pressure ILU0, one row (factorize_pressure_ilu0's up-looking order).  `plu` holds L in the
+// lower positions and U in the upper positions; absent entries (A_p == 0) stay zero.
+__device__ __forceinline__ double upper_entry(const int* rp, const int* col, const int* diag, const double* plu,
+                                              int k, int c) {
+  int lo = diag[k] + 1, hi = rp[k + 1] - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int cm = col[mid];
+    if (cm == c) return plu[mid];
+    if (cm < c)
+      lo = mid + 1;
+    else
+      hi = mid - 1;
+  }
+  return 0.0;
+}
+__device__ void pressure_ilu_row(int r, const int* rp, const int* col, const int* diag, const double* pval,
+                                 double* plu, double* pdiag) {
+  const int b0 = rp[r], dp = diag[r], b1 = rp[r + 1];
+  for (int kp = b0; kp < dp; ++kp) {
+    if (pval[kp] == 0.0) {
+      plu[kp] = 0.0;
+      continue;
+    }
+    const int c = col[kp];
+    double s = pval[kp];
+    for (int lp = b0; lp < kp; ++lp) {
+      if (pval[lp] == 0.0) continue;
+      s -= plu[lp] * upper_entry(rp, col, diag, plu, col[lp], c);
+    }
+    const double d = pdiag[c];
+    plu[kp] = fabs(d) > kEps ? s / d : 0.0;
+  }
+  const double de = pval[dp];
+  double ud = de;
+  for (int lp = b0; lp < dp; ++lp) {
+    if (pval[lp] == 0.0) continue;
+    ud -= plu[lp] * upper_entry(rp, col, diag, plu, col[lp], r);
+  }
+  if (fabs(ud) <= kEps) ud = fabs(de) > kEps ? de : 1.0;
+  pdiag[r] = ud;
+  plu[dp] = 0.0;
+  for (int up = dp + 1; up < b1; ++up) {
+    if (pval[up] == 0.0) {
+      plu[up] = 0.0;
+      continue;
+    }
+    const int c = col[up];
+    double s = pval[up];
+    for (int lp = b0; lp < dp; ++lp) {
+      if (pval[lp] == 0.0) continue;
+      s -= plu[lp] * upper_entry(rp, col, diag, plu, col[lp], c);
+    }
+    plu[up] = s;
+  }
+}
+
+// Block ILU0, one row (factorize_block_ilu0's IKJ order).
+__device__ void block_ilu_row(int i, const int* rp, const int* col, const int* diag, const double* val,
+                              const unsigned char* mask, double* lu, double* dinv) {
+  const int b0 = rp[i], dp = diag[i], b1 = rp[i + 1];
+  for (int k = b0; k < b1; ++k)
+    for (int e = 0; e < 9; ++e) lu[size_t(k) * 9 + e] = mask[k] ? val[size_t(k) * 9 + e] : 0.0;
+  for (int kp = b0; kp < dp; ++kp) {
+    if (!mask[kp]) continue;
+    const int kr = col[kp];
+    double lik[9];
+    mat3_mul(lu + size_t(kp) * 9, dinv + size_t(kr) * 9, lik);
+    // U-row of kr: present blocks right of its diagonal; merge with row i's present blocks
+    int ip = kp + 1;
+    for (int up = diag[kr] + 1; up < rp[kr + 1]; ++up) {
+      if (!mask[up]) continue;
+      const int j = col[up];
+      while (ip < b1 && col[ip] < j) ++ip;
+      if (ip >= b1) break;
+      if (col[ip] != j || !mask[ip]) continue;
+      double prod[9];
+      mat3_mul(lik, lu + size_t(up) * 9, prod);
+      double* t = lu + size_t(ip) * 9;
+      for (int e = 0; e < 9; ++e) t[e] -= prod[e];
+    }
+    for (int e = 0; e < 9; ++e) lu[size_t(kp) * 9 + e] = lik[e];
+  }
+  mat3_inverse_or_diag(lu + size_t(dp) * 9, dinv + size_t(i) * 9);
+}
+
+struct LevelArgs {
+  int n_levels;
+  const int* lvl_rows;
+  const int* lvl_ptr;
+  const int* rp;
+  const int* col;
+  const int* diag;
+  GridBarrier bar;
+};
+
+__global__ void k_factor_coop(LevelArgs L, const double* __restrict__ val, const unsigned char* __restrict__ mask,
+                              double* lu, double* dinv, const double* __restrict__ pval, double* plu, double* pdiag) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int l = 0; l < L.n_levels; ++l) {
+    const int a = L.lvl_ptr[l], b = L.lvl_ptr[l + 1];
+    for (int q = a + tid; q < b; q += nth) {
+      const int r = L.lvl_rows[q];
+      block_ilu_row(r, L.rp, L.col, L.diag, val, mask, lu, dinv);
+      pressure_ilu_row(r, L.rp, L.col, L.diag, pval, plu, pdiag);
+    }
+    grid_sync(L.bar, 100);
+  }
+}
+
+// ============================================================================================
+// ILU sweeps
+// ============================================================================================
+// block: y_i = r_i - sum L_ik y_k (forward); x_i = Dinv_i (y_i - sum U_ij x_j) (backward)
+__device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* col, const int* diag,
+                                              const double* lu, const double* r, double* y) {
+  double b0 = r[3 * i], b1 = r[3 * i + 1], b2 = r[3 * i + 2];
+  for (int k = rp[i]; k < diag[i]; ++k) {
+    const double* L = lu + size_t(k) * 9;
+    const int j = col[k];
+    const double y0 = y[3 * j], y1 = y[3 * j + 1], y2 = y[3 * j + 2];
+    b0 -= L[0] * y0 + L[1] * y1 + L[2] * y2;
+    b1 -= L[3] * y0 + L[4] * y1 + L[5] * y2;
+    b2 -= L[6] * y0 + L[7] * y1 + L[8] * y2;
+  }
+  y[3 * i] = b0;
+  y[3 * i + 1] = b1;
+  y[3 * i + 2] = b2;
+}
+__device__ __forceinline__ void block_bwd_row(int i, const int* rp, const int* col, const int* diag,
+                                              const double* lu, const double* dinv, const double* y, double* x) {
+  double b0 = y[3 * i], b1 = y[3 * i + 1], b2 = y[3 * i + 2];
+  for (int k = diag[i] + 1; k < rp[i + 1]; ++k) {
+    const double* U = lu + size_t(k) * 9;
+    const int j = col[k];
+    const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+    b0 -= U[0] * x0 + U[1] * x1 + U[2] * x2;
+    b1 -= U[3] * x0 + U[4] * x1 + U[5] * x2;
+    b2 -= U[6] * x0 + U[7] * x1 + U[8] * x2;
+  }
+  const double* D = dinv + size_t(i) * 9;
+  x[3 * i] = D[0] * b0 + D[1] * b1 + D[2] * b2;
+  x[3 * i + 1] = D[3] * b0 + D[4] * b1 + D[5] * b2;
+  x[3 * i + 2] = D[6] * b0 + D[7] * b1 + D[8] * b2;
+}
+
+// out = x_p (prolonged correction) + BlockILU(v - A x_p)   [cooperative: forward then backward]
+__global__ void k_block_sweep_coop(LevelArgs L, const double* __restrict__ lu, const double* __restrict__ dinv,
+                                   const double* __restrict__ cr, double* y, double* x) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int l = 0; l < L.n_levels; ++l) {
+    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+      block_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, cr, y);
+    grid_sync(L.bar, 200);
+  }
+  for (int l = L.n_levels - 1; l >= 0; --l) {
+    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+      block_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, dinv, y, x);
+    grid_sync(L.bar, 201);
+  }
+}
+
+// scalar pressure ILU rows
+__device__ __forceinline__ void p_fwd_row(int r, const int* rp, const int* col, const int* diag, const double* plu,
+                                          const double* rhs, double* y) {
+  double s = rhs[r];
+  for (int k = rp[r]; k < diag[r]; ++k) s -= plu[k] * y[col[k]];
+  y[r] = s;
+}
+__device__ __forceinline__ void p_bwd_row(int r, const int* rp, const int* col, const int* diag, const double* plu,
+                                          const double* pdiag, const double* y, double* x) {
+  double s = y[r];
+  for (int k = diag[r] + 1; k < rp[r + 1]; ++k) s -= plu[k] * x[col[k]];
+  const double d = pdiag[r];
+  x[r] = fabs(d) > kEps ? s / d : s;
+}
+
+// ============================================================================================
+// Cooperative BiCGStab on the pressure system (solve_pressure_with_bicgstab)
+// ============================================================================================
+struct BicgArgs {
+  LevelArgs L;
+  int n;
+  const double* pval;
+  const double* plu;
+  const double* pdiag;
+  const double* rhs;
+  double* x;
+  double* r;
+  double* rh;
+  double* p;
+  double* v;
+  double* ph;
+  double* s;
+  double* sh;
+  double* t;
+  double* y;
+  double* partials;  // 4 * gridDim.x
+  double tol;
+  int max_iters;
+};
+
+// grid-wide sums of up to 3 per-thread values; every block ends with the same totals
+__device__ void grid_sums(const GridBarrier& bar, double* partials, int nq, const double* vals, double* out,
+                          double* sh, int where) {
+  for (int q = 0; q < nq; ++q) {
+    const double r = block_sum<kBlock>(vals[q], sh);
+    if (threadIdx.x == 0) partials[q * gridDim.x + blockIdx.x] = r;
+  }
+  grid_sync(bar, where);
+  __shared__ double tot[4];
+  if (threadIdx.x < nq) {
+    double a = 0.0;
+    const volatile double* pv = partials + threadIdx.x * gridDim.x;
+    for (unsigned b = 0; b < gridDim.x; ++b) a += pv[b];
+    tot[threadIdx.x] = a;
+  }
+  __syncthreads();
+  for (int q = 0; q < nq; ++q) out[q] = tot[q];
+  __syncthreads();
+}
+
+__device__ void pressure_spmv(const LevelArgs& L, const double* pval, const double* x, double* y, int n) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int r = tid; r < n; r += nth) {
+    double s = 0.0;
+    for (int k = L.rp[r]; k < L.rp[r + 1]; ++k) s += pval[k] * x[L.col[k]];
+    y[r] = s;
+  }
+}
+
+__device__ void pressure_ilu_apply(const BicgArgs& a, const double* rhs, double* out) {
+  const LevelArgs& L = a.L;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int l = 0; l < L.n_levels; ++l) {
+    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+      p_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, a.plu, rhs, a.y);
+    grid_sync(L.bar, 300);
+  }
+  for (int l = L.n_levels - 1; l >= 0; --l) {
+    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+      p_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, a.plu, a.pdiag, a.y, out);
+    grid_sync(L.bar, 301);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
+  __shared__ double sh[32];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int n = a.n;
+  double v3[3], o3[3];
+  // x = 0; r = rhs - A*0; r0 norm
+  for (int i = tid; i < n; i += nth) {
+    a.x[i] = 0.0;
+    a.r[i] = a.rhs[i] - 0.0;
+    a.rh[i] = a.r[i];
+    a.v[i] = 0.0;
+    a.p[i] = 0.0;
+  }
+  v3[0] = 0.0;
+  for (int i = tid; i < n; i += nth) v3[0] += a.r[i] * a.r[i];
+  grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 400);
+  if (sqrt(o3[0]) <= a.tol) return;
+  double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  for (int it = 0; it < a.max_iters; ++it) {
+    v3[0] = 0.0;
+    for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.r[i];
+    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 401);
+    const double rho = o3[0];
+    if (!isfinite(rho) || fabs(rho) < kEps) break;
+    if (it == 0) {
+      for (int i = tid; i < n; i += nth) a.p[i] = a.r[i];
+    } else {
+      const double beta = (rho / rho_prev) * (alpha / omega);
+      for (int i = tid; i < n; i += nth) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+    }
+    grid_sync(a.L.bar, 402);
+    pressure_ilu_apply(a, a.p, a.ph);
+    pressure_spmv(a.L, a.pval, a.ph, a.v, n);
+    v3[0] = 0.0;
+    grid_sync(a.L.bar, 403);
+    for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.v[i];
+    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 404);
+    const double vd = o3[0];
+    if (!isfinite(vd) || fabs(vd) < kEps) break;
+    alpha = rho / vd;
+    v3[0] = 0.0;
+    for (int i = tid; i < n; i += nth) {
+      const double si = a.r[i] - alpha * a.v[i];
+      a.s[i] = si;
+      v3[0] += si * si;
+    }
+    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 405);
+    if (sqrt(o3[0]) <= a.tol) {
+      for (int i = tid; i < n; i += nth) a.x[i] += alpha * a.ph[i];
+      break;
+    }
+    pressure_ilu_apply(a, a.s, a.sh);
+    pressure_spmv(a.L, a.pval, a.sh, a.t, n);
+    grid_sync(a.L.bar, 406);
+    v3[0] = 0.0;
+    v3[1] = 0.0;
+    for (int i = tid; i < n; i += nth) {
+      v3[0] += a.t[i] * a.t[i];
+      v3[1] += a.t[i] * a.s[i];
+    }
+    grid_sums(a.L.bar, a.partials, 2, v3, o3, sh, 407);
+    const double tt = o3[0];
+    if (!isfinite(tt) || tt <= kEps) break;
+    omega = o3[1] / tt;
+    if (!isfinite(omega) || fabs(omega) < kEps) break;
+    v3[0] = 0.0;
+    for (int i = tid; i < n; i += nth) {
+      a.x[i] += alpha * a.ph[i] + omega * a.sh[i];
+      const double ri = a.s[i] - omega * a.t[i];
+      a.r[i] = ri;
+      v3[0] += ri * ri;
+    }
+    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 408);
+    if (sqrt(o3[0]) <= a.tol) break;
+    rho_prev = rho;
+  }
+}
+
+// ============================================================================================
+// CPR apply pieces
+// ============================================================================================
+__global__ void k_restrict(int nb, const double* __restrict__ w, const double* __restrict__ v, double* __restrict__ pr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  double s = 0.0;
+  s += w[3 * i] * v[3 * i];
+  s += w[3 * i + 1] * v[3 * i + 1];
+  s += w[3 * i + 2] * v[3 * i + 2];
+  pr[i] = s;
+}
+__global__ void k_prolong(int nb, const double* __restrict__ corr, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  out[3 * i] = 0.0 + 1.0 * corr[i];
+  out[3 * i + 1] = 0.0;
+  out[3 * i + 2] = 0.0;
+}
+__global__ void k_dense_matvec(int n, const double* __restrict__ a, const double* __restrict__ x, double* __restrict__ y) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double s = 0.0;
+  for (int c = 0; c < n; ++c) s += a[size_t(r) * n + c] * x[c];
+  y[r] = s;
+}
+// dense pressure matrix (N <= 299) from the block-pattern values
+__global__ void k_dense_build(int nb, const int* __restrict__ rp, const int* __restrict__ col,
+                              const double* __restrict__ pval, double* __restrict__ a) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nb) return;
+  for (int c = 0; c < nb; ++c) a[size_t(r) * nb + c] = 0.0;
+  for (int k = rp[r]; k < rp[r + 1]; ++k) a[size_t(r) * nb + col[k]] = pval[k];
+}
+// Gauss-Jordan inverse with partial pivoting in global memory, one CTA; ok[0] = 0 when singular.
+__global__ void k_dense_invert(int n, double* a, double* inv, int* ok) {
+  __shared__ int s_piv;
+  __shared__ double s_best;
+  const int t = threadIdx.x;
+  for (int k = t; k < n * n; k += blockDim.x) inv[k] = (k / n == k % n) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int c = 0; c < n; ++c) {
+    if (t == 0) {
+      int piv = c;
+      double best = fabs(a[size_t(c) * n + c]);
+      for (int r = c + 1; r < n; ++r) {
+        const double v = fabs(a[size_t(r) * n + c]);
+        if (v > best) {
+          best = v;
+          piv = r;
+        }
+      }
+      s_piv = piv;
+      s_best = best;
+    }
+    __syncthreads();
+    if (s_best == 0.0) {
+      if (t == 0) ok[0] = 0;
+      return;
+    }
+    const int piv = s_piv;
+    if (piv != c)
+      for (int k = t; k < n; k += blockDim.x) {
+        double x = a[size_t(c) * n + k];
+        a[size_t(c) * n + k] = a[size_t(piv) * n + k];
+        a[size_t(piv) * n + k] = x;
+        x = inv[size_t(c) * n + k];
+        inv[size_t(c) * n + k] = inv[size_t(piv) * n + k];
+        inv[size_t(piv) * n + k] = x;
+      }
+    __syncthreads();
+    const double d = a[size_t(c) * n + c];
+    __syncthreads();
+    for (int k = t; k < n; k += blockDim.x) {
+      a[size_t(c) * n + k] /= d;
+      inv[size_t(c) * n + k] /= d;
+    }
+    __syncthreads();
+    for (long long idx = t; idx < (long long)n * n; idx += blockDim.x) {
+      const int r = int(idx / n), k = int(idx % n);
+      if (r == c) continue;
+      const double f = a[size_t(r) * n + c];
+      if (f == 0.0) continue;
+      if (k != c) a[size_t(r) * n + k] -= f * a[size_t(c) * n + k];
+      inv[size_t(r) * n + k] -= f * inv[size_t(c) * n + k];
+    }
+    __syncthreads();
+    for (int r = t; r < n; r += blockDim.x)
+      if (r != c) a[size_t(r) * n + c] = 0.0;
+    __syncthreads();
+  }
+  if (t == 0) ok[0] = 1;
+}
+
+// ============================================================================================
+// host side
+// ============================================================================================
+static int reduce_blocks(Ctx& c, long long n) {
+  long long b = (n + kBlock - 1) / kBlock;
+  const long long cap = 4ll * c.num_sms;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return int(b);
+}
+
+static void dot_dev(Ctx& c, long long n, const double* a, const double* b, double* out, bool take_sqrt) {
+  const int nb = reduce_blocks(c, n);
+  k_dot_partial<<<nb, kBlock, 0, c.stream>>>(n, a, b, c.d_partials.p);
+  k_reduce_to<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, out, take_sqrt ? 1 : 0);
+  c.launches += 2;
+}
+
+static void spmv_res(Ctx& c, const double* x, const double* b, double* y) {
+  k_spmv<1><<<blocks_for(c.n), kBlock, 0, c.stream>>>(c.n, c.d_row_ptr.p, c.d_col.p, c.d_val.p, x, b, y);
+  c.launches++;
+}
+static void spmv(Ctx& c, const double* x, double* y) {
+  k_spmv<0><<<blocks_for(c.n), kBlock, 0, c.stream>>>(c.n, c.d_row_ptr.p, c.d_col.p, c.d_val.p, x, nullptr, y);
+  c.launches++;
+}
+
+static LevelArgs level_args(Ctx& c) {
+  LevelArgs L;
+  L.n_levels = c.levels.n_levels;
+  L.lvl_rows = c.levels.d_rows;
+  L.lvl_ptr = c.levels.d_ptr;
+  L.rp = c.d_row_ptr.p;
+  L.col = c.d_col.p;
+  L.diag = c.d_diag.p;
+  L.bar.count = c.d_barrier.p;
+  L.bar.gen = c.d_barrier.p + 1;
+  L.bar.status = c.d_status.p;
+  return L;
+}
+
+static void coop_launch(Ctx& c, const void* fn, int blocks, void** args) {
+  RF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kBlock), args, 0, c.stream));
+  c.launches++;
+}
+
+static void check_status(Ctx& c, const char* what) {
+  DeviceStatus st;
+  RF_CUDA(cudaMemcpyAsync(&st, c.d_status.p, sizeof(st), cudaMemcpyDeviceToHost, c.stream));
+  RF_CUDA(cudaStreamSynchronize(c.stream));
+  if (st.code != 0) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "device status %d at site %d after %s", st.code, st.where, what);
+    throw CudaError(buf);
+  }
+}
+
+// CPR preconditioner build on the current reduced matrix
+static void cpr_build(Ctx& c) {
+  const int n = c.n;
+  k_cpr_weights<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_diag.p, c.d_val.p, c.d_cpr_w.p,
+                                                         c.d_bmask.p);
+  k_pressure_matrix<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_val.p, c.d_cpr_w.p, c.d_pval.p);
+  c.launches += 2;
+  LevelArgs L = level_args(c);
+  const double* val = c.d_val.p;
+  const unsigned char* mask = c.d_bmask.p;
+  double* lu = c.d_lu.p;
+  double* dinv = c.d_dinv.p;
+  const double* pval = c.d_pval.p;
+  double* plu = c.d_plu.p;
+  double* pdiag = c.d_pdiag.p;
+  void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
+  coop_launch(c, (const void*)k_factor_coop, c.coop_blocks_sweep, args);
+  c.dense_ok = 0;
+  if (n <= 299) {
+    k_dense_build<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_col.p, c.d_pval.p, c.d_tmp2.p);
+    k_dense_invert<<<1, 1024, 0, c.stream>>>(n, c.d_tmp2.p, c.d_dense.p, c.d_flag_dense.p);
+    c.launches += 2;
+    int ok = 0;
+    RF_CUDA(cudaMemcpyAsync(&ok, c.d_flag_dense.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    c.dense_ok = ok;
+  }
+}
+
+// z = CPR(v)
+static void cpr_apply(Ctx& c, const double* v, double* z) {
+  const int n = c.n;
+  double* prhs = c.d_pvec.p + size_t(10) * n;
+  double* corr = c.d_pvec.p + size_t(11) * n;
+  k_restrict<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_cpr_w.p, v, prhs);
+  c.launches++;
+  if (c.dense_ok) {
+    k_dense_matvec<<<blocks_for(n, 64), 64, 0, c.stream>>>(n, c.d_dense.p, prhs, corr);
+    c.launches++;
+  } else {
+    // tol = max(|prhs|, EPS) * 1e-6 (host reads the norm: the cooperative kernel takes it by value)
+    dot_dev(c, n, prhs, nullptr, c.d_scal.p + 20, true);
+    double nr = 0.0;
+    RF_CUDA(cudaMemcpyAsync(&nr, c.d_scal.p + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    BicgArgs a;
+    a.L = level_args(c);
+    a.n = n;
+    a.pval = c.d_pval.p;
+    a.plu = c.d_plu.p;
+    a.pdiag = c.d_pdiag.p;
+    a.rhs = prhs;
+    a.x = corr;
+    double* base = c.d_pvec.p;
+    a.r = base;
+    a.rh = base + n;
+    a.p = base + 2 * size_t(n);
+    a.v = base + 3 * size_t(n);
+    a.ph = base + 4 * size_t(n);
+    a.s = base + 5 * size_t(n);
+    a.sh = base + 6 * size_t(n);
+    a.t = base + 7 * size_t(n);
+    a.y = base + 8 * size_t(n);
+    a.partials = c.d_partials.p;
+    a.tol = fmax(nr, kEps) * 1e-6;
+    a.max_iters = 50;
+    void* args[] = {&a};
+    coop_launch(c, (const void*)k_bicgstab_coop, c.coop_blocks_bicg, args);
+  }
+  k_prolong<<<blocks_for(n), kBlock, 0, c.stream>>>(n, corr, z);
+  c.launches++;
+  // cr = v - A z_p ; sm = ILU(cr) ; z += sm
+  double* cr = c.d_tmp.p;
+  double* ysw = c.d_tmp2.p;
+  spmv_res(c, z, v, cr);
+  LevelArgs L = level_args(c);
+  const double* lu = c.d_lu.p;
+  const double* dinv = c.d_dinv.p;
+  const double* crp = cr;
+  double* xo = c.d_w.p;
+  void* args[] = {&L, (void*)&lu, (void*)&dinv, (void*)&crp, &ysw, &xo};
+  coop_launch(c, (const void*)k_block_sweep_coop, c.coop_blocks_sweep, args);
+  k_add_inplace<<<reduce_blocks(c, 3ll * n), kBlock, 0, c.stream>>>(3ll * n, c.d_w.p, z);
+  c.launches++;
+}
+
+static inline void givens(double a, double b, double& cs, double& sn) {
+  const double rad = std::hypot(a, b);
+  if (rad <= kEps) {
+    cs = 1.0;
+    sn = 0.0;
+  } else {
+    cs = a / rad;
+    sn = b / rad;
+  }
+}
+
+LinResult linear_solve_reduced(Ctx& c) {
+  LinResult out;
+  const long long n3 = 3ll * c.n;
+  const int R = Ctx::kRestart;
+  double* V = c.d_V.p;
+  double* Z = c.d_Z.p;
+  double* b = c.d_rhs_red.p;
+  double* hbuf = c.d_scal.p + 32;  // H column (R+2)
+  cpr_build(c);
+  dot_dev(c, n3, b, nullptr, c.d_scal.p + 21, true);
+  double rhs_norm = 0.0;
+  RF_CUDA(cudaMemcpyAsync(&rhs_norm, c.d_scal.p + 21, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  RF_CUDA(cudaStreamSynchronize(c.stream));
+  out.rhs_norm = rhs_norm;
+  const double tol = 1e-12 + 5e-3 * fmax(rhs_norm, kEps);
+  // x0 = 0: r = b - A*0, computed explicitly as the reference does
+  RF_CUDA(cudaMemsetAsync(c.d_x.p, 0, sizeof(double) * n3, c.stream));
+  spmv_res(c, c.d_x.p, b, c.d_cres.p);
+  dot_dev(c, n3, c.d_cres.p, nullptr, c.d_scal.p + 22, true);
+  double rn = 0.0;
+  RF_CUDA(cudaMemcpyAsync(&rn, c.d_scal.p + 22, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  RF_CUDA(cudaStreamSynchronize(c.stream));
+  if (rn <= tol) {
+    out.converged = true;
+    out.iterations = 0;
+    out.final_residual_norm = rn;
+    return out;
+  }
+  const double beta = rn;
+  // V0 = r / beta
+  k_scale_div<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_cres.p, c.d_scal.p + 22, V);
+  c.launches++;
+  std::vector<double> H((R + 1) * R, 0.0), cs(R, 0.0), sn(R, 0.0), g(R + 1, 0.0), hcol(R + 2);
+  g[0] = beta;
+  int iters = 0;
+  for (int j = 0; j < R; ++j) {
+    double* vj = V + size_t(j) * n3;
+    double* zj = Z + size_t(j) * n3;
+    double* w = c.d_cand.p;
+    cpr_apply(c, vj, zj);
+    spmv(c, zj, w);
+    for (int p = 0; p <= j; ++p) {
+      double* vp = V + size_t(p) * n3;
+      dot_dev(c, n3, vp, w, hbuf + p, false);
+      k_axpy_dev<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, hbuf + p, vp, w);
+      c.launches++;
+    }
+    dot_dev(c, n3, w, nullptr, hbuf + j + 1, true);
+    RF_CUDA(cudaMemcpyAsync(hcol.data(), hbuf, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    const double nn = hcol[j + 1];
+    auto Hc = [&](int r, int cc) -> double& { return H[size_t(r) * R + cc]; };
+    for (int p = 0; p <= j + 1; ++p) Hc(p, j) = hcol[p];
+    if (nn > kEps && j + 1 <= R) {
+      k_scale_div<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, w, hbuf + j + 1, V + size_t(j + 1) * n3);
+      c.launches++;
+    }
+    for (int p = 0; p < j; ++p) {
+      const double a = Hc(p, j), bb = Hc(p + 1, j);
+      Hc(p, j) = cs[p] * a + sn[p] * bb;
+      Hc(p + 1, j) = -sn[p] * a + cs[p] * bb;
+    }
+    double cc, ss;
+    givens(Hc(j, j), Hc(j + 1, j), cc, ss);
+    cs[j] = cc;
+    sn[j] = ss;
+    {
+      const double a = Hc(j, j), bb = Hc(j + 1, j);
+      Hc(j, j) = cc * a + ss * bb;
+      Hc(j + 1, j) = -ss * a + cc * bb;
+      const double g0 = g[j], g1 = g[j + 1];
+      g[j] = cc * g0 + ss * g1;
+      g[j + 1] = -ss * g0 + cc * g1;
+    }
+    ++iters;
+    const int cols = j + 1;
+    std::vector<double> y(cols, 0.0);
+    for (int r = cols - 1; r >= 0; --r) {
+      double sum = g[r];
+      for (int k = r + 1; k < cols; ++k) sum -= Hc(r, k) * y[k];
+      const double d = Hc(r, r);
+      y[r] = std::fabs(d) > kEps ? sum / d : 0.0;
+    }
+    RF_CUDA(cudaMemcpyAsync(c.d_scal.p + 64, y.data(), sizeof(double) * cols, cudaMemcpyHostToDevice, c.stream));
+    k_combine<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, cols, Z, n3, c.d_scal.p + 64, nullptr, c.d_x.p);
+    spmv_res(c, c.d_x.p, b, c.d_cres.p);
+    dot_dev(c, n3, c.d_cres.p, nullptr, c.d_scal.p + 23, true);
+    c.launches++;
+    double trn = 0.0;
+    RF_CUDA(cudaMemcpyAsync(&trn, c.d_scal.p + 23, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    if (trn <= tol) {
+      out.converged = true;
+      out.iterations = iters;
+      out.final_residual_norm = trn;
+      break;
+    }
+    if (nn <= kEps || iters >= std::max(20, R)) {
+      out.converged = false;
+      out.iterations = iters;
+      out.final_residual_norm = trn;
+      break;
+    }
+  }
+  check_status(c, "FGMRES");
+  return out;
+}
+
+LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
+  const int n = c.n;
+  const long long n3 = 3ll * n;
+  // rhs_red = -res (cell rows); Schur corrects the perforated rows and adds the fill
+  k_neg<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_res.p, c.d_rhs_red.p);
+  c.launches++;
+  const int W = c.topo.n_wells;
+  if (W > 0) {
+    SchurArgs s;
+    s.n_wells = W;
+    s.well_ptr = c.d_well_ptr.p;
+    s.well_perfs = c.d_well_perfs.p;
+    s.perf_cell = c.d_perf_cell.p;
+    s.perf_has_wi = c.d_perf_has_wi.p;
+    s.jrw = c.d_jrw.p;
+    s.jwr_perf = c.d_jwr_perf.p;
+    s.jwr_ctrl = c.d_jwr_ctrl.p;
+    s.jww_perf_bhp = c.d_jww_perf_bhp.p;
+    s.jww_ctrl_q = c.d_jww_ctrl_q.p;
+    s.jww_ctrl_bhp = c.d_jww_ctrl_bhp.p;
+    s.res = c.d_res.p;
+    s.res_tail = c.d_res_tail.p;
+    s.tinv_off = c.d_tinv_off.p;
+    s.tinv = c.d_tinv.p;
+    s.row_ptr = c.d_row_ptr.p;
+    s.fill_off = c.d_fill_off.p;
+    s.fill_pos = c.d_fill_pos.p;
+    s.perf_row_off = c.d_perf_row_off.p;
+    s.val = c.d_val.p;
+    s.jrr_perf = c.d_jrr_perf.p;
+    s.rhs_red = c.d_rhs_red.p;
+    const int nt = 1 + c.topo.max_perfs_per_well;
+    const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
+    k_schur<<<W, kBlock, smem, c.stream>>>(s);
+    c.launches++;
+  }
+  LinResult lin = linear_solve_reduced(c);
+  h_dx_tail.assign(size_t(W) + c.topo.n_perfs, 0.0);
+  // full-system residual: reduced residual for unperforated rows, direct rows elsewhere
+  k_copy<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_cres.p, c.d_full.p);
+  c.launches++;
+  double tail_sq_sum = 0.0;
+  if (W > 0) {
+    RecoverArgs r;
+    r.n_wells = W;
+    r.well_ptr = c.d_well_ptr.p;
+    r.well_perfs = c.d_well_perfs.p;
+    r.perf_cell = c.d_perf_cell.p;
+    r.perf_has_wi = c.d_perf_has_wi.p;
+    r.jrw = c.d_jrw.p;
+    r.jwr_perf = c.d_jwr_perf.p;
+    r.jwr_ctrl = c.d_jwr_ctrl.p;
+    r.jww_perf_bhp = c.d_jww_perf_bhp.p;
+    r.jww_ctrl_q = c.d_jww_ctrl_q.p;
+    r.jww_ctrl_bhp = c.d_jww_ctrl_bhp.p;
+    r.res = c.d_res.p;
+    r.res_tail = c.d_res_tail.p;
+    r.tinv_off = c.d_tinv_off.p;
+    r.tinv = c.d_tinv.p;
+    r.x = c.d_x.p;
+    r.dx_tail = c.d_dx_tail.p;
+    r.row_ptr = c.d_row_ptr.p;
+    r.col = c.d_col.p;
+    r.perf_row_off = c.d_perf_row_off.p;
+    r.jrr_perf = c.d_jrr_perf.p;
+    r.full = c.d_full.p;
+    r.tail_sq = c.d_scal.p + 4096;
+    k_recover<<<W, 32, 0, c.stream>>>(r);
+    c.launches++;
+    RF_CUDA(cudaMemcpyAsync(h_dx_tail.data(), c.d_dx_tail.p, sizeof(double) * h_dx_tail.size(),
+                            cudaMemcpyDeviceToHost, c.stream));
+    std::vector<double> tsq(W);
+    RF_CUDA(cudaMemcpyAsync(tsq.data(), c.d_scal.p + 4096, sizeof(double) * W, cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    for (double v : tsq) tail_sq_sum += v;
+  }
+  dot_dev(c, n3, c.d_full.p, nullptr, c.d_scal.p + 24, false);
+  double sq = 0.0;
+  RF_CUDA(cudaMemcpyAsync(&sq, c.d_scal.p + 24, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  // rhs norm of the full system: |[-res; -res_tail]|
+  dot_dev(c, n3, c.d_res.p, nullptr, c.d_scal.p + 25, false);
+  double rsq = 0.0;
+  RF_CUDA(cudaMemcpyAsync(&rsq, c.d_scal.p + 25, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  std::vector<double> rt(size_t(W) + c.topo.n_perfs);
+  if (!rt.empty())
+    RF_CUDA(cudaMemcpyAsync(rt.data(), c.d_res_tail.p, sizeof(double) * rt.size(), cudaMemcpyDeviceToHost, c.stream));
+  // finiteness of the solution
+  RF_CUDA(cudaMemsetAsync(c.d_flag_dense.p + 1, 0, sizeof(int), c.stream));
+  k_count_nonfinite<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_x.p, c.d_flag_dense.p + 1);
+  c.launches++;
+  int nonfinite = 0;
+  RF_CUDA(cudaMemcpyAsync(&nonfinite, c.d_flag_dense.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  RF_CUDA(cudaStreamSynchronize(c.stream));
+  for (double v : rt) rsq += v * v;
+  for (double v : h_dx_tail)
+    if (!std::isfinite(v)) nonfinite = 1;
+  const double full_norm = std::sqrt(sq + tail_sq_sum);
+  const double rhs_norm = std::sqrt(rsq);
+  const double tol = 1e-12 + 5e-3 * fmax(rhs_norm, kEps);
+  LinResult out;
+  out.iterations = lin.iterations;
+  out.rhs_norm = rhs_norm;
+  out.final_residual_norm = full_norm;
+  out.converged = lin.converged && full_norm <= tol;
+  out.finite = nonfinite == 0;
+  return out;
+}
+
+// ---- one-time setup ----
+void build_levels(Ctx& c) {
+  const int n = c.n;
+  std::vector<int> lvl(n, 0);
+  int maxl = 0;
+  for (int i = 0; i < n; ++i) {
+    int l = 0;
+    for (int k = c.h_row_ptr[i]; k < c.h_diag[i]; ++k) l = std::max(l, lvl[c.h_col[k]] + 1);
+    lvl[i] = l;
+    maxl = std::max(maxl, l);
+  }
+  c.levels.n_levels = maxl + 1;
+  c.levels.h_ptr.assign(c.levels.n_levels + 1, 0);
+  for (int i = 0; i < n; ++i) c.levels.h_ptr[lvl[i] + 1]++;
+  for (int l = 0; l < c.levels.n_levels; ++l) c.levels.h_ptr[l + 1] += c.levels.h_ptr[l];
+  std::vector<int> rows(n), fillp(c.levels.h_ptr.begin(), c.levels.h_ptr.end() - 1);
+  for (int i = 0; i < n; ++i) rows[fillp[lvl[i]]++] = i;
+  RF_CUDA(cudaMalloc(&c.levels.d_rows, sizeof(int) * n));
+  RF_CUDA(cudaMalloc(&c.levels.d_ptr, sizeof(int) * (c.levels.n_levels + 1)));
+  RF_CUDA(cudaMemcpy(c.levels.d_rows, rows.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.levels.d_ptr, c.levels.h_ptr.data(), sizeof(int) * (c.levels.n_levels + 1),
+                     cudaMemcpyHostToDevice));
+}
+
+void setup_linear_workspace(Ctx& c) {
+  const size_t n = c.n, n3 = 3 * n;
+  const int R = Ctx::kRestart;
+  c.d_V.alloc((R + 1) * n3);
+  c.d_Z.alloc(R * n3);
+  c.d_w.alloc(n3);
+  c.d_x.alloc(n3);
+  c.d_tmp.alloc(n3 > n * n ? n3 : n * n);
+  c.d_tmp2.alloc(n3 > n * n ? n3 : n * n);
+  c.d_cand.alloc(n3);
+  c.d_cres.alloc(n3);
+  c.d_full.alloc(n3);
+  c.d_cpr_w.alloc(n3);
+  c.d_pval.alloc(c.nnzb);
+  c.d_plu.alloc(c.nnzb);
+  c.d_pdiag.alloc(n);
+  c.d_lu.alloc(size_t(c.nnzb) * 9);
+  c.d_dinv.alloc(n * 9);
+  c.d_bmask.alloc(c.nnzb);
+  if (n <= 299) c.d_dense.alloc(n * n);
+  c.d_pvec.alloc(12 * n);
+  c.d_partials.alloc(4 * 4096);
+  c.d_scal.alloc(8192);
+  c.d_status.alloc(1);
+  c.d_barrier.alloc(2);
+  c.d_flag_dense.alloc(4);
+  RF_CUDA(cudaMemset(c.d_status.p, 0, sizeof(DeviceStatus)));
+  RF_CUDA(cudaMemset(c.d_barrier.p, 0, 2 * sizeof(unsigned int)));
+  int per_sm = 0;
+  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_coop, kBlock, 0));
+  c.coop_blocks_bicg = std::max(1, std::min(per_sm, 2) * c.num_sms);
+  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_block_sweep_coop, kBlock, 0));
+  int per_sm2 = 0;
+  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_factor_coop, kBlock, 0));
+  c.coop_blocks_sweep = std::max(1, std::min(std::min(per_sm, per_sm2), 2) * c.num_sms);
+  const int nt = 1 + c.topo.max_perfs_per_well;
+  const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
+  if (smem > 48 * 1024) RF_CUDA(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+}
+
+}  // namespace rf

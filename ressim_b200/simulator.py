@@ -1,0 +1,155 @@
+"""`ReservoirSimulator`: the reference simulator's construction/step API over the device path.
+
+Construction and setters mirror the reference (`Deck`); `step(dt)` runs one report step of the
+fully implicit controller on the GPU through the C ABI.  The device context is created at the
+first step, from the deck and the current state.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, _lib
+from .deck import Deck
+
+
+class DeviceError(RuntimeError):
+    pass
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class ReservoirSimulator(Deck):
+    """Drop-in for the reference `ReservoirSimulator` (src/lib/ressim/src/frontend.rs) on the
+    FIM path.  Setters are inherited from `Deck`; the device context is built lazily."""
+
+    def __init__(self, nx, ny, nz, porosity_val, **kw):
+        super().__init__(nx, ny, nz, porosity_val, **kw)
+        self._h = None
+        self._keep = None
+        self.time_days = 0.0
+        self.last_solver_warning = ""
+        self.last_step_report = None
+
+    @classmethod
+    def from_deck(cls, deck: Deck) -> "ReservoirSimulator":
+        sim = cls.__new__(cls)
+        sim.__dict__.update({k: v for k, v in deck.__dict__.items()})
+        sim.wells = list(deck.wells)
+        sim._h = None
+        sim._keep = None
+        sim.time_days = 0.0
+        sim.last_solver_warning = ""
+        sim.last_step_report = None
+        return sim
+
+    # ---- device context ----
+    def _context(self):
+        if self._h is not None:
+            return self._h
+        L = _lib.load()
+        d, keep = self.to_abi()
+        h = C.c_void_p()
+        rc = L.rf_create(C.byref(d), C.byref(h))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_create failed ({rc}): {_lib.last_error(None)}")
+        self._h, self._keep = h, (d, keep)
+        p = np.ascontiguousarray(self.pressure, dtype=np.float64)
+        sw = np.ascontiguousarray(self.sat_water, dtype=np.float64)
+        rc = L.rf_set_state(h, _ptr(p), _ptr(sw), None, None, float(self.time_days))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_set_state failed ({rc}): {_lib.last_error(h)}")
+        return h
+
+    def close(self):
+        if self._h is not None:
+            _lib.load().rf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- stepping (frontend.rs:345-349) ----
+    def step(self, target_dt_days: float) -> dict:
+        h = self._context()
+        rep = _abi.RfStepReport()
+        rc = _lib.load().rf_step(h, float(target_dt_days), C.byref(rep))
+        if rc < 0:
+            raise DeviceError(f"rf_step failed ({rc}): {_lib.last_error(h)}")
+        self.time_days = rep.time_days
+        self.last_step_report = rep.as_dict()
+        self.last_solver_warning = "" if rep.warning == 0 else f"solver warning {rep.warning}"
+        return self.last_step_report
+
+    # ---- getters (frontend.rs:523-605) ----
+    def _state(self):
+        h = self._context()
+        n = self.n_cells
+        out = {k: np.zeros(n) for k in ("pressure", "sat_water", "sat_oil", "sat_gas", "rs")}
+        t = C.c_double()
+        rc = _lib.load().rf_get_state(h, _ptr(out["pressure"]), _ptr(out["sat_water"]), _ptr(out["sat_oil"]),
+                                      _ptr(out["sat_gas"]), _ptr(out["rs"]), C.byref(t))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_get_state failed ({rc}): {_lib.last_error(h)}")
+        out["time"] = t.value
+        return out
+
+    def get_pressures(self):
+        return self._state()["pressure"]
+
+    def get_sat_water(self):
+        return self._state()["sat_water"]
+
+    def get_sat_oil(self):
+        return self._state()["sat_oil"]
+
+    def get_time(self):
+        return self.time_days
+
+    def get_well_bhp(self):
+        b = np.zeros(len(self.wells))
+        _lib.load().rf_get_well_bhp(self._context(), _ptr(b), len(b))
+        return b
+
+    def get_rate_history(self):
+        h = self._context()
+        L = _lib.load()
+        out = []
+        for i in range(L.rf_rate_history_len(h)):
+            r = _abi.RfTimePointRates()
+            L.rf_rate_history_get(h, i, C.byref(r))
+            out.append(r.as_dict())
+        return out
+
+    def get_last_solver_warning(self):
+        return self.last_solver_warning
+
+    def kernel_launches(self) -> int:
+        return int(_lib.load().rf_kernel_launches(self._context()))
+
+    def state(self):
+        return self._state()
+
+
+def linear_solve_bsr(sim: ReservoirSimulator, row_ptr, cols, vals, rhs):
+    """Linear-solver seam: CPR-FGMRES on a tail-free 3x3 block system on `sim`'s grid."""
+    h = sim._context()
+    n = sim.n_cells
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    cl = np.ascontiguousarray(cols, dtype=np.int32)
+    vl = np.ascontiguousarray(vals, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.zeros(3 * n)
+    rep = _abi.RfLinearReport()
+    rc = _lib.load().rf_linear_solve_bsr(h, n, rp.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         cl.ctypes.data_as(C.POINTER(C.c_int32)), _ptr(vl), _ptr(b), _ptr(x),
+                                         C.byref(rep))
+    if rc != _abi.RF_OK:
+        raise DeviceError(f"rf_linear_solve_bsr failed ({rc}): {_lib.last_error(h)}")
+    return x, rep
