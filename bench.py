@@ -1,0 +1,398 @@
+"""FIM report-step throughput on one B200 (cell-steps/s), plus the reference CPU arm.
+
+One bench step is one report step of the fully implicit controller (Newton iterations with
+assembly, well Schur elimination, CPR-FGMRES and the update, including any substeps and retries)
+on a seeded synthetic waterflood deck, run through the C ABI (`rf_step`).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload 72k|2m|1d] [--dt DAYS] [--no-cpu-baseline]
+
+Legs of the default (`--impl ours`) run, all on the same deck:
+  value     device time of K report steps with the state resident in HBM (CUDA events recorded
+            by the library on its own stream around each `rf_step`; L2 flushed between steps);
+  e2e       K more report steps through the public API with host buffers: every step uploads the
+            state from pinned host memory (`rf_set_state`), steps, and reads the state back
+            (`rf_get_state`); each step is timed from before the upload to after the read-back
+            (host clock around synchronous calls, so it covers the device work and the copies);
+  roofline  the cooperative BiCGStab kernel (the pressure stage, the dominant kernel): algorithmic
+            bytes per iteration x iterations per launch / mean launch time (CUDA events);
+  cpu_baseline  the CPU restatement (C++, single thread, like the reference) on the same deck and
+            the same report steps (after the same warm-up steps), in a spawned process beside the
+            GPU legs, bounded to about `--cpu-sample-s` seconds of timed work.
+
+Multi-GPU: the report step does not shard across GPUs in this build, so `--gpus N` under torchrun
+runs N independent replicas of the same deck (weak scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+HBM_FALLBACK_GBS = 6650.0
+
+WORKLOADS = {
+    # name: (nx, ny, nz, dt_days, description)
+    "72k": (60, 60, 20, 10.0,
+            "waterflood_3d 60x60x20 (72,000 cells), two-phase oil-water, log-normal kh (ln-mean ln 100 mD, "
+            "sigma 1, 5-cell correlation), kv/kh 0.1, inverted five-spot (4 rate injectors, 1 BHP producer), "
+            "no gravity, dt 10 d report steps, FP64"),
+    "2m": (200, 200, 50, 10.0,
+           "waterflood_3d 200x200x50 (2,000,000 cells), same statistics and wells, dt 10 d report steps, FP64"),
+    "1d": (200, 1, 1, 10.0, "waterflood_1d 200x1x1, rate injector cell 0, BHP producer cell 199, dt 10 d, FP64"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="72k")
+    ap.add_argument("--dt", type=float, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="wall budget of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def make_deck(workload):
+    from ressim_b200 import decks
+
+    nx, ny, nz, dt, desc = WORKLOADS[workload]
+    if workload == "1d":
+        deck, _, _ = decks.waterflood_1d()
+    else:
+        deck = decks.waterflood_3d(nx, ny, nz, seed=7)
+    return deck, dt, desc
+
+
+def dist_setup(args):
+    """Rank/world from torchrun's environment; each rank sees only its own GPU."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        sm, smax, power = [], [], []
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "power_w_max": max(power) if power else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def measured_hbm_peak():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def bicgstab_bytes_per_iteration(n_cells, nnzb):
+    """Algorithmic bytes of one BiCGStab iteration of the pressure stage (FP64 values, int32 indices):
+    two ILU0 applications (forward + backward: L/U values and columns once, 12 B per entry; per row
+    rhs, y written and read, out, inverse pivot, level row ids and row pointers = 64 B), two SpMVs
+    (12 B per entry; row pointer, x, y = 20 B per row) and the vector updates and dot products
+    (160 B per row)."""
+    return 2 * (12 * nnzb + 64 * n_cells) + 2 * (12 * nnzb + 20 * n_cells) + 160 * n_cells
+
+
+def cpu_leg(workload, dt, warmup, steps, budget_s):
+    """The CPU restatement of the reference FIM (C++, one thread, like the reference) on the same
+    deck and the same report steps as the GPU legs: `warmup` untimed report steps from the initial
+    state, then up to `steps` timed ones (stopping once `budget_s` of wall time is spent, after at
+    least one).  Returns (cell-steps/s, timed steps, seconds, Newton iterations)."""
+    sys.path.insert(0, HERE)
+    from oracle.oracle_py import OracleSimulator
+
+    deck, dt_default, _ = make_deck(workload)
+    dt = dt if dt is not None else dt_default
+    sim = OracleSimulator(deck)
+    for _ in range(warmup):
+        sim.step(dt)
+    n = deck.n_cells
+    k = 0
+    newton = 0
+    el = 0.0
+    while k < steps:
+        t0 = time.perf_counter()
+        _, rep = sim.step(dt)
+        el += time.perf_counter() - t0
+        newton += rep.newton_iterations
+        k += 1
+        if el >= budget_s:
+            break
+    sim.close()
+    return n * k / el, k, el, newton
+
+
+def run_reference(args):
+    """Reference arm: the reference's FIM path on the host cores.  The reference (Rust/WASM) cannot
+    be built in this image (no cargo, rustc or node), so its C++ restatement (oracle) is timed, one
+    thread, as the reference's FIM runs, on the same deck and the same report steps as the GPU arm
+    (W untimed warm-up steps from the initial state, then K timed steps).  Rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    _, dt_default, desc = make_deck(args.workload)
+    dt = args.dt if args.dt is not None else dt_default
+    v, k, el, newton = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
+    n = WORKLOADS[args.workload][0] * WORKLOADS[args.workload][1] * WORKLOADS[args.workload][2]
+    line = {
+        "metric": "FIM cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * el / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded deck generator)",
+        "config": {"workload": desc, "cells": n, "dt_days": dt, "newton_iterations": newton},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                         "sample": f"report steps {args.warmup}..{args.warmup + k - 1} of the deck "
+                                   f"({newton} Newton iterations), C++ restatement of the reference FIM, 1 thread"},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_setup(args)
+    cpu_job = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "2m":
+        import multiprocessing as mp
+
+        pool = mp.get_context("spawn").Pool(1)
+        cpu_job = (pool, pool.apply_async(cpu_leg, (args.workload, args.dt, args.warmup, 2, args.cpu_sample_s)))
+
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from ressim_b200 import ReservoirSimulator, _abi, _lib
+
+    if not torch.cuda.is_available():
+        print(json.dumps({"error": "no CUDA device"}))
+        return 1
+    torch.cuda.set_device(0)
+    dev_index = local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", 0))
+        pg = dist
+
+    deck, dt_default, desc = make_deck(args.workload)
+    dt = args.dt if args.dt is not None else dt_default
+    n = deck.n_cells
+    sim = ReservoirSimulator.from_deck(deck)
+    L = _lib.load()
+    h = sim._context()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def l2_flush():
+        flush.zero_()
+        torch.cuda.synchronize()
+
+    # ---- warm-up (untimed) ----
+    for _ in range(args.warmup):
+        sim.step(dt)
+    l2_flush()
+
+    # ---- device-resident leg ----
+    sim.profile(enable=True, reset=True)
+    launches0 = sim.kernel_launches()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev_index)
+    clocks.start()
+    dev_ms = 0.0
+    newton = lin = substeps = 0
+    reps = []
+    for _ in range(args.steps):
+        r = sim.step(dt)
+        reps.append(r)
+        dev_ms += r["device_ms"]
+        newton += r["newton_iterations"]
+        lin += r["linear_iterations"]
+        substeps += r["substeps"]
+        l2_flush()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = sim.kernel_launches() - launches0
+    prof = sim.profile(enable=False, reset=True)
+    if pg:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_ms_max = float(t.item())
+        pg.barrier()
+    else:
+        dev_ms_max = dev_ms
+    value = world * n * args.steps / (dev_ms_max / 1e3)
+
+    # ---- end-to-end leg: host buffers, copies inside the timed region ----
+    p_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    sw_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    st = sim.state()
+    p_host.numpy()[:] = st["pressure"]
+    sw_host.numpy()[:] = st["sat_water"]
+    pp = C.cast(p_host.data_ptr(), C.POINTER(C.c_double))
+    sp = C.cast(sw_host.data_ptr(), C.POINTER(C.c_double))
+    tt = C.c_double()
+    rep = _abi.RfStepReport()
+    l2_flush()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rc = L.rf_set_state(h, pp, sp, None, None, C.c_double(sim.time_days))
+        if rc != 0:
+            raise RuntimeError(f"rf_set_state failed: {_lib.last_error(h)}")
+        rc = L.rf_step(h, C.c_double(dt), C.byref(rep))
+        if rc < 0:
+            raise RuntimeError(f"rf_step failed: {_lib.last_error(h)}")
+        sim.time_days = rep.time_days
+        rc = L.rf_get_state(h, pp, sp, None, None, None, C.byref(tt))
+        if rc != 0:
+            raise RuntimeError(f"rf_get_state failed: {_lib.last_error(h)}")
+        e2e_s += time.perf_counter() - t0
+        l2_flush()
+    torch.cuda.synchronize()
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n * args.steps / e2e_s
+
+    # ---- roofline of the dominant kernel (BiCGStab pressure stage) ----
+    peak, peak_kind = measured_hbm_peak()
+    iters, launches_b, nnzb = prof["bicgstab_iterations"], prof["bicgstab_launches"], prof["nnzb"]
+    kernel_ms = prof["bicgstab_kernel"]
+    roof = None
+    if launches_b > 0 and kernel_ms > 0:
+        bytes_launch = bicgstab_bytes_per_iteration(n, nnzb) * iters / launches_b
+        ms_launch = kernel_ms / launches_b
+        achieved = bytes_launch / (ms_launch / 1e3) / 1e9
+        roof = {"kernel": "k_bicgstab_coop", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "bytes_per_launch": bytes_launch, "ms_per_launch": ms_launch,
+                "iterations_per_launch": iters / launches_b,
+                "share_of_step": kernel_ms / max(dev_ms, 1e-9)}
+    phases = {k: round(prof[k], 1) for k in _lib.PHASES}
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----
+    cpu = None
+    if cpu_job is not None:
+        pool, job = cpu_job
+        try:
+            v, k, el, cnewton = job.get(timeout=900)
+            cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                   "sample": f"report steps {args.warmup}..{args.warmup + k - 1} of the same deck after "
+                             f"{args.warmup} untimed ones ({cnewton} Newton iterations, {el:.1f} s), C++ "
+                             f"restatement of the reference FIM, 1 thread, run beside the GPU legs"}
+        except Exception as e:  # noqa: BLE001 - reported in the line
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+        pool.terminate()
+
+    if rank == 0:
+        line = {
+            "metric": "FIM cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded deck generator)",
+            "config": {"workload": desc, "cells": n, "dt_days": dt, "parallelism": f"replicas{world}",
+                       "l2": "flushed (256 MB write) between timed report steps",
+                       "newton_iterations": newton, "linear_iterations": lin, "substeps": substeps},
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * n,
+                    "d2h_bytes_per_step": 2 * 8 * n},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
+            "phase_ms": phases,
+        }
+        print(json.dumps(line), flush=True)
+    del sim
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -167,6 +167,15 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
 /* Number of kernel launches this context has issued since creation (device work counter). */
 int64_t rf_kernel_launches(const RfCtx* ctx);
 
+/* Phase timing (FimStepStats' assembly / preconditioner / linear-solve / update split,
+ * src/lib/ressim/src/reporting.rs:191-243) measured with CUDA events on the context's stream.
+ * out (may be NULL) receives up to n values, read before the enable/reset below take effect:
+ * ms for assembly, well elimination, CPR build, pressure stage, block-ILU0 smoother, Krylov,
+ * update, the BiCGStab kernel alone; then the BiCGStab iteration total, the number of BiCGStab
+ * launches timed, and the block count of the reduced matrix.
+ * enable > 0 switches the profiler on, 0 off, < 0 leaves it as is; reset != 0 zeroes the totals. */
+int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n);
+
 #ifdef __cplusplus
 }
 #endif

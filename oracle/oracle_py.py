@@ -59,7 +59,9 @@ def lib():
         L.orc_water_inverse_fvf.restype = C.c_double
         L.orc_well_index.argtypes = [C.POINTER(_abi.RfDeck), C.c_int32]
         L.orc_well_index.restype = C.c_double
-        L.orc_ad_probe.argtypes = [C.c_double, C.c_double, _dp]
+        L.orc_ad_probe.argtypes = [C.c_int32, C.c_double, C.c_double, _dp]
+        L.orc_assemble_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp, _ip, _ip, _dp, _ip, _ip, _dp]
+        L.orc_topology.argtypes = [C.c_void_p, _ip, _ip]
         _lib = L
     return _lib
 
@@ -136,6 +138,27 @@ class OracleSimulator:
         val = np.zeros(nnz.value)
         lib().orc_assemble_current(self._h, dt, C.byref(nu), C.byref(nnz), ptr(res), iptr(ptr_), iptr(col),
                                    ptr(val))
+        return res, ptr_, col, val
+
+    def topology(self):
+        w, p = C.c_int32(), C.c_int32()
+        lib().orc_topology(self._h, C.byref(w), C.byref(p))
+        return w.value, p.value
+
+    def assemble_state(self, dt, prev, cur, bhp, q):
+        """Residual and CSR Jacobian at (cur, bhp, q) against `prev`; prev/cur are (n, 3) arrays."""
+        prev = np.ascontiguousarray(prev, dtype=np.float64).ravel()
+        cur = np.ascontiguousarray(cur, dtype=np.float64).ravel()
+        bhp = np.ascontiguousarray(bhp, dtype=np.float64)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        nu, nnz = C.c_int32(), C.c_int32()
+        args = (self._h, dt, ptr(prev), ptr(cur), ptr(bhp) if bhp.size else None, ptr(q) if q.size else None)
+        lib().orc_assemble_state(*args, C.byref(nu), C.byref(nnz), None, None, None, None)
+        res = np.zeros(nu.value)
+        ptr_ = np.zeros(nu.value + 1, dtype=np.int32)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        val = np.zeros(nnz.value)
+        lib().orc_assemble_state(*args, C.byref(nu), C.byref(nnz), ptr(res), iptr(ptr_), iptr(col), ptr(val))
         return res, ptr_, col, val
 
     def initial_well_state(self, n_wells, n_perfs):

@@ -276,7 +276,10 @@ inline bool try_inverse(const Dense& m, Dense& out) {
     out(2, 2) = (m11 * m22 - m21 * m12) / det;
     return true;
   }
-  // LU with partial pivoting.
+  // LU with partial pivoting, in nalgebra's operation order (linalg/lu.rs `try_invert_to`,
+  // `gauss_step`; linalg/solve.rs triangular solves): the first largest |pivot| wins, the
+  // multipliers are scaled by the pivot's reciprocal, each update is y = (-p) * c + y, and the
+  // back substitution applies the columns from the last one down.
   Dense lu = m;
   std::vector<int> perm(n);
   std::iota(perm.begin(), perm.end(), 0);
@@ -289,31 +292,31 @@ inline bool try_inverse(const Dense& m, Dense& out) {
         piv = r;
       }
     }
-    if (best == 0.0) return false;
+    if (lu(piv, c) == 0.0) return false;
     if (piv != c) {
       for (int k = 0; k < n; ++k) std::swap(lu(c, k), lu(piv, k));
       std::swap(perm[c], perm[piv]);
     }
-    const double d = lu(c, c);
-    for (int r = c + 1; r < n; ++r) {
-      const double f = lu(r, c) / d;
-      lu(r, c) = f;
-      if (f != 0.0)
-        for (int k = c + 1; k < n; ++k) lu(r, k) -= f * lu(c, k);
+    const double inv_pivot = 1.0 / lu(c, c);
+    for (int r = c + 1; r < n; ++r) lu(r, c) = lu(r, c) * inv_pivot;
+    for (int k = c + 1; k < n; ++k) {
+      const double p = -lu(c, k);
+      for (int r = c + 1; r < n; ++r) lu(r, k) = p * lu(r, c) + lu(r, k);
     }
   }
   std::vector<double> col(n);
   for (int j = 0; j < n; ++j) {
     for (int r = 0; r < n; ++r) col[r] = (perm[r] == j) ? 1.0 : 0.0;
-    for (int r = 0; r < n; ++r) {
-      double s = col[r];
-      for (int k = 0; k < r; ++k) s -= lu(r, k) * col[k];
-      col[r] = s;
+    for (int i = 0; i + 1 < n; ++i) {
+      const double coeff = -col[i];
+      for (int r = i + 1; r < n; ++r) col[r] = coeff * lu(r, i) + col[r];
     }
-    for (int r = n - 1; r >= 0; --r) {
-      double s = col[r];
-      for (int k = r + 1; k < n; ++k) s -= lu(r, k) * col[k];
-      col[r] = s / lu(r, r);
+    for (int i = n - 1; i >= 0; --i) {
+      const double d = lu(i, i);
+      if (d == 0.0) return false;
+      const double coeff = col[i] / d;
+      col[i] = coeff;
+      for (int r = 0; r < i; ++r) col[r] = (-coeff) * lu(r, i) + col[r];
     }
     for (int r = 0; r < n; ++r) out(r, j) = col[r];
   }

@@ -36,6 +36,7 @@ def load():
     L.rf_linear_solve_bsr.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp, _dp, _dp, C.POINTER(_abi.RfLinearReport)]
     L.rf_kernel_launches.argtypes = [C.c_void_p]
     L.rf_kernel_launches.restype = C.c_int64
+    L.rf_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32]
     _lib = L
     return L
 
@@ -49,4 +50,8 @@ def last_error(handle) -> str:
 EXPORTED_SYMBOLS = (
     "rf_create", "rf_destroy", "rf_last_error", "rf_set_state", "rf_get_state", "rf_get_well_bhp",
     "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_kernel_launches",
+    "rf_profile",
 )
+
+PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",
+          "bicgstab_kernel")

@@ -288,9 +288,12 @@ static NewtonReport run_newton(Ctx& c, WellState& ws, double dt) {
   std::vector<double> dx_tail;
   PerfCells pc;
   for (int it = 0; it < max_it; ++it) {
-    upload_wells(c, ws);
-    launch_assembly(c, dt);
-    launch_norms(c, dt, st);
+    {
+      PhaseScope ps(c, kPhAssembly);
+      upload_wells(c, ws);
+      launch_assembly(c, dt);
+      launch_norms(c, dt, st);
+    }
     FamNorms fam;
     fam.w = st[0];
     fam.o = st[1];
@@ -321,6 +324,7 @@ static NewtonReport run_newton(Ctx& c, WellState& ws, double dt) {
       }
     }
     // wells: relaxed + chopped update of BHP (dbhp-max-rel 1.0, floor 1 bar) and rates
+    PhaseScope ps_update(c, kPhUpdate);
     const int W = c.topo.n_wells, P = c.topo.n_perfs;
     WellState cand = ws;
     for (int w = 0; w < W; ++w) {
@@ -545,6 +549,7 @@ static int step(Ctx& c, double target, RfStepReport* out) {
     }
   }
   if (!warning && substeps == max_sub && stepped < target) warning = 3;
+  prof_resolve(c);
   RF_CUDA(cudaEventRecord(c.ev1, c.stream));
   RF_CUDA(cudaEventSynchronize(c.ev1));
   float ms = 0.f;
@@ -857,6 +862,8 @@ static void setup_device(Ctx& c) {
   c.d_rhs_red.alloc(3 * size_t(n));
   build_levels(c);
   setup_linear_workspace(c);
+  // every upload above used the default stream; the context's stream is non-blocking
+  RF_CUDA(cudaDeviceSynchronize());
 }
 
 static void free_ctx(Ctx& c) {
@@ -870,14 +877,20 @@ static void free_ctx(Ctx& c) {
     b->free();
   for (auto* b : {&c.d_row_ptr, &c.d_col, &c.d_diag, &c.d_stencil, &c.d_fill_off, &c.d_fill_pos, &c.d_perf_cell,
                   &c.d_perf_well, &c.d_perf_inj, &c.d_perf_has_wi, &c.d_well_ptr, &c.d_well_perfs, &c.d_tinv_off,
-                  &c.d_perf_row_off, &c.d_flag_dense})
+                  &c.d_perf_row_off, &c.d_flag_dense, &c.d_dense_perm})
     b->free();
   c.d_bmask.free();
   c.d_ctrl.free();
   c.d_status.free();
   c.d_barrier.free();
+  if (c.d_bar64) cudaFree(c.d_bar64);
+  c.d_bar64 = nullptr;
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
+  for (cudaEvent_t e : c.ev_pool) cudaEventDestroy(e);
+  c.ev_pool.clear();
+  if (c.d_bicg_iters) cudaFree(c.d_bicg_iters);
+  c.d_bicg_iters = nullptr;
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   if (c.stream) cudaStreamDestroy(c.stream);
@@ -965,9 +978,10 @@ int32_t rf_set_state(RfCtx* ctx, const double* p, const double* sw, const double
     (void)rs;
     c.h_p.assign(p, p + c.n);
     c.h_sw.assign(sw, sw + c.n);
-    RF_CUDA(cudaMemcpy(c.d_p.p, p, sizeof(double) * c.n, cudaMemcpyHostToDevice));
-    RF_CUDA(cudaMemcpy(c.d_sw.p, sw, sizeof(double) * c.n, cudaMemcpyHostToDevice));
-    RF_CUDA(cudaMemset(c.d_hc.p, 0, sizeof(double) * c.n));
+    RF_CUDA(cudaMemcpyAsync(c.d_p.p, p, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream));
+    RF_CUDA(cudaMemcpyAsync(c.d_sw.p, sw, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream));
+    RF_CUDA(cudaMemsetAsync(c.d_hc.p, 0, sizeof(double) * c.n, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
     c.time_days = t;
     return RF_OK;
   });
@@ -979,8 +993,9 @@ int32_t rf_get_state(const RfCtx* cctx, double* p, double* sw, double* so, doubl
   return guarded(ctx, [&]() -> int32_t {
     rf::Ctx& c = ctx->c;
     std::vector<double> hp(c.n), hsw(c.n);
-    RF_CUDA(cudaMemcpy(hp.data(), c.d_p.p, sizeof(double) * c.n, cudaMemcpyDeviceToHost));
-    RF_CUDA(cudaMemcpy(hsw.data(), c.d_sw.p, sizeof(double) * c.n, cudaMemcpyDeviceToHost));
+    RF_CUDA(cudaMemcpyAsync(hp.data(), c.d_p.p, sizeof(double) * c.n, cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaMemcpyAsync(hsw.data(), c.d_sw.p, sizeof(double) * c.n, cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
     for (int i = 0; i < c.n; ++i) {
       if (p) p[i] = hp[i];
       if (sw) sw[i] = hsw[i];
@@ -1035,10 +1050,12 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
         const size_t pos = size_t(it - c.h_col.begin());
         for (int q = 0; q < 9; ++q) vals[pos * 9 + q] += block_vals[size_t(k) * 9 + q];
       }
-    RF_CUDA(cudaMemcpy(c.d_val.p, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice));
-    RF_CUDA(cudaMemcpy(c.d_rhs_red.p, rhs, sizeof(double) * 3 * c.n, cudaMemcpyHostToDevice));
+    RF_CUDA(cudaMemcpyAsync(c.d_val.p, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, c.stream));
+    RF_CUDA(cudaMemcpyAsync(c.d_rhs_red.p, rhs, sizeof(double) * 3 * c.n, cudaMemcpyHostToDevice, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
     rf::LinResult r = rf::linear_solve_reduced(c);
-    RF_CUDA(cudaMemcpy(x, c.d_x.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost));
+    RF_CUDA(cudaMemcpyAsync(x, c.d_x.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
     if (out) {
       out->converged = r.converged;
       out->iterations = r.iterations;
@@ -1050,5 +1067,32 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
 }
 
 int64_t rf_kernel_launches(const RfCtx* ctx) { return ctx ? ctx->c.launches : 0; }
+
+int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n) {
+  if (!ctx) return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t {
+    rf::Ctx& c = ctx->c;
+    rf::prof_resolve(c);
+    if (out) {
+      long long it = 0;
+      RF_CUDA(cudaMemcpyAsync(&it, c.d_bicg_iters, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+      RF_CUDA(cudaStreamSynchronize(c.stream));
+      for (int k = 0; k < n && k < rf::kPhCount; ++k) out[k] = c.phase_ms[k];
+      if (n > rf::kPhCount) out[rf::kPhCount] = double(it);
+      if (n > rf::kPhCount + 1) out[rf::kPhCount + 1] = double(c.phase_count[rf::kPhBicgKernel]);
+      if (n > rf::kPhCount + 2) out[rf::kPhCount + 2] = double(c.nnzb);
+    }
+    if (enable >= 0) c.profiling = enable > 0;
+    if (reset) {
+      for (int k = 0; k < 8; ++k) {
+        c.phase_ms[k] = 0.0;
+        c.phase_count[k] = 0;
+      }
+      RF_CUDA(cudaMemsetAsync(c.d_bicg_iters, 0, sizeof(long long), c.stream));
+      RF_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    return RF_OK;
+  });
+}
 
 }  // extern "C"

@@ -119,16 +119,79 @@ struct Ctx {
   DBuf<unsigned char> d_bmask;  // block present in the reduced matrix (any |v| > EPS, or diagonal)
   DBuf<double> d_cres, d_full;  // last FGMRES true residual, full-system residual rows
   DBuf<double> d_dense;       // N*N dense pressure inverse when N <= 299
+  DBuf<int> d_dense_perm;     // its row permutation
   int dense_ok = 0;
   DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
   DBuf<double> d_partials, d_scal;
   DBuf<DeviceStatus> d_status;
   DBuf<unsigned int> d_barrier;  // count, gen
+  unsigned long long* d_bar64 = nullptr;  // grid-barrier arrival counter of cooperative launches
   int coop_blocks_bicg = 0, coop_blocks_sweep = 0;
   DBuf<int> d_flag_dense;
 
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // opt-in phase profiler: pairs of events per phase, resolved at the end of each step
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long phase_count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long* d_bicg_iters = nullptr;  // device counter of BiCGStab iterations
 };
+
+// Phases of one Newton iteration reported by rf_profile.
+enum Phase {
+  kPhAssembly = 0,  // residual/Jacobian assembly and norms
+  kPhSchur = 1,     // well elimination and recovery
+  kPhCprBuild = 2,  // weights, pressure matrix, ILU0 factorisations
+  kPhCoarse = 3,    // pressure stage (BiCGStab or dense)
+  kPhSmoother = 4,  // r - A x_p and the block-ILU0 sweep
+  kPhKrylov = 5,    // FGMRES SpMV, Gram-Schmidt, candidate and true residual
+  kPhUpdate = 6,    // chop/update, wells, substep reductions
+  kPhBicgKernel = 7,  // the cooperative BiCGStab kernel alone (inside kPhCoarse)
+  kPhCount = 8
+};
+
+inline cudaEvent_t prof_event(Ctx& c) {
+  if (c.ev_used == c.ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c.ev_pool.push_back(e);
+  }
+  return c.ev_pool[c.ev_used++];
+}
+struct PhaseScope {
+  Ctx& c;
+  int phase;
+  cudaEvent_t a = nullptr;
+  PhaseScope(Ctx& c_, int ph) : c(c_), phase(ph) {
+    if (c.profiling) {
+      a = prof_event(c);
+      cudaEventRecord(a, c.stream);
+    }
+  }
+  ~PhaseScope() {
+    if (c.profiling) {
+      cudaEvent_t b = prof_event(c);
+      cudaEventRecord(b, c.stream);
+      c.ev_pending.push_back({phase, {a, b}});
+    }
+  }
+};
+inline void prof_resolve(Ctx& c) {
+  if (!c.profiling) return;
+  cudaStreamSynchronize(c.stream);
+  for (auto& pe : c.ev_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
+      c.phase_ms[pe.first] += ms;
+      c.phase_count[pe.first]++;
+    }
+  }
+  c.ev_pending.clear();
+  c.ev_used = 0;
+}
 
 }  // namespace rf

@@ -72,40 +72,43 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
   return r;
 }
 
-// Software grid barrier for cooperative launches (all blocks co-resident).  `count` and `gen`
-// live in device memory and start at zero.  The spin is bounded: after `kBarrierPollLimit`
-// polls the barrier records code 1 in `status` and releases.  Once the status word is set every
-// later barrier returns at once, so a failed launch runs its bounded loops to the end instead
-// of hanging; the host reads the status after the launch and reports the failure.
+// Software grid barrier for cooperative launches (all blocks co-resident).  `count` is a 64-bit
+// arrival counter set to zero before each launch (stream-ordered memset); barrier k of a launch
+// completes when it reaches (k + 1) * gridDim.x.  Arrival is a release reduction and the wait an
+// acquire load followed by a fence, so the block's writes before the barrier are visible to every
+// block's plain loads after it.  The
+// spin is bounded: after kBarrierPollLimit polls it records code 1 in `status` and releases; once
+// the status is set every later barrier returns at once, so a failed launch runs its bounded
+// loops to the end instead of hanging, and the host reports the failure after the launch.
 struct GridBarrier {
-  unsigned int* count;
-  volatile unsigned int* gen;
+  unsigned long long* count;
   volatile DeviceStatus* status;
 };
 
 constexpr long long kBarrierPollLimit = 1ll << 24;
 
-__device__ __forceinline__ void grid_sync(const GridBarrier& b, int where) {
+__device__ __forceinline__ void grid_sync(const GridBarrier& b, unsigned long long& target, int where) {
   __syncthreads();
-  if (threadIdx.x == 0 && b.status->code == 0) {
-    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned int my_gen = *b.gen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(b.count, 1u);
-    if (arrived == nblocks - 1) {
-      *b.count = 0;
-      __threadfence();
-      atomicAdd((unsigned int*)b.gen, 1u);
-    } else {
+  target += gridDim.x * gridDim.y * gridDim.z;
+  if (threadIdx.x == 0) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(b.count) : "memory");
+    if (b.status->code == 0) {
       long long polls = 0;
-      while (*b.gen == my_gen && b.status->code == 0) {
-        if (++polls > kBarrierPollLimit) {
-          b.status->where = where;
-          b.status->code = 1;
-          break;
+      while (true) {
+        unsigned long long v;
+        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(b.count) : "memory");
+        if (v >= target) break;
+        if ((++polls & 255) == 0) {
+          if (b.status->code != 0) break;
+          if (polls > kBarrierPollLimit) {
+            b.status->where = where;
+            b.status->code = 1;
+            break;
+          }
         }
       }
     }
+    // make every thread's later plain loads see the other blocks' writes (L1 is not coherent)
     __threadfence();
   }
   __syncthreads();

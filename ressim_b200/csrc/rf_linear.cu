@@ -552,6 +552,9 @@ __device__ void block_ilu_row(int i, const int* rp, const int* col, const int* d
   mat3_inverse_or_diag(lu + size_t(dp) * 9, dinv + size_t(i) * 9);
 }
 
+// Level-scheduled triangular work: rows of level l depend only on rows of lower levels, so each
+// level is one parallel pass followed by a grid barrier.  The row arithmetic is the reference's,
+// in the reference's order, so factors and solves equal the natural-order sequential ones.
 struct LevelArgs {
   int n_levels;
   const int* lvl_rows;
@@ -562,17 +565,19 @@ struct LevelArgs {
   GridBarrier bar;
 };
 
-__global__ void k_factor_coop(LevelArgs L, const double* __restrict__ val, const unsigned char* __restrict__ mask,
-                              double* lu, double* dinv, const double* __restrict__ pval, double* plu, double* pdiag) {
+__global__ void __launch_bounds__(kBlock) k_factor_coop(LevelArgs L, const double* __restrict__ val,
+                                                         const unsigned char* __restrict__ mask, double* lu,
+                                                         double* dinv, const double* __restrict__ pval, double* plu,
+                                                         double* pdiag) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  unsigned long long bt = 0;
   for (int l = 0; l < L.n_levels; ++l) {
-    const int a = L.lvl_ptr[l], b = L.lvl_ptr[l + 1];
-    for (int q = a + tid; q < b; q += nth) {
+    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth) {
       const int r = L.lvl_rows[q];
       block_ilu_row(r, L.rp, L.col, L.diag, val, mask, lu, dinv);
       pressure_ilu_row(r, L.rp, L.col, L.diag, pval, plu, pdiag);
     }
-    grid_sync(L.bar, 100);
+    grid_sync(L.bar, bt, 100);
   }
 }
 
@@ -584,12 +589,12 @@ __device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* c
                                               const double* lu, const double* r, double* y) {
   double b0 = r[3 * i], b1 = r[3 * i + 1], b2 = r[3 * i + 2];
   for (int k = rp[i]; k < diag[i]; ++k) {
-    const double* L = lu + size_t(k) * 9;
+    const double* Lb = lu + size_t(k) * 9;
     const int j = col[k];
     const double y0 = y[3 * j], y1 = y[3 * j + 1], y2 = y[3 * j + 2];
-    b0 -= L[0] * y0 + L[1] * y1 + L[2] * y2;
-    b1 -= L[3] * y0 + L[4] * y1 + L[5] * y2;
-    b2 -= L[6] * y0 + L[7] * y1 + L[8] * y2;
+    b0 -= Lb[0] * y0 + Lb[1] * y1 + Lb[2] * y2;
+    b1 -= Lb[3] * y0 + Lb[4] * y1 + Lb[5] * y2;
+    b2 -= Lb[6] * y0 + Lb[7] * y1 + Lb[8] * y2;
   }
   y[3 * i] = b0;
   y[3 * i + 1] = b1;
@@ -612,19 +617,21 @@ __device__ __forceinline__ void block_bwd_row(int i, const int* rp, const int* c
   x[3 * i + 2] = D[6] * b0 + D[7] * b1 + D[8] * b2;
 }
 
-// out = x_p (prolonged correction) + BlockILU(v - A x_p)   [cooperative: forward then backward]
-__global__ void k_block_sweep_coop(LevelArgs L, const double* __restrict__ lu, const double* __restrict__ dinv,
-                                   const double* __restrict__ cr, double* y, double* x) {
+// x = BlockILU(cr)   [cooperative: forward levels, then backward levels]
+__global__ void __launch_bounds__(kBlock) k_block_sweep_coop(LevelArgs L, const double* __restrict__ lu,
+                                                              const double* __restrict__ dinv,
+                                                              const double* __restrict__ cr, double* y, double* x) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  unsigned long long bt = 0;
   for (int l = 0; l < L.n_levels; ++l) {
     for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
       block_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, cr, y);
-    grid_sync(L.bar, 200);
+    grid_sync(L.bar, bt, 200);
   }
   for (int l = L.n_levels - 1; l >= 0; --l) {
     for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
       block_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, dinv, y, x);
-    grid_sync(L.bar, 201);
+    if (l > 0) grid_sync(L.bar, bt, 201);
   }
 }
 
@@ -663,23 +670,30 @@ struct BicgArgs {
   double* sh;
   double* t;
   double* y;
-  double* partials;  // 4 * gridDim.x
+  double* partials;  // 2 x 4 x gridDim.x
   double tol;
   int max_iters;
+  long long* iter_counter;  // incremented by the iterations this solve ran
 };
 
-// grid-wide sums of up to 3 per-thread values; every block ends with the same totals
-__device__ void grid_sums(const GridBarrier& bar, double* partials, int nq, const double* vals, double* out,
-                          double* sh, int where) {
+// Grid-wide sums of up to 4 per-thread values; every block ends with the same totals.  The
+// partials alternate between two buffers (`parity`, advanced identically by every block): a block
+// may run ahead into the next reduction and overwrite its own slot while a slower block is still
+// reading this reduction's partials, but it cannot reach the reduction after that before the
+// slower block has passed the barrier in between.
+__device__ void grid_sums(const GridBarrier& bar, unsigned long long& bt, double* partials, int& parity, int nq,
+                          const double* vals, double* out, double* sh, int where) {
+  double* buf = partials + (parity & 1) * 4 * gridDim.x;
+  ++parity;
   for (int q = 0; q < nq; ++q) {
     const double r = block_sum<kBlock>(vals[q], sh);
-    if (threadIdx.x == 0) partials[q * gridDim.x + blockIdx.x] = r;
+    if (threadIdx.x == 0) buf[q * gridDim.x + blockIdx.x] = r;
   }
-  grid_sync(bar, where);
+  grid_sync(bar, bt, where);
   __shared__ double tot[4];
   if (threadIdx.x < nq) {
     double a = 0.0;
-    const volatile double* pv = partials + threadIdx.x * gridDim.x;
+    const volatile double* pv = buf + threadIdx.x * gridDim.x;
     for (unsigned b = 0; b < gridDim.x; ++b) a += pv[b];
     tot[threadIdx.x] = a;
   }
@@ -697,18 +711,20 @@ __device__ void pressure_spmv(const LevelArgs& L, const double* pval, const doub
   }
 }
 
-__device__ void pressure_ilu_apply(const BicgArgs& a, const double* rhs, double* out) {
+// out = PressureILU(rhs): forward levels, backward levels, each level ended by a grid barrier
+// (the last one also publishes `out` to the SpMV that follows).
+__device__ void pressure_ilu_apply(const BicgArgs& a, const double* rhs, double* out, unsigned long long& bt) {
   const LevelArgs& L = a.L;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int l = 0; l < L.n_levels; ++l) {
     for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
       p_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, a.plu, rhs, a.y);
-    grid_sync(L.bar, 300);
+    grid_sync(L.bar, bt, 300);
   }
   for (int l = L.n_levels - 1; l >= 0; --l) {
     for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
       p_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, a.plu, a.pdiag, a.y, out);
-    grid_sync(L.bar, 301);
+    grid_sync(L.bar, bt, 301);
   }
 }
 
@@ -717,6 +733,8 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const int n = a.n;
   double v3[3], o3[3];
+  int parity = 0;
+  unsigned long long bt = 0;
   // x = 0; r = rhs - A*0; r0 norm
   for (int i = tid; i < n; i += nth) {
     a.x[i] = 0.0;
@@ -727,13 +745,15 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
   }
   v3[0] = 0.0;
   for (int i = tid; i < n; i += nth) v3[0] += a.r[i] * a.r[i];
-  grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 400);
-  if (sqrt(o3[0]) <= a.tol) return;
+  grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 400);
+  const int max_iters = sqrt(o3[0]) <= a.tol ? 0 : a.max_iters;
   double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
-  for (int it = 0; it < a.max_iters; ++it) {
+  int started = 0;
+  for (int it = 0; it < max_iters; ++it) {
+    started = it + 1;
     v3[0] = 0.0;
     for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.r[i];
-    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 401);
+    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 401);
     const double rho = o3[0];
     if (!isfinite(rho) || fabs(rho) < kEps) break;
     if (it == 0) {
@@ -742,13 +762,13 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
       const double beta = (rho / rho_prev) * (alpha / omega);
       for (int i = tid; i < n; i += nth) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
     }
-    grid_sync(a.L.bar, 402);
-    pressure_ilu_apply(a, a.p, a.ph);
+    grid_sync(a.L.bar, bt, 402);
+    pressure_ilu_apply(a, a.p, a.ph, bt);
     pressure_spmv(a.L, a.pval, a.ph, a.v, n);
     v3[0] = 0.0;
-    grid_sync(a.L.bar, 403);
+    grid_sync(a.L.bar, bt, 403);
     for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.v[i];
-    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 404);
+    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 404);
     const double vd = o3[0];
     if (!isfinite(vd) || fabs(vd) < kEps) break;
     alpha = rho / vd;
@@ -758,21 +778,21 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
       a.s[i] = si;
       v3[0] += si * si;
     }
-    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 405);
+    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 405);
     if (sqrt(o3[0]) <= a.tol) {
       for (int i = tid; i < n; i += nth) a.x[i] += alpha * a.ph[i];
       break;
     }
-    pressure_ilu_apply(a, a.s, a.sh);
+    pressure_ilu_apply(a, a.s, a.sh, bt);
     pressure_spmv(a.L, a.pval, a.sh, a.t, n);
-    grid_sync(a.L.bar, 406);
+    grid_sync(a.L.bar, bt, 406);
     v3[0] = 0.0;
     v3[1] = 0.0;
     for (int i = tid; i < n; i += nth) {
       v3[0] += a.t[i] * a.t[i];
       v3[1] += a.t[i] * a.s[i];
     }
-    grid_sums(a.L.bar, a.partials, 2, v3, o3, sh, 407);
+    grid_sums(a.L.bar, bt, a.partials, parity, 2, v3, o3, sh, 407);
     const double tt = o3[0];
     if (!isfinite(tt) || tt <= kEps) break;
     omega = o3[1] / tt;
@@ -784,10 +804,11 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
       a.r[i] = ri;
       v3[0] += ri * ri;
     }
-    grid_sums(a.L.bar, a.partials, 1, v3, o3, sh, 408);
+    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 408);
     if (sqrt(o3[0]) <= a.tol) break;
     rho_prev = rho;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.iter_counter) atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
 }
 
 // ============================================================================================
@@ -824,61 +845,100 @@ __global__ void k_dense_build(int nb, const int* __restrict__ rp, const int* __r
   for (int c = 0; c < nb; ++c) a[size_t(r) * nb + c] = 0.0;
   for (int k = rp[r]; k < rp[r + 1]; ++k) a[size_t(r) * nb + col[k]] = pval[k];
 }
-// Gauss-Jordan inverse with partial pivoting in global memory, one CTA; ok[0] = 0 when singular.
-__global__ void k_dense_invert(int n, double* a, double* inv, int* ok) {
-  __shared__ int s_piv;
-  __shared__ double s_best;
-  const int t = threadIdx.x;
-  for (int k = t; k < n * n; k += blockDim.x) inv[k] = (k / n == k % n) ? 1.0 : 0.0;
+// Dense inverse by LU with partial pivoting in nalgebra's operation order (linalg/lu.rs
+// `try_invert_to` and `gauss_step`, linalg/solve.rs triangular solves), one CTA, matrices in
+// global memory.  Every step updates each element once, so spreading a step over threads keeps
+// the sequential rounding: the first largest |pivot| of the column wins, multipliers are scaled by
+// the pivot's reciprocal, updates are y = (-p) * c + y, the forward solve has a unit diagonal and
+// the back substitution applies the columns from the last one down.  ok[0] = 0 when a pivot is
+// exactly zero.  `a` is overwritten by the factors; `perm` holds n ints.
+__global__ void __launch_bounds__(1024) k_dense_invert(int n, double* a, double* inv, int* perm, int* ok) {
+  __shared__ int s_piv[32];
+  __shared__ double s_best[32];
+  __shared__ int s_fail;
+  const int t = threadIdx.x, nt = blockDim.x, lane = t & 31;
+  for (int r = t; r < n; r += nt) perm[r] = r;
+  if (t == 0) s_fail = 0;
   __syncthreads();
   for (int c = 0; c < n; ++c) {
-    if (t == 0) {
-      int piv = c;
-      double best = fabs(a[size_t(c) * n + c]);
-      for (int r = c + 1; r < n; ++r) {
+    if (t < 32) {
+      // first maximum of |a[r][c]| over r >= c (strictly larger replaces)
+      int piv = -1;
+      double best = 0.0;
+      for (int r = c + lane; r < n; r += 32) {
         const double v = fabs(a[size_t(r) * n + c]);
-        if (v > best) {
+        if (piv < 0 || v > best) {
           best = v;
           piv = r;
         }
       }
-      s_piv = piv;
-      s_best = best;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int op = __shfl_down_sync(0xffffffffu, piv, o);
+        if (op >= 0 && (piv < 0 || ob > best || (ob == best && op < piv))) {
+          best = ob;
+          piv = op;
+        }
+      }
+      if (lane == 0) {
+        s_piv[0] = piv;
+        if (a[size_t(piv) * n + c] == 0.0) s_fail = 1;
+      }
     }
     __syncthreads();
-    if (s_best == 0.0) {
+    if (s_fail) {
       if (t == 0) ok[0] = 0;
       return;
     }
-    const int piv = s_piv;
-    if (piv != c)
-      for (int k = t; k < n; k += blockDim.x) {
-        double x = a[size_t(c) * n + k];
+    const int piv = s_piv[0];
+    if (piv != c) {
+      for (int k = t; k < n; k += nt) {
+        const double x = a[size_t(c) * n + k];
         a[size_t(c) * n + k] = a[size_t(piv) * n + k];
         a[size_t(piv) * n + k] = x;
-        x = inv[size_t(c) * n + k];
-        inv[size_t(c) * n + k] = inv[size_t(piv) * n + k];
-        inv[size_t(piv) * n + k] = x;
       }
-    __syncthreads();
-    const double d = a[size_t(c) * n + c];
-    __syncthreads();
-    for (int k = t; k < n; k += blockDim.x) {
-      a[size_t(c) * n + k] /= d;
-      inv[size_t(c) * n + k] /= d;
+      if (t == 0) {
+        const int q = perm[c];
+        perm[c] = perm[piv];
+        perm[piv] = q;
+      }
     }
     __syncthreads();
-    for (long long idx = t; idx < (long long)n * n; idx += blockDim.x) {
-      const int r = int(idx / n), k = int(idx % n);
-      if (r == c) continue;
-      const double f = a[size_t(r) * n + c];
-      if (f == 0.0) continue;
-      if (k != c) a[size_t(r) * n + k] -= f * a[size_t(c) * n + k];
-      inv[size_t(r) * n + k] -= f * inv[size_t(c) * n + k];
+    const double inv_pivot = 1.0 / a[size_t(c) * n + c];
+    for (int r = c + 1 + t; r < n; r += nt) a[size_t(r) * n + c] = a[size_t(r) * n + c] * inv_pivot;
+    __syncthreads();
+    const int m = n - c - 1;
+    for (long long idx = t; idx < (long long)m * m; idx += nt) {
+      const int r = c + 1 + int(idx / m), k = c + 1 + int(idx % m);
+      const double p = -a[size_t(c) * n + k];
+      a[size_t(r) * n + k] = p * a[size_t(r) * n + c] + a[size_t(r) * n + k];
     }
     __syncthreads();
-    for (int r = t; r < n; r += blockDim.x)
-      if (r != c) a[size_t(r) * n + c] = 0.0;
+  }
+  // inv = P I, then the unit-lower and upper solves on all columns at once
+  for (long long idx = t; idx < (long long)n * n; idx += nt) {
+    const int r = int(idx / n), j = int(idx % n);
+    inv[idx] = (perm[r] == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int i = 0; i + 1 < n; ++i) {
+    const int m = n - i - 1;
+    for (long long idx = t; idx < (long long)m * n; idx += nt) {
+      const int r = i + 1 + int(idx / n), j = int(idx % n);
+      const double coeff = -inv[size_t(i) * n + j];
+      inv[size_t(r) * n + j] = coeff * a[size_t(r) * n + i] + inv[size_t(r) * n + j];
+    }
+    __syncthreads();
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    const double d = a[size_t(i) * n + i];
+    for (int j = t; j < n; j += nt) inv[size_t(i) * n + j] = inv[size_t(i) * n + j] / d;
+    __syncthreads();
+    for (long long idx = t; idx < (long long)i * n; idx += nt) {
+      const int r = int(idx / n), j = int(idx % n);
+      const double coeff = inv[size_t(i) * n + j];
+      inv[size_t(r) * n + j] = (-coeff) * a[size_t(r) * n + i] + inv[size_t(r) * n + j];
+    }
     __syncthreads();
   }
   if (t == 0) ok[0] = 1;
@@ -911,6 +971,7 @@ static void spmv(Ctx& c, const double* x, double* y) {
   c.launches++;
 }
 
+// Arguments of one cooperative level-scheduled launch; the barrier counter is reset in stream order.
 static LevelArgs level_args(Ctx& c) {
   LevelArgs L;
   L.n_levels = c.levels.n_levels;
@@ -919,9 +980,9 @@ static LevelArgs level_args(Ctx& c) {
   L.rp = c.d_row_ptr.p;
   L.col = c.d_col.p;
   L.diag = c.d_diag.p;
-  L.bar.count = c.d_barrier.p;
-  L.bar.gen = c.d_barrier.p + 1;
+  L.bar.count = c.d_bar64;
   L.bar.status = c.d_status.p;
+  RF_CUDA(cudaMemsetAsync(c.d_bar64, 0, sizeof(unsigned long long), c.stream));
   return L;
 }
 
@@ -943,6 +1004,7 @@ static void check_status(Ctx& c, const char* what) {
 
 // CPR preconditioner build on the current reduced matrix
 static void cpr_build(Ctx& c) {
+  PhaseScope ps(c, kPhCprBuild);
   const int n = c.n;
   k_cpr_weights<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_diag.p, c.d_val.p, c.d_cpr_w.p,
                                                          c.d_bmask.p);
@@ -961,7 +1023,7 @@ static void cpr_build(Ctx& c) {
   c.dense_ok = 0;
   if (n <= 299) {
     k_dense_build<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_col.p, c.d_pval.p, c.d_tmp2.p);
-    k_dense_invert<<<1, 1024, 0, c.stream>>>(n, c.d_tmp2.p, c.d_dense.p, c.d_flag_dense.p);
+    k_dense_invert<<<1, 1024, 0, c.stream>>>(n, c.d_tmp2.p, c.d_dense.p, c.d_dense_perm.p, c.d_flag_dense.p);
     c.launches += 2;
     int ok = 0;
     RF_CUDA(cudaMemcpyAsync(&ok, c.d_flag_dense.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
@@ -975,6 +1037,8 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
   const int n = c.n;
   double* prhs = c.d_pvec.p + size_t(10) * n;
   double* corr = c.d_pvec.p + size_t(11) * n;
+  {
+  PhaseScope ps(c, kPhCoarse);
   k_restrict<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_cpr_w.p, v, prhs);
   c.launches++;
   if (c.dense_ok) {
@@ -1007,11 +1071,15 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
     a.partials = c.d_partials.p;
     a.tol = fmax(nr, kEps) * 1e-6;
     a.max_iters = 50;
+    a.iter_counter = c.d_bicg_iters;
     void* args[] = {&a};
+    PhaseScope pk(c, kPhBicgKernel);
     coop_launch(c, (const void*)k_bicgstab_coop, c.coop_blocks_bicg, args);
   }
   k_prolong<<<blocks_for(n), kBlock, 0, c.stream>>>(n, corr, z);
   c.launches++;
+  }
+  PhaseScope ps(c, kPhSmoother);
   // cr = v - A z_p ; sm = ILU(cr) ; z += sm
   double* cr = c.d_tmp.p;
   double* ysw = c.d_tmp2.p;
@@ -1078,6 +1146,7 @@ LinResult linear_solve_reduced(Ctx& c) {
     double* zj = Z + size_t(j) * n3;
     double* w = c.d_cand.p;
     cpr_apply(c, vj, zj);
+    PhaseScope ps(c, kPhKrylov);
     spmv(c, zj, w);
     for (int p = 0; p <= j; ++p) {
       double* vp = V + size_t(p) * n3;
@@ -1154,6 +1223,7 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
   c.launches++;
   const int W = c.topo.n_wells;
   if (W > 0) {
+    PhaseScope ps(c, kPhSchur);
     SchurArgs s;
     s.n_wells = W;
     s.well_ptr = c.d_well_ptr.p;
@@ -1189,6 +1259,7 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
   c.launches++;
   double tail_sq_sum = 0.0;
   if (W > 0) {
+    PhaseScope ps(c, kPhSchur);
     RecoverArgs r;
     r.n_wells = W;
     r.well_ptr = c.d_well_ptr.p;
@@ -1285,8 +1356,8 @@ void setup_linear_workspace(Ctx& c) {
   c.d_Z.alloc(R * n3);
   c.d_w.alloc(n3);
   c.d_x.alloc(n3);
-  c.d_tmp.alloc(n3 > n * n ? n3 : n * n);
-  c.d_tmp2.alloc(n3 > n * n ? n3 : n * n);
+  c.d_tmp.alloc(n3);
+  c.d_tmp2.alloc(n <= 299 && n * n > n3 ? n * n : n3);  // also the dense pressure matrix when N <= 299
   c.d_cand.alloc(n3);
   c.d_cres.alloc(n3);
   c.d_full.alloc(n3);
@@ -1297,22 +1368,29 @@ void setup_linear_workspace(Ctx& c) {
   c.d_lu.alloc(size_t(c.nnzb) * 9);
   c.d_dinv.alloc(n * 9);
   c.d_bmask.alloc(c.nnzb);
-  if (n <= 299) c.d_dense.alloc(n * n);
+  if (n <= 299) {
+    c.d_dense.alloc(n * n);
+    c.d_dense_perm.alloc(n);
+  }
   c.d_pvec.alloc(12 * n);
   c.d_partials.alloc(4 * 4096);
   c.d_scal.alloc(8192);
   c.d_status.alloc(1);
   c.d_barrier.alloc(2);
   c.d_flag_dense.alloc(4);
+  RF_CUDA(cudaMalloc(&c.d_bar64, sizeof(unsigned long long)));
+  RF_CUDA(cudaMemset(c.d_bar64, 0, sizeof(unsigned long long)));
+  RF_CUDA(cudaMalloc(&c.d_bicg_iters, sizeof(long long)));
+  RF_CUDA(cudaMemset(c.d_bicg_iters, 0, sizeof(long long)));
   RF_CUDA(cudaMemset(c.d_status.p, 0, sizeof(DeviceStatus)));
   RF_CUDA(cudaMemset(c.d_barrier.p, 0, 2 * sizeof(unsigned int)));
   int per_sm = 0;
   RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_coop, kBlock, 0));
-  c.coop_blocks_bicg = std::max(1, std::min(per_sm, 2) * c.num_sms);
+  c.coop_blocks_bicg = std::max(1, std::min(per_sm, 1) * c.num_sms);
   RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_block_sweep_coop, kBlock, 0));
   int per_sm2 = 0;
   RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_factor_coop, kBlock, 0));
-  c.coop_blocks_sweep = std::max(1, std::min(std::min(per_sm, per_sm2), 2) * c.num_sms);
+  c.coop_blocks_sweep = std::max(1, std::min(std::min(per_sm, per_sm2), 1) * c.num_sms);
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
   if (smem > 48 * 1024) RF_CUDA(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));

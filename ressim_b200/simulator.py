@@ -130,6 +130,21 @@ class ReservoirSimulator(Deck):
     def get_last_solver_warning(self):
         return self.last_solver_warning
 
+    def profile(self, enable=None, reset=False) -> dict:
+        """Phase timings (ms, CUDA events) and the BiCGStab iteration total; `enable` switches the
+        profiler on/off."""
+        out = np.zeros(len(_lib.PHASES) + 3)
+        en = -1 if enable is None else int(bool(enable))
+        rc = _lib.load().rf_profile(self._context(), en, int(reset), _ptr(out), len(out))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_profile failed ({rc}): {_lib.last_error(self._context())}")
+        d = {k: float(v) for k, v in zip(_lib.PHASES, out)}
+        k = len(_lib.PHASES)
+        d["bicgstab_iterations"] = int(out[k])
+        d["bicgstab_launches"] = int(out[k + 1])
+        d["nnzb"] = int(out[k + 2])
+        return d
+
     def kernel_launches(self) -> int:
         return int(_lib.load().rf_kernel_launches(self._context()))
 

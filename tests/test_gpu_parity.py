@@ -96,8 +96,9 @@ def _csr_to_bsr(n_cells, ptr, col, val):
     return np.array(rp), np.array(cols), np.concatenate(vals)
 
 
-def test_linear_seam_matches_oracle():
-    deck = decks.waterflood_3d(10, 9, 3, seed=11, rate_per_perf=20.0)
+@pytest.mark.parametrize("dims", [(10, 9, 3), (12, 10, 3)])  # dense coarse inverse | BiCGStab coarse
+def test_linear_seam_matches_oracle(dims):
+    deck = decks.waterflood_3d(*dims, seed=11, rate_per_perf=20.0)
     deck.wells = []  # tail-free system
     deck.pressure = deck.pressure + np.linspace(0.0, 30.0, deck.n_cells)
     cpu = OracleSimulator(deck)
