@@ -81,7 +81,8 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1 and args.impl == "ours":
-        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+        visible = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+        os.environ["CUDA_VISIBLE_DEVICES"] = visible[local] if local < len(visible) else str(local)
     return rank, world, local
 
 
@@ -246,7 +247,8 @@ def main():
         print(json.dumps({"error": "no CUDA device"}))
         return 1
     torch.cuda.set_device(0)
-    dev_index = local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)
+    # nvidia-smi -i takes the index or UUID that CUDA_VISIBLE_DEVICES names (set per rank above)
+    dev_index = (os.environ.get("CUDA_VISIBLE_DEVICES", "") or "0").split(",")[0].strip() or "0"
     pg = None
     if world > 1:
         import datetime

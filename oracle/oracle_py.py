@@ -60,6 +60,7 @@ def lib():
         L.orc_well_index.argtypes = [C.POINTER(_abi.RfDeck), C.c_int32]
         L.orc_well_index.restype = C.c_double
         L.orc_ad_probe.argtypes = [C.c_int32, C.c_double, C.c_double, _dp]
+        L.orc_set_sum_order.argtypes = [C.c_int32]
         L.orc_assemble_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp, _ip, _ip, _dp, _ip, _ip, _dp]
         L.orc_topology.argtypes = [C.c_void_p, _ip, _ip]
         _lib = L

@@ -396,15 +396,25 @@ inline void csr_matvec(const Csr& m, const std::vector<double>& x, std::vector<d
   }
 }
 
-inline double vnorm(const std::vector<double>& x) {
+// Summation order of the vector dots and norms: 0 is the reference's left-to-right order.  A
+// test hook sets 1 (256 interleaved partial sums, then added in order), which changes only the
+// rounding, to measure how far rounding alone moves a run.
+inline int g_sum_order = 0;
+inline double vdot_n(size_t n, const double* a, const double* b) {
+  if (g_sum_order == 0) {
+    double s = 0.0;
+    for (size_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+  }
+  double part[256] = {0.0};
+  for (size_t i = 0; i < n; ++i) part[i & 255] += a[i] * b[i];
   double s = 0.0;
-  for (double v : x) s += v * v;
-  return std::sqrt(s);
-}
-inline double vdot(const std::vector<double>& a, const std::vector<double>& b) {
-  double s = 0.0;
-  for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+  for (int k = 0; k < 256; ++k) s += part[k];
   return s;
+}
+inline double vnorm(const std::vector<double>& x) { return std::sqrt(vdot_n(x.size(), x.data(), x.data())); }
+inline double vdot(const std::vector<double>& a, const std::vector<double>& b) {
+  return vdot_n(a.size(), a.data(), b.data());
 }
 
 }  // namespace orc

@@ -881,10 +881,6 @@ static void free_ctx(Ctx& c) {
     b->free();
   c.d_bmask.free();
   c.d_ctrl.free();
-  c.d_status.free();
-  c.d_barrier.free();
-  if (c.d_bar64) cudaFree(c.d_bar64);
-  c.d_bar64 = nullptr;
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
   for (cudaEvent_t e : c.ev_pool) cudaEventDestroy(e);

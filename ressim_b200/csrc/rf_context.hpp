@@ -123,10 +123,7 @@ struct Ctx {
   int dense_ok = 0;
   DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
   DBuf<double> d_partials, d_scal;
-  DBuf<DeviceStatus> d_status;
-  DBuf<unsigned int> d_barrier;  // count, gen
-  unsigned long long* d_bar64 = nullptr;  // grid-barrier arrival counter of cooperative launches
-  int coop_blocks_bicg = 0, coop_blocks_sweep = 0;
+  int cluster_size = 0;  // CTAs in the one cluster that runs the level-scheduled kernels
   DBuf<int> d_flag_dense;
 
   // timing
@@ -150,7 +147,7 @@ enum Phase {
   kPhSmoother = 4,  // r - A x_p and the block-ILU0 sweep
   kPhKrylov = 5,    // FGMRES SpMV, Gram-Schmidt, candidate and true residual
   kPhUpdate = 6,    // chop/update, wells, substep reductions
-  kPhBicgKernel = 7,  // the cooperative BiCGStab kernel alone (inside kPhCoarse)
+  kPhBicgKernel = 7,  // the BiCGStab kernel alone (inside kPhCoarse)
   kPhCount = 8
 };
 

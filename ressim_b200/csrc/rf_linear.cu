@@ -8,7 +8,7 @@
 //                              pressure ILU0 and block ILU0 factorisations in the reference's
 //                              natural order (gmres_block_jacobi.rs:178-353, 746-808, 919-1363)
 //   CPR apply                  restrict -> coarse solve (dense inverse when N <= 299, else a
-//                              cooperative persistent BiCGStab with pressure ILU0, at most 50
+//                              one-cluster persistent BiCGStab with pressure ILU0, at most 50
 //                              iterations, tol 1e-6 relative) -> prolong -> r - A x_p ->
 //                              block-ILU0 sweep -> add (gmres_block_jacobi.rs:471-729)
 //   FGMRES(30)                 right-preconditioned flexible GMRES, x0 = 0, modified
@@ -18,7 +18,6 @@
 // A block is "present" in the ILU pattern when any of its entries exceeds EPS in magnitude (the
 // reference builds its ILU0 pattern that way); absent blocks are held as zeros and receive no
 // fill.  Pressure-matrix entries with |v| <= 1e-14 are dropped, as the reference does.
-#include <cooperative_groups.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -553,31 +552,65 @@ __device__ void block_ilu_row(int i, const int* rp, const int* col, const int* d
 }
 
 // Level-scheduled triangular work: rows of level l depend only on rows of lower levels, so each
-// level is one parallel pass followed by a grid barrier.  The row arithmetic is the reference's,
-// in the reference's order, so factors and solves equal the natural-order sequential ones.
-struct LevelArgs {
+// level is one parallel pass followed by a barrier.  The row arithmetic is the reference's, in the
+// reference's order, so factors and solves equal the natural-order sequential ones.
+//
+// These kernels run as ONE thread-block cluster (up to 16 CTAs of 512-1024 threads) and separate
+// the levels with the hardware cluster barrier (barrier.cluster arrive.release / wait.acquire):
+// a level of a 7-point grid holds at most a few thousand rows, so a cluster covers it in one pass,
+// and the per-level cost is the cluster barrier instead of a grid-wide software barrier through
+// L2.  Every thread of every CTA takes the same number of barriers (loop bounds are uniform), so no
+// wait can be left open.  Vectors written by other CTAs inside the same launch are read with
+// ld.global.cg (L2), never from a possibly stale L1 line.
+constexpr int kCBlock = 1024;      // threads per CTA: sweeps and BiCGStab
+constexpr int kFBlock = 512;       // threads per CTA: factorisation (more registers per row)
+constexpr int kSmemLevels = 4096;  // level pointers staged in shared memory up to this many levels
+
+struct LevelSched {
   int n_levels;
   const int* lvl_rows;
   const int* lvl_ptr;
   const int* rp;
   const int* col;
   const int* diag;
-  GridBarrier bar;
 };
 
-__global__ void __launch_bounds__(kBlock) k_factor_coop(LevelArgs L, const double* __restrict__ val,
-                                                         const unsigned char* __restrict__ mask, double* lu,
-                                                         double* dinv, const double* __restrict__ pval, double* plu,
-                                                         double* pdiag) {
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile(
+      "barrier.cluster.arrive.release.aligned;\n\t"
+      "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_nblocks() {
+  unsigned v;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(v));
+  return v;
+}
+
+// level pointers from shared memory when they fit (one fewer dependent global load per level)
+__device__ __forceinline__ const int* stage_levels(const LevelSched& L, int* s_ptr) {
+  if (L.n_levels + 1 <= kSmemLevels) {
+    for (int i = threadIdx.x; i <= L.n_levels; i += blockDim.x) s_ptr[i] = L.lvl_ptr[i];
+    __syncthreads();
+    return s_ptr;
+  }
+  return L.lvl_ptr;
+}
+
+__global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(LevelSched L, const double* __restrict__ val,
+                                                                const unsigned char* __restrict__ mask, double* lu,
+                                                                double* dinv, const double* __restrict__ pval,
+                                                                double* plu, double* pdiag) {
+  __shared__ int s_ptr[kSmemLevels];
+  const int* lp = stage_levels(L, s_ptr);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  unsigned long long bt = 0;
   for (int l = 0; l < L.n_levels; ++l) {
-    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth) {
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) {
       const int r = L.lvl_rows[q];
       block_ilu_row(r, L.rp, L.col, L.diag, val, mask, lu, dinv);
       pressure_ilu_row(r, L.rp, L.col, L.diag, pval, plu, pdiag);
     }
-    grid_sync(L.bar, bt, 100);
+    cluster_barrier();
   }
 }
 
@@ -587,11 +620,11 @@ __global__ void __launch_bounds__(kBlock) k_factor_coop(LevelArgs L, const doubl
 // block: y_i = r_i - sum L_ik y_k (forward); x_i = Dinv_i (y_i - sum U_ij x_j) (backward)
 __device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* col, const int* diag,
                                               const double* lu, const double* r, double* y) {
-  double b0 = r[3 * i], b1 = r[3 * i + 1], b2 = r[3 * i + 2];
+  double b0 = __ldcg(r + 3 * i), b1 = __ldcg(r + 3 * i + 1), b2 = __ldcg(r + 3 * i + 2);
   for (int k = rp[i]; k < diag[i]; ++k) {
     const double* Lb = lu + size_t(k) * 9;
     const int j = col[k];
-    const double y0 = y[3 * j], y1 = y[3 * j + 1], y2 = y[3 * j + 2];
+    const double y0 = __ldcg(y + 3 * j), y1 = __ldcg(y + 3 * j + 1), y2 = __ldcg(y + 3 * j + 2);
     b0 -= Lb[0] * y0 + Lb[1] * y1 + Lb[2] * y2;
     b1 -= Lb[3] * y0 + Lb[4] * y1 + Lb[5] * y2;
     b2 -= Lb[6] * y0 + Lb[7] * y1 + Lb[8] * y2;
@@ -602,11 +635,11 @@ __device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* c
 }
 __device__ __forceinline__ void block_bwd_row(int i, const int* rp, const int* col, const int* diag,
                                               const double* lu, const double* dinv, const double* y, double* x) {
-  double b0 = y[3 * i], b1 = y[3 * i + 1], b2 = y[3 * i + 2];
+  double b0 = __ldcg(y + 3 * i), b1 = __ldcg(y + 3 * i + 1), b2 = __ldcg(y + 3 * i + 2);
   for (int k = diag[i] + 1; k < rp[i + 1]; ++k) {
     const double* U = lu + size_t(k) * 9;
     const int j = col[k];
-    const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+    const double x0 = __ldcg(x + 3 * j), x1 = __ldcg(x + 3 * j + 1), x2 = __ldcg(x + 3 * j + 2);
     b0 -= U[0] * x0 + U[1] * x1 + U[2] * x2;
     b1 -= U[3] * x0 + U[4] * x1 + U[5] * x2;
     b2 -= U[6] * x0 + U[7] * x1 + U[8] * x2;
@@ -617,44 +650,45 @@ __device__ __forceinline__ void block_bwd_row(int i, const int* rp, const int* c
   x[3 * i + 2] = D[6] * b0 + D[7] * b1 + D[8] * b2;
 }
 
-// x = BlockILU(cr)   [cooperative: forward levels, then backward levels]
-__global__ void __launch_bounds__(kBlock) k_block_sweep_coop(LevelArgs L, const double* __restrict__ lu,
-                                                              const double* __restrict__ dinv,
-                                                              const double* __restrict__ cr, double* y, double* x) {
+// x = BlockILU(cr)   [one cluster: forward levels, then backward levels]
+__global__ void __launch_bounds__(kCBlock, 1) k_block_sweep_cluster(LevelSched L, const double* __restrict__ lu,
+                                                                     const double* __restrict__ dinv,
+                                                                     const double* __restrict__ cr, double* y,
+                                                                     double* x) {
+  __shared__ int s_ptr[kSmemLevels];
+  const int* lp = stage_levels(L, s_ptr);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  unsigned long long bt = 0;
   for (int l = 0; l < L.n_levels; ++l) {
-    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
-      block_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, cr, y);
-    grid_sync(L.bar, bt, 200);
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) block_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, cr, y);
+    cluster_barrier();
   }
   for (int l = L.n_levels - 1; l >= 0; --l) {
-    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth)
       block_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, dinv, y, x);
-    if (l > 0) grid_sync(L.bar, bt, 201);
+    if (l > 0) cluster_barrier();
   }
 }
 
 // scalar pressure ILU rows
 __device__ __forceinline__ void p_fwd_row(int r, const int* rp, const int* col, const int* diag, const double* plu,
                                           const double* rhs, double* y) {
-  double s = rhs[r];
-  for (int k = rp[r]; k < diag[r]; ++k) s -= plu[k] * y[col[k]];
+  double s = __ldcg(rhs + r);
+  for (int k = rp[r]; k < diag[r]; ++k) s -= plu[k] * __ldcg(y + col[k]);
   y[r] = s;
 }
 __device__ __forceinline__ void p_bwd_row(int r, const int* rp, const int* col, const int* diag, const double* plu,
                                           const double* pdiag, const double* y, double* x) {
-  double s = y[r];
-  for (int k = diag[r] + 1; k < rp[r + 1]; ++k) s -= plu[k] * x[col[k]];
+  double s = __ldcg(y + r);
+  for (int k = diag[r] + 1; k < rp[r + 1]; ++k) s -= plu[k] * __ldcg(x + col[k]);
   const double d = pdiag[r];
   x[r] = fabs(d) > kEps ? s / d : s;
 }
 
 // ============================================================================================
-// Cooperative BiCGStab on the pressure system (solve_pressure_with_bicgstab)
+// BiCGStab on the pressure system (solve_pressure_with_bicgstab), one cluster
 // ============================================================================================
 struct BicgArgs {
-  LevelArgs L;
+  LevelSched L;
   int n;
   const double* pval;
   const double* plu;
@@ -670,31 +704,37 @@ struct BicgArgs {
   double* sh;
   double* t;
   double* y;
-  double* partials;  // 2 x 4 x gridDim.x
-  double tol;
   int max_iters;
   long long* iter_counter;  // incremented by the iterations this solve ran
 };
 
-// Grid-wide sums of up to 4 per-thread values; every block ends with the same totals.  The
-// partials alternate between two buffers (`parity`, advanced identically by every block): a block
-// may run ahead into the next reduction and overwrite its own slot while a slower block is still
-// reading this reduction's partials, but it cannot reach the reduction after that before the
-// slower block has passed the barrier in between.
-__device__ void grid_sums(const GridBarrier& bar, unsigned long long& bt, double* partials, int& parity, int nq,
-                          const double* vals, double* out, double* sh, int where) {
-  double* buf = partials + (parity & 1) * 4 * gridDim.x;
+// Cluster-wide sums of up to 4 per-thread values; every CTA ends with the same totals (each CTA
+// adds the CTAs' partials in rank order from distributed shared memory, so the result is
+// deterministic and identical everywhere).  The partials alternate between two slots (`parity`,
+// advanced identically by every CTA): a CTA may run ahead into the next reduction and overwrite
+// its own slot while a slower CTA is still reading this reduction's partials, but it cannot reach
+// the reduction after that before the slower CTA has passed the barrier in between.
+__device__ void cluster_sums(double* red /* shared [2][4] */, int& parity, int nq, const double* vals, double* out,
+                             double* sh) {
+  double* buf = red + (parity & 1) * 4;
   ++parity;
   for (int q = 0; q < nq; ++q) {
-    const double r = block_sum<kBlock>(vals[q], sh);
-    if (threadIdx.x == 0) buf[q * gridDim.x + blockIdx.x] = r;
+    const double r = block_sum<kCBlock>(vals[q], sh);
+    if (threadIdx.x == 0) buf[q] = r;
   }
-  grid_sync(bar, bt, where);
+  cluster_barrier();
   __shared__ double tot[4];
   if (threadIdx.x < nq) {
     double a = 0.0;
-    const volatile double* pv = buf + threadIdx.x * gridDim.x;
-    for (unsigned b = 0; b < gridDim.x; ++b) a += pv[b];
+    const unsigned nb = cluster_nblocks();
+    const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(buf + threadIdx.x));
+    for (unsigned b = 0; b < nb; ++b) {
+      unsigned remote;
+      double v;
+      asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(addr), "r"(b));
+      asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(remote) : "memory");
+      a += v;
+    }
     tot[threadIdx.x] = a;
   }
   __syncthreads();
@@ -702,58 +742,65 @@ __device__ void grid_sums(const GridBarrier& bar, unsigned long long& bt, double
   __syncthreads();
 }
 
-__device__ void pressure_spmv(const LevelArgs& L, const double* pval, const double* x, double* y, int n) {
+__device__ __forceinline__ void pressure_spmv(const LevelSched& L, const double* pval, const double* x, double* y,
+                                              int n) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int r = tid; r < n; r += nth) {
     double s = 0.0;
-    for (int k = L.rp[r]; k < L.rp[r + 1]; ++k) s += pval[k] * x[L.col[k]];
+    for (int k = L.rp[r]; k < L.rp[r + 1]; ++k) s += pval[k] * __ldcg(x + L.col[k]);
     y[r] = s;
   }
 }
 
-// out = PressureILU(rhs): forward levels, backward levels, each level ended by a grid barrier
+// out = PressureILU(rhs): forward levels, backward levels, each level ended by a cluster barrier
 // (the last one also publishes `out` to the SpMV that follows).
-__device__ void pressure_ilu_apply(const BicgArgs& a, const double* rhs, double* out, unsigned long long& bt) {
-  const LevelArgs& L = a.L;
+__device__ void pressure_ilu_apply(const BicgArgs& a, const int* lp, const double* rhs, double* out) {
+  const LevelSched& L = a.L;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int l = 0; l < L.n_levels; ++l) {
-    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth)
       p_fwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, a.plu, rhs, a.y);
-    grid_sync(L.bar, bt, 300);
+    cluster_barrier();
   }
   for (int l = L.n_levels - 1; l >= 0; --l) {
-    for (int q = L.lvl_ptr[l] + tid; q < L.lvl_ptr[l + 1]; q += nth)
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth)
       p_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, a.plu, a.pdiag, a.y, out);
-    grid_sync(L.bar, bt, 301);
+    cluster_barrier();
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
+// The whole BiCGStab solve in one launch.  tol = max(|rhs|, EPS) * 1e-6 is formed from the first
+// reduction (r0 = rhs - A*0 = rhs), as the reference forms it from the right-hand side.
+__global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
   __shared__ double sh[32];
+  __shared__ double red[8];
+  __shared__ int s_ptr[kSmemLevels];
+  const int* lp = stage_levels(a.L, s_ptr);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const int n = a.n;
   double v3[3], o3[3];
   int parity = 0;
-  unsigned long long bt = 0;
-  // x = 0; r = rhs - A*0; r0 norm
+  v3[0] = 0.0;
   for (int i = tid; i < n; i += nth) {
+    const double ri = a.rhs[i] - 0.0;
     a.x[i] = 0.0;
-    a.r[i] = a.rhs[i] - 0.0;
-    a.rh[i] = a.r[i];
+    a.r[i] = ri;
+    a.rh[i] = ri;
     a.v[i] = 0.0;
     a.p[i] = 0.0;
+    v3[0] += ri * ri;
   }
-  v3[0] = 0.0;
-  for (int i = tid; i < n; i += nth) v3[0] += a.r[i] * a.r[i];
-  grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 400);
-  const int max_iters = sqrt(o3[0]) <= a.tol ? 0 : a.max_iters;
+  cluster_sums(red, parity, 1, v3, o3, sh);
+  const double rnorm0 = sqrt(o3[0]);
+  const double tol = fmax(rnorm0, kEps) * 1e-6;
+  const int max_iters = rnorm0 <= tol ? 0 : a.max_iters;
   double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
   int started = 0;
   for (int it = 0; it < max_iters; ++it) {
     started = it + 1;
     v3[0] = 0.0;
     for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.r[i];
-    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 401);
+    cluster_sums(red, parity, 1, v3, o3, sh);
     const double rho = o3[0];
     if (!isfinite(rho) || fabs(rho) < kEps) break;
     if (it == 0) {
@@ -762,13 +809,12 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
       const double beta = (rho / rho_prev) * (alpha / omega);
       for (int i = tid; i < n; i += nth) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
     }
-    grid_sync(a.L.bar, bt, 402);
-    pressure_ilu_apply(a, a.p, a.ph, bt);
+    cluster_barrier();
+    pressure_ilu_apply(a, lp, a.p, a.ph);
     pressure_spmv(a.L, a.pval, a.ph, a.v, n);
     v3[0] = 0.0;
-    grid_sync(a.L.bar, bt, 403);
     for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.v[i];
-    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 404);
+    cluster_sums(red, parity, 1, v3, o3, sh);
     const double vd = o3[0];
     if (!isfinite(vd) || fabs(vd) < kEps) break;
     alpha = rho / vd;
@@ -778,37 +824,39 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(BicgArgs a) {
       a.s[i] = si;
       v3[0] += si * si;
     }
-    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 405);
-    if (sqrt(o3[0]) <= a.tol) {
-      for (int i = tid; i < n; i += nth) a.x[i] += alpha * a.ph[i];
+    cluster_sums(red, parity, 1, v3, o3, sh);
+    if (sqrt(o3[0]) <= tol) {
+      for (int i = tid; i < n; i += nth) a.x[i] += alpha * __ldcg(a.ph + i);
       break;
     }
-    pressure_ilu_apply(a, a.s, a.sh, bt);
+    pressure_ilu_apply(a, lp, a.s, a.sh);
     pressure_spmv(a.L, a.pval, a.sh, a.t, n);
-    grid_sync(a.L.bar, bt, 406);
     v3[0] = 0.0;
     v3[1] = 0.0;
     for (int i = tid; i < n; i += nth) {
       v3[0] += a.t[i] * a.t[i];
       v3[1] += a.t[i] * a.s[i];
     }
-    grid_sums(a.L.bar, bt, a.partials, parity, 2, v3, o3, sh, 407);
+    cluster_sums(red, parity, 2, v3, o3, sh);
     const double tt = o3[0];
     if (!isfinite(tt) || tt <= kEps) break;
     omega = o3[1] / tt;
     if (!isfinite(omega) || fabs(omega) < kEps) break;
     v3[0] = 0.0;
     for (int i = tid; i < n; i += nth) {
-      a.x[i] += alpha * a.ph[i] + omega * a.sh[i];
+      a.x[i] += alpha * __ldcg(a.ph + i) + omega * __ldcg(a.sh + i);
       const double ri = a.s[i] - omega * a.t[i];
       a.r[i] = ri;
       v3[0] += ri * ri;
     }
-    grid_sums(a.L.bar, bt, a.partials, parity, 1, v3, o3, sh, 408);
-    if (sqrt(o3[0]) <= a.tol) break;
+    cluster_sums(red, parity, 1, v3, o3, sh);
+    if (sqrt(o3[0]) <= tol) break;
     rho_prev = rho;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && a.iter_counter) atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.iter_counter)
+    atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
+  // no CTA may leave while another can still read its shared partials
+  cluster_barrier();
 }
 
 // ============================================================================================
@@ -853,8 +901,7 @@ __global__ void k_dense_build(int nb, const int* __restrict__ rp, const int* __r
 // the back substitution applies the columns from the last one down.  ok[0] = 0 when a pivot is
 // exactly zero.  `a` is overwritten by the factors; `perm` holds n ints.
 __global__ void __launch_bounds__(1024) k_dense_invert(int n, double* a, double* inv, int* perm, int* ok) {
-  __shared__ int s_piv[32];
-  __shared__ double s_best[32];
+  __shared__ int s_piv[1];
   __shared__ int s_fail;
   const int t = threadIdx.x, nt = blockDim.x, lane = t & 31;
   for (int r = t; r < n; r += nt) perm[r] = r;
@@ -971,35 +1018,33 @@ static void spmv(Ctx& c, const double* x, double* y) {
   c.launches++;
 }
 
-// Arguments of one cooperative level-scheduled launch; the barrier counter is reset in stream order.
-static LevelArgs level_args(Ctx& c) {
-  LevelArgs L;
+static LevelSched level_sched(Ctx& c) {
+  LevelSched L;
   L.n_levels = c.levels.n_levels;
   L.lvl_rows = c.levels.d_rows;
   L.lvl_ptr = c.levels.d_ptr;
   L.rp = c.d_row_ptr.p;
   L.col = c.d_col.p;
   L.diag = c.d_diag.p;
-  L.bar.count = c.d_bar64;
-  L.bar.status = c.d_status.p;
-  RF_CUDA(cudaMemsetAsync(c.d_bar64, 0, sizeof(unsigned long long), c.stream));
   return L;
 }
 
-static void coop_launch(Ctx& c, const void* fn, int blocks, void** args) {
-  RF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kBlock), args, 0, c.stream));
+// one cluster of c.cluster_size CTAs
+static void cluster_launch(Ctx& c, const void* fn, int block, void** args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(c.cluster_size);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c.stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = c.cluster_size;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  RF_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
   c.launches++;
-}
-
-static void check_status(Ctx& c, const char* what) {
-  DeviceStatus st;
-  RF_CUDA(cudaMemcpyAsync(&st, c.d_status.p, sizeof(st), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
-  if (st.code != 0) {
-    char buf[160];
-    std::snprintf(buf, sizeof buf, "device status %d at site %d after %s", st.code, st.where, what);
-    throw CudaError(buf);
-  }
 }
 
 // CPR preconditioner build on the current reduced matrix
@@ -1010,7 +1055,7 @@ static void cpr_build(Ctx& c) {
                                                          c.d_bmask.p);
   k_pressure_matrix<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_val.p, c.d_cpr_w.p, c.d_pval.p);
   c.launches += 2;
-  LevelArgs L = level_args(c);
+  LevelSched L = level_sched(c);
   const double* val = c.d_val.p;
   const unsigned char* mask = c.d_bmask.p;
   double* lu = c.d_lu.p;
@@ -1019,7 +1064,7 @@ static void cpr_build(Ctx& c) {
   double* plu = c.d_plu.p;
   double* pdiag = c.d_pdiag.p;
   void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
-  coop_launch(c, (const void*)k_factor_coop, c.coop_blocks_sweep, args);
+  cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
   c.dense_ok = 0;
   if (n <= 299) {
     k_dense_build<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_col.p, c.d_pval.p, c.d_tmp2.p);
@@ -1045,13 +1090,8 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
     k_dense_matvec<<<blocks_for(n, 64), 64, 0, c.stream>>>(n, c.d_dense.p, prhs, corr);
     c.launches++;
   } else {
-    // tol = max(|prhs|, EPS) * 1e-6 (host reads the norm: the cooperative kernel takes it by value)
-    dot_dev(c, n, prhs, nullptr, c.d_scal.p + 20, true);
-    double nr = 0.0;
-    RF_CUDA(cudaMemcpyAsync(&nr, c.d_scal.p + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
     BicgArgs a;
-    a.L = level_args(c);
+    a.L = level_sched(c);
     a.n = n;
     a.pval = c.d_pval.p;
     a.plu = c.d_plu.p;
@@ -1068,13 +1108,11 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
     a.sh = base + 6 * size_t(n);
     a.t = base + 7 * size_t(n);
     a.y = base + 8 * size_t(n);
-    a.partials = c.d_partials.p;
-    a.tol = fmax(nr, kEps) * 1e-6;
     a.max_iters = 50;
     a.iter_counter = c.d_bicg_iters;
     void* args[] = {&a};
     PhaseScope pk(c, kPhBicgKernel);
-    coop_launch(c, (const void*)k_bicgstab_coop, c.coop_blocks_bicg, args);
+    cluster_launch(c, (const void*)k_bicgstab_cluster, kCBlock, args);
   }
   k_prolong<<<blocks_for(n), kBlock, 0, c.stream>>>(n, corr, z);
   c.launches++;
@@ -1084,13 +1122,13 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
   double* cr = c.d_tmp.p;
   double* ysw = c.d_tmp2.p;
   spmv_res(c, z, v, cr);
-  LevelArgs L = level_args(c);
+  LevelSched L = level_sched(c);
   const double* lu = c.d_lu.p;
   const double* dinv = c.d_dinv.p;
   const double* crp = cr;
   double* xo = c.d_w.p;
   void* args[] = {&L, (void*)&lu, (void*)&dinv, (void*)&crp, &ysw, &xo};
-  coop_launch(c, (const void*)k_block_sweep_coop, c.coop_blocks_sweep, args);
+  cluster_launch(c, (const void*)k_block_sweep_cluster, kCBlock, args);
   k_add_inplace<<<reduce_blocks(c, 3ll * n), kBlock, 0, c.stream>>>(3ll * n, c.d_w.p, z);
   c.launches++;
 }
@@ -1211,7 +1249,7 @@ LinResult linear_solve_reduced(Ctx& c) {
       break;
     }
   }
-  check_status(c, "FGMRES");
+  RF_CUDA(cudaGetLastError());
   return out;
 }
 
@@ -1375,22 +1413,38 @@ void setup_linear_workspace(Ctx& c) {
   c.d_pvec.alloc(12 * n);
   c.d_partials.alloc(4 * 4096);
   c.d_scal.alloc(8192);
-  c.d_status.alloc(1);
-  c.d_barrier.alloc(2);
   c.d_flag_dense.alloc(4);
-  RF_CUDA(cudaMalloc(&c.d_bar64, sizeof(unsigned long long)));
-  RF_CUDA(cudaMemset(c.d_bar64, 0, sizeof(unsigned long long)));
   RF_CUDA(cudaMalloc(&c.d_bicg_iters, sizeof(long long)));
   RF_CUDA(cudaMemset(c.d_bicg_iters, 0, sizeof(long long)));
-  RF_CUDA(cudaMemset(c.d_status.p, 0, sizeof(DeviceStatus)));
-  RF_CUDA(cudaMemset(c.d_barrier.p, 0, 2 * sizeof(unsigned int)));
-  int per_sm = 0;
-  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_coop, kBlock, 0));
-  c.coop_blocks_bicg = std::max(1, std::min(per_sm, 1) * c.num_sms);
-  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_block_sweep_coop, kBlock, 0));
-  int per_sm2 = 0;
-  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_factor_coop, kBlock, 0));
-  c.coop_blocks_sweep = std::max(1, std::min(std::min(per_sm, per_sm2), 1) * c.num_sms);
+  // the largest cluster (16 CTAs, non-portable; else 8) that every level-scheduled kernel can run
+  const void* fns[3] = {(const void*)k_factor_cluster, (const void*)k_block_sweep_cluster,
+                        (const void*)k_bicgstab_cluster};
+  const int blocks[3] = {kFBlock, kCBlock, kCBlock};
+  c.cluster_size = 0;
+  for (int cs : {16, 8, 4, 2, 1}) {
+    bool ok = true;
+    for (int f = 0; f < 3 && ok; ++f) {
+      if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(blocks[f]);
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cs;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, fns[f], &cfg) != cudaSuccess || nclusters < 1) ok = false;
+    }
+    cudaGetLastError();
+    if (ok) {
+      c.cluster_size = cs;
+      break;
+    }
+  }
+  if (c.cluster_size == 0) throw CudaError("no thread-block cluster shape fits the level-scheduled kernels");
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
   if (smem > 48 * 1024) RF_CUDA(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));

@@ -86,6 +86,43 @@ def waterflood_3d(nx: int, ny: int, nz: int, seed: int = 7, dx: float = 20.0, dz
     return d
 
 
+def ensemble_variant(index: int, seed: int = 1000, steps: int = 40, dt_days: float = 10.0) -> Deck:
+    """One variant of the sensitivity ensemble: nx, ny ~ U{20..64}, nz ~ U{5..16}, ln kh with
+    sigma ~ U[0.5, 1.5] (5-cell correlation), mobility ratio mu_o/mu_w ~ U[0.5, 10] (mu_w 0.5 cP),
+    Corey n_w, n_o ~ U[1.5, 4], kv/kh ~ U[0.01, 1]; quarter five-spot: a rate injector in the
+    (0, 0) column delivering 0.5 pore volumes over `steps` x `dt_days`, a 250-bar BHP producer in
+    the opposite column, every layer perforated.  Variant `index` draws from seed + index."""
+    rng = np.random.default_rng(seed + index)
+    nx, ny = (int(v) for v in rng.integers(20, 65, size=2))
+    nz = int(rng.integers(5, 17))
+    sigma = float(rng.uniform(0.5, 1.5))
+    mob = float(rng.uniform(0.5, 10.0))
+    n_w, n_o = (float(v) for v in rng.uniform(1.5, 4.0, size=2))
+    kv_kh = float(rng.uniform(0.01, 1.0))
+    d = Deck(nx, ny, nz, 0.2)
+    d.set_cell_dimensions(20.0, 20.0, 2.0)
+    kh, z = lognormal_field((nz, ny, nx), seed + index, math.log(100.0), sigma, 5.0)
+    d.set_permeability_field(kh, kh, kv_kh * kh)
+    d.set_porosity_field(np.clip(0.1 + 0.02 * z, 0.05, 0.3))
+    d.set_rel_perm_props(0.2, 0.2, n_w, n_o, 1.0, 1.0)
+    d.set_fluid_properties(0.5 * mob, 0.5)
+    d.set_fluid_compressibilities(1e-5, 1e-5)
+    d.set_rock_properties(0.0, 0.0, 1.0, 1.0)
+    d.set_capillary_params(0.0, 2.0)
+    d.set_gravity_enabled(False)
+    d.set_initial_pressure(300.0)
+    d.set_initial_saturation(0.2)
+    pv_total = float(np.sum(d.porosity) * 20.0 * 20.0 * 2.0)
+    d.set_well_control_modes("rate", "pressure")
+    d.set_target_well_rates(0.5 * pv_total / (steps * dt_days), 0.0)
+    d.set_well_bhp_limits(50.0, 600.0)
+    for k in range(nz):
+        d.add_well_with_id(0, 0, k, 500.0, 0.1, 0.0, True, "INJ")
+    for k in range(nz):
+        d.add_well_with_id(nx - 1, ny - 1, k, 250.0, 0.1, 0.0, False, "PROD")
+    return d
+
+
 def mixed_precision_deck(seed: int = 7) -> Deck:
     """The 2M-cell waterflood (200 x 200 x 50) of the mixed-precision configuration."""
     return waterflood_3d(200, 200, 50, seed=seed)

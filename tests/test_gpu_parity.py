@@ -1,7 +1,9 @@
 """Device FIM path vs the CPU oracle on the same seeded decks (GPU tests).
 
 Parity bar: pressure, water saturation, well BHP and well rates within 1e-6 relative after every
-report step, and Newton iteration counts within one per report step.
+report step, and Newton iteration counts within one per report step.  Where the reference's own
+rounding moves a run by more than that (pressure BiCGStab stopped at its iteration cap), the bar
+is three times the oracle-vs-oracle difference under a changed summation order, plus 1e-6.
 """
 import numpy as np
 import pytest
@@ -76,6 +78,43 @@ def test_waterflood_3d_bicgstab_parity():
     check_rows(rows, hg, hc)
 
 
+def test_waterflood_3d_mid_parity_at_rounding_floor():
+    """30 x 30 x 10 (9,000 cells): the pressure BiCGStab stops at its 50-iteration cap, so a
+    different summation order alone moves the Newton end state by more than 1e-6 in saturation.
+    The oracle run twice, with the reference's left-to-right dot products and with interleaved
+    partial sums, measures that rounding floor; the device path must stay within it (x3, plus
+    1e-6), with Newton counts within one."""
+    from oracle.oracle_py import lib
+
+    deck = decks.waterflood_3d(30, 30, 10, seed=7)
+    dt, steps = 10.0, 3
+    runs = {}
+    try:
+        for mode in (0, 1):
+            lib().orc_set_sum_order(mode)
+            o = OracleSimulator(deck)
+            runs[mode] = []
+            for _ in range(steps):
+                rc, r = o.step(dt)
+                assert rc == 0
+                st = o.state()
+                runs[mode].append((st["pressure"].copy(), st["sat_water"].copy(), r.newton_iterations))
+            o.close()
+    finally:
+        lib().orc_set_sum_order(0)
+    gpu = ReservoirSimulator.from_deck(deck)
+    for s in range(steps):
+        rg = gpu.step(dt)
+        gs = gpu.state()
+        p0, sw0, n0 = runs[0][s]
+        p1, sw1, _ = runs[1][s]
+        floor_p = rel_err(p1, p0)
+        floor_sw = rel_err(sw1, sw0)
+        assert rel_err(gs["pressure"], p0) <= 3 * floor_p + FIELD_RTOL, (s, rel_err(gs["pressure"], p0), floor_p)
+        assert rel_err(gs["sat_water"], sw0) <= 3 * floor_sw + FIELD_RTOL, (s, rel_err(gs["sat_water"], sw0), floor_sw)
+        assert abs(rg["newton_iterations"] - n0) <= 1, (s, rg["newton_iterations"], n0)
+
+
 def _csr_to_bsr(n_cells, ptr, col, val):
     """Tail-free 3x3 block CSR from a scalar CSR with 3 unknowns per cell."""
     blocks = {}
@@ -96,7 +135,8 @@ def _csr_to_bsr(n_cells, ptr, col, val):
     return np.array(rp), np.array(cols), np.concatenate(vals)
 
 
-@pytest.mark.parametrize("dims", [(10, 9, 3), (12, 10, 3)])  # dense coarse inverse | BiCGStab coarse
+# dense coarse inverse | BiCGStab coarse | BiCGStab over 38 levels
+@pytest.mark.parametrize("dims", [(10, 9, 3), (12, 10, 3), (24, 24, 8)])
 def test_linear_seam_matches_oracle(dims):
     deck = decks.waterflood_3d(*dims, seed=11, rate_per_perf=20.0)
     deck.wells = []  # tail-free system
