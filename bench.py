@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="72k")
     ap.add_argument("--dt", type=float, default=None)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="linear-solver precision of the device path (mixed: FP32 ILU and pressure stage)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="wall budget of the CPU baseline sample")
     return ap.parse_args()
@@ -149,6 +151,30 @@ class ClockSampler:
         }
 
 
+def max_over_ranks(value, dist=None, device="cpu"):
+    """The maximum of `value` over all ranks of the default process group (identity when `dist`
+    is None); every rank takes the same collective step."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def partition_by_cells(sizes, world):
+    """Greedy longest-first assignment of independent variants (cell counts `sizes`) to `world`
+    ranks; returns one index list per rank.  Deterministic for given inputs."""
+    loads = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda q: (loads[q], q))
+        parts[r].append(i)
+        loads[r] += sizes[i]
+    return parts
+
+
 def measured_hbm_peak():
     path = os.path.join(HERE, "MEASURED_PEAKS.json")
     try:
@@ -172,7 +198,8 @@ def cpu_leg(workload, dt, warmup, steps, budget_s):
     """The CPU restatement of the reference FIM (C++, one thread, like the reference) on the same
     deck and the same report steps as the GPU legs: `warmup` untimed report steps from the initial
     state, then up to `steps` timed ones (stopping once `budget_s` of wall time is spent, after at
-    least one).  Returns (cell-steps/s, timed steps, seconds, Newton iterations)."""
+    least one).  Returns (cell-steps/s, timed steps, seconds, Newton iterations, [(p, sw) after
+    each timed step])."""
     sys.path.insert(0, HERE)
     from oracle.oracle_py import OracleSimulator
 
@@ -185,16 +212,19 @@ def cpu_leg(workload, dt, warmup, steps, budget_s):
     k = 0
     newton = 0
     el = 0.0
+    states = []
     while k < steps:
         t0 = time.perf_counter()
         _, rep = sim.step(dt)
         el += time.perf_counter() - t0
         newton += rep.newton_iterations
+        st = sim.state()
+        states.append((st["pressure"], st["sat_water"]))
         k += 1
         if el >= budget_s:
             break
     sim.close()
-    return n * k / el, k, el, newton
+    return n * k / el, k, el, newton, states
 
 
 def run_reference(args):
@@ -207,7 +237,7 @@ def run_reference(args):
         return 0
     _, dt_default, desc = make_deck(args.workload)
     dt = args.dt if args.dt is not None else dt_default
-    v, k, el, newton = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
+    v, k, el, newton, _ = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
     n = WORKLOADS[args.workload][0] * WORKLOADS[args.workload][1] * WORKLOADS[args.workload][2]
     line = {
         "metric": "FIM cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
@@ -265,6 +295,7 @@ def main():
     sim = ReservoirSimulator.from_deck(deck)
     L = _lib.load()
     h = sim._context()
+    sim.set_linear_precision(args.precision)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def l2_flush():
@@ -287,10 +318,13 @@ def main():
     dev_ms = 0.0
     newton = lin = substeps = 0
     reps = []
+    gpu_states = []
     for _ in range(args.steps):
         r = sim.step(dt)
         reps.append(r)
         dev_ms += r["device_ms"]
+        st = sim.state()  # outside the device-timed region (rf_step's own events)
+        gpu_states.append((st["pressure"], st["sat_water"]))
         newton += r["newton_iterations"]
         lin += r["linear_iterations"]
         substeps += r["substeps"]
@@ -299,13 +333,9 @@ def main():
     clk = clocks.stop()
     launches = sim.kernel_launches() - launches0
     prof = sim.profile(enable=False, reset=True)
+    dev_ms_max = max_over_ranks(dev_ms, pg, "cuda")
     if pg:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms_max = float(t.item())
         pg.barrier()
-    else:
-        dev_ms_max = dev_ms
     value = world * n * args.steps / (dev_ms_max / 1e3)
 
     # ---- end-to-end leg: host buffers, copies inside the timed region ----
@@ -338,10 +368,7 @@ def main():
         e2e_s += time.perf_counter() - t0
         l2_flush()
     torch.cuda.synchronize()
-    if pg:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, pg, "cuda")
     e2e_value = world * n * args.steps / e2e_s
 
     # ---- roofline of the dominant kernel (BiCGStab pressure stage) ----
@@ -353,7 +380,7 @@ def main():
         bytes_launch = bicgstab_bytes_per_iteration(n, nnzb) * iters / launches_b
         ms_launch = kernel_ms / launches_b
         achieved = bytes_launch / (ms_launch / 1e3) / 1e9
-        roof = {"kernel": "k_bicgstab_coop", "bound": "hbm", "achieved": achieved, "peak": peak,
+        roof = {"kernel": "k_bicgstab_cluster", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                 "bytes_per_launch": bytes_launch, "ms_per_launch": ms_launch,
                 "iterations_per_launch": iters / launches_b,
@@ -362,10 +389,17 @@ def main():
 
     # ---- CPU baseline (rank 0, N = 1 only) ----
     cpu = None
+    field_err = None
     if cpu_job is not None:
         pool, job = cpu_job
         try:
-            v, k, el, cnewton = job.get(timeout=900)
+            v, k, el, cnewton, cpu_states = job.get(timeout=900)
+            ep = max(float(np.max(np.abs(g[0] - c[0]) / np.maximum(np.abs(c[0]), 1.0)))
+                     for g, c in zip(gpu_states, cpu_states))
+            es = max(float(np.max(np.abs(g[1] - c[1]))) for g, c in zip(gpu_states, cpu_states))
+            field_err = {"pressure_rel": ep, "sat_water_abs": es,
+                         "report_steps": [args.warmup + i for i in range(min(len(gpu_states), len(cpu_states)))],
+                         "against": "FP64 oracle (C++ restatement of the reference), same deck and steps"}
             cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                    "sample": f"report steps {args.warmup}..{args.warmup + k - 1} of the same deck after "
                              f"{args.warmup} untimed ones ({cnewton} Newton iterations, {el:.1f} s), C++ "
@@ -378,7 +412,8 @@ def main():
         line = {
             "metric": "FIM cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f64+f32",
             "data": "synthetic (seeded deck generator)",
             "config": {"workload": desc, "cells": n, "dt_days": dt, "parallelism": f"replicas{world}",
                        "l2": "flushed (256 MB write) between timed report steps",
@@ -386,7 +421,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 2 * 8 * n},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
-            "phase_ms": phases,
+            "phase_ms": phases, "precision": args.precision, "field_error_vs_oracle": field_err,
         }
         print(json.dumps(line), flush=True)
     del sim

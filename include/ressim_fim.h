@@ -28,7 +28,11 @@ extern "C" {
 #define RF_ERR_INVALID (-1)      /* invalid argument or deck */
 #define RF_ERR_UNSUPPORTED (-2)  /* deck uses a feature the device path does not implement */
 #define RF_ERR_CUDA (-3)         /* CUDA runtime error */
-#define RF_ERR_DEVICE_STATUS (-4)/* a device-side bounded wait or check reported failure */
+#define RF_ERR_DEVICE_STATUS (-4)/* a device-side check reported failure (reserved) */
+
+/* linear-solver precision modes (rf_set_linear_precision) */
+#define RF_PRECISION_FP64 0
+#define RF_PRECISION_MIXED 1
 
 /* One completion entry (src/lib/ressim/src/well.rs:64-90).  Entries that share a physical well
  * id (or, when none is given, the legacy fingerprint injector/i/j/bhp/radius/skin) form one
@@ -164,6 +168,21 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
                             const int32_t* block_cols, const double* block_vals,
                             const double* rhs, double* x, RfLinearReport* out);
 
+/* Precision of the CPR-FGMRES linear solver.  RF_PRECISION_FP64 (default) computes everything in
+ * FP64, as the reference does.  RF_PRECISION_MIXED keeps the block-ILU0 factors, the pressure
+ * matrix, its ILU0 factors and the pressure BiCGStab vectors in FP32 (dot products accumulate in
+ * FP64), under the FP64 FGMRES; residuals, the well Schur complement, Gram-Schmidt and the Newton
+ * update stay FP64.  No counterpart in the reference (an extension of the device path); takes
+ * effect at the next linear solve. */
+int32_t rf_set_linear_precision(RfCtx* ctx, int32_t mode);
+
+/* Tuning: CTAs (1..16, rounded down to a launchable power of two) in the thread-block cluster that
+ * runs the level-scheduled ILU factorisation, ILU sweeps and pressure BiCGStab; 0 restores the
+ * automatic choice (enough 1024-thread CTAs for the widest level).  Returns the size in use (> 0)
+ * or an error.  The size fixes the reduction order, so results are deterministic for a given size
+ * and differ between sizes only by rounding.  No counterpart in the reference. */
+int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas);
+
 /* Number of kernel launches this context has issued since creation (device work counter). */
 int64_t rf_kernel_launches(const RfCtx* ctx);
 
@@ -175,6 +194,19 @@ int64_t rf_kernel_launches(const RfCtx* ctx);
  * launches timed, and the block count of the reduced matrix.
  * enable > 0 switches the profiler on, 0 off, < 0 leaves it as is; reset != 0 zeroes the totals. */
 int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n);
+
+/* ---- Ensemble batch (sensitivity variants of uneven sizes); no counterpart in the reference, whose
+ * simulator object steps one deck.  Each variant gets its own context (the rf_* calls above work on
+ * rf_batch_context(b, i)); rf_batch_step advances every variant by one report step, driving the
+ * variants from `host_threads` host threads (<= 0: one per hardware thread, at most n) so their
+ * kernels run concurrently on the device from separate streams.  Returns the first negative
+ * status of any variant, else the largest positive one; per-variant reports go to reports[n]. */
+typedef struct RfBatch RfBatch;
+int32_t rf_batch_create(const RfDeck* const* decks, int32_t n, int32_t host_threads, RfBatch** out);
+int32_t rf_batch_destroy(RfBatch* batch);
+int32_t rf_batch_size(const RfBatch* batch);
+RfCtx* rf_batch_context(RfBatch* batch, int32_t index);
+int32_t rf_batch_step(RfBatch* batch, double target_dt_days, RfStepReport* reports);
 
 #ifdef __cplusplus
 }

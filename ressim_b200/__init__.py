@@ -6,3 +6,4 @@ checks) run as CUDA kernels for sm_100a behind the C ABI declared in include/res
 """
 from .deck import Deck, Well  # noqa: F401
 from .simulator import ReservoirSimulator, linear_solve_bsr  # noqa: F401
+from .ensemble import Ensemble  # noqa: F401

@@ -11,6 +11,8 @@ RF_ERR_INVALID = -1
 RF_ERR_UNSUPPORTED = -2
 RF_ERR_CUDA = -3
 RF_ERR_DEVICE_STATUS = -4
+RF_PRECISION_FP64 = 0
+RF_PRECISION_MIXED = 1
 
 _dp = C.POINTER(C.c_double)
 

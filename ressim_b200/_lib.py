@@ -37,6 +37,14 @@ def load():
     L.rf_kernel_launches.argtypes = [C.c_void_p]
     L.rf_kernel_launches.restype = C.c_int64
     L.rf_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32]
+    L.rf_set_linear_precision.argtypes = [C.c_void_p, C.c_int32]
+    L.rf_set_cluster_size.argtypes = [C.c_void_p, C.c_int32]
+    L.rf_batch_create.argtypes = [C.POINTER(C.POINTER(_abi.RfDeck)), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.rf_batch_destroy.argtypes = [C.c_void_p]
+    L.rf_batch_size.argtypes = [C.c_void_p]
+    L.rf_batch_context.argtypes = [C.c_void_p, C.c_int32]
+    L.rf_batch_context.restype = C.c_void_p
+    L.rf_batch_step.argtypes = [C.c_void_p, C.c_double, C.POINTER(_abi.RfStepReport)]
     _lib = L
     return L
 
@@ -50,7 +58,8 @@ def last_error(handle) -> str:
 EXPORTED_SYMBOLS = (
     "rf_create", "rf_destroy", "rf_last_error", "rf_set_state", "rf_get_state", "rf_get_well_bhp",
     "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_kernel_launches",
-    "rf_profile",
+    "rf_profile", "rf_set_linear_precision", "rf_set_cluster_size", "rf_batch_create", "rf_batch_destroy", "rf_batch_size",
+    "rf_batch_context", "rf_batch_step",
 )
 
 PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",

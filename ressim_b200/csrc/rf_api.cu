@@ -18,7 +18,9 @@
 #include <limits>
 #include <map>
 #include <memory>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <tuple>
 
 #include "rf_ops.hpp"
@@ -879,6 +881,8 @@ static void free_ctx(Ctx& c) {
                   &c.d_perf_well, &c.d_perf_inj, &c.d_perf_has_wi, &c.d_well_ptr, &c.d_well_perfs, &c.d_tinv_off,
                   &c.d_perf_row_off, &c.d_flag_dense, &c.d_dense_perm})
     b->free();
+  for (auto* b : {&c.d_lu32, &c.d_dinv32, &c.d_plu32, &c.d_pval32, &c.d_pdiag32, &c.d_pvec32, &c.d_sweep32})
+    b->free();
   c.d_bmask.free();
   c.d_ctrl.free();
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
@@ -1064,6 +1068,29 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
 
 int64_t rf_kernel_launches(const RfCtx* ctx) { return ctx ? ctx->c.launches : 0; }
 
+int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas) {
+  if (!ctx || ctas < 0 || ctas > 16) return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t {
+    if (ctas == 0) {
+      int widest = 1;
+      const auto& hp = ctx->c.levels.h_ptr;
+      for (size_t l = 0; l + 1 < hp.size(); ++l) widest = std::max(widest, hp[l + 1] - hp[l]);
+      int want = 1;
+      while (want < 16 && want * 1024 < widest) want *= 2;
+      return rf::set_cluster_size(ctx->c, want);
+    }
+    return rf::set_cluster_size(ctx->c, ctas);
+  });
+}
+
+int32_t rf_set_linear_precision(RfCtx* ctx, int32_t mode) {
+  if (!ctx || (mode != RF_PRECISION_FP64 && mode != RF_PRECISION_MIXED)) return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t {
+    rf::set_linear_precision(ctx->c, mode);
+    return RF_OK;
+  });
+}
+
 int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n) {
   if (!ctx) return RF_ERR_INVALID;
   return guarded(ctx, [&]() -> int32_t {
@@ -1089,6 +1116,87 @@ int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32
     }
     return RF_OK;
   });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ensemble batch: independent decks stepped concurrently.  Every variant keeps its own context
+// (device buffers, CUDA stream, one-cluster level-scheduled launches), and a pool of host threads
+// drives the variants' controllers, largest first, so the device runs many variants' kernels at
+// once from separate streams.  The variants never exchange data.
+// ---------------------------------------------------------------------------------------------
+struct RfBatch {
+  std::vector<RfCtx*> ctx;
+  std::vector<int> order;  // variant indices by descending cell count
+  int threads = 1;
+  int device = 0;
+};
+
+int32_t rf_batch_create(const RfDeck* const* decks, int32_t n, int32_t host_threads, RfBatch** out) {
+  if (!out || !decks || n <= 0) return RF_ERR_INVALID;
+  *out = nullptr;
+  auto* b = new RfBatch();
+  cudaGetDevice(&b->device);
+  for (int32_t i = 0; i < n; ++i) {
+    RfCtx* c = nullptr;
+    const int32_t rc = rf_create(decks[i], &c);
+    if (rc != RF_OK) {
+      {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_last_create_error = "variant " + std::to_string(i) + ": " + g_last_create_error;
+      }
+      for (RfCtx* x : b->ctx) rf_destroy(x);
+      delete b;
+      return rc;
+    }
+    b->ctx.push_back(c);
+  }
+  b->order.resize(n);
+  for (int32_t i = 0; i < n; ++i) b->order[i] = i;
+  std::stable_sort(b->order.begin(), b->order.end(),
+                   [&](int x, int y) { return b->ctx[x]->c.n > b->ctx[y]->c.n; });
+  const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
+  b->threads = host_threads > 0 ? host_threads : std::min<int>(n, hw);
+  *out = b;
+  return RF_OK;
+}
+
+int32_t rf_batch_destroy(RfBatch* b) {
+  if (!b) return RF_OK;
+  for (RfCtx* c : b->ctx) rf_destroy(c);
+  delete b;
+  return RF_OK;
+}
+
+int32_t rf_batch_size(const RfBatch* b) { return b ? int32_t(b->ctx.size()) : 0; }
+
+RfCtx* rf_batch_context(RfBatch* b, int32_t i) {
+  if (!b || i < 0 || i >= int32_t(b->ctx.size())) return nullptr;
+  return b->ctx[i];
+}
+
+int32_t rf_batch_step(RfBatch* b, double target_dt_days, RfStepReport* reports) {
+  if (!b || !reports || !(target_dt_days > 0.0) || !std::isfinite(target_dt_days)) return RF_ERR_INVALID;
+  const int n = int(b->ctx.size());
+  std::vector<int32_t> rcs(n, RF_OK);
+  std::atomic<int> next{0};
+  auto work = [&]() {
+    cudaSetDevice(b->device);
+    for (int k = next.fetch_add(1); k < n; k = next.fetch_add(1)) {
+      const int i = b->order[k];
+      rcs[i] = rf_step(b->ctx[i], target_dt_days, &reports[i]);
+    }
+  };
+  std::vector<std::thread> pool;
+  const int extra = std::min(b->threads, n) - 1;
+  for (int t = 0; t < extra; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  int32_t worst = RF_OK;
+  for (int i = 0; i < n; ++i) {
+    if (rcs[i] < 0) return rcs[i];
+    if (rcs[i] > worst) worst = rcs[i];
+  }
+  return worst;
 }
 
 }  // extern "C"

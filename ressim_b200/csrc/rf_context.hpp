@@ -124,6 +124,9 @@ struct Ctx {
   DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
   DBuf<double> d_partials, d_scal;
   int cluster_size = 0;  // CTAs in the one cluster that runs the level-scheduled kernels
+  // linear-solver precision: 0 FP64; 1 mixed (FP32 block-ILU0 and pressure stage under FP64 FGMRES)
+  int precision = 0;
+  DBuf<float> d_lu32, d_dinv32, d_plu32, d_pval32, d_pdiag32, d_pvec32, d_sweep32;
   DBuf<int> d_flag_dense;
 
   // timing

@@ -617,14 +617,19 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(LevelSched L, con
 // ============================================================================================
 // ILU sweeps
 // ============================================================================================
+// Storage type T of factors and work vectors: double for the FP64 path, float for the mixed form
+// (FP32 block-ILU0 and pressure stage under the FP64 FGMRES).  Inputs and outputs at the FGMRES
+// boundary stay double; row sums run in T.
+//
 // block: y_i = r_i - sum L_ik y_k (forward); x_i = Dinv_i (y_i - sum U_ij x_j) (backward)
-__device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* col, const int* diag,
-                                              const double* lu, const double* r, double* y) {
-  double b0 = __ldcg(r + 3 * i), b1 = __ldcg(r + 3 * i + 1), b2 = __ldcg(r + 3 * i + 2);
+template <class T>
+__device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* col, const int* diag, const T* lu,
+                                              const double* r, T* y) {
+  T b0 = T(__ldcg(r + 3 * i)), b1 = T(__ldcg(r + 3 * i + 1)), b2 = T(__ldcg(r + 3 * i + 2));
   for (int k = rp[i]; k < diag[i]; ++k) {
-    const double* Lb = lu + size_t(k) * 9;
+    const T* Lb = lu + size_t(k) * 9;
     const int j = col[k];
-    const double y0 = __ldcg(y + 3 * j), y1 = __ldcg(y + 3 * j + 1), y2 = __ldcg(y + 3 * j + 2);
+    const T y0 = __ldcg(y + 3 * j), y1 = __ldcg(y + 3 * j + 1), y2 = __ldcg(y + 3 * j + 2);
     b0 -= Lb[0] * y0 + Lb[1] * y1 + Lb[2] * y2;
     b1 -= Lb[3] * y0 + Lb[4] * y1 + Lb[5] * y2;
     b2 -= Lb[6] * y0 + Lb[7] * y1 + Lb[8] * y2;
@@ -633,27 +638,38 @@ __device__ __forceinline__ void block_fwd_row(int i, const int* rp, const int* c
   y[3 * i + 1] = b1;
   y[3 * i + 2] = b2;
 }
-__device__ __forceinline__ void block_bwd_row(int i, const int* rp, const int* col, const int* diag,
-                                              const double* lu, const double* dinv, const double* y, double* x) {
-  double b0 = __ldcg(y + 3 * i), b1 = __ldcg(y + 3 * i + 1), b2 = __ldcg(y + 3 * i + 2);
+template <class T>
+__device__ __forceinline__ void block_bwd_row(int i, const int* rp, const int* col, const int* diag, const T* lu,
+                                              const T* dinv, const T* y, T* xt, double* x) {
+  T b0 = __ldcg(y + 3 * i), b1 = __ldcg(y + 3 * i + 1), b2 = __ldcg(y + 3 * i + 2);
   for (int k = diag[i] + 1; k < rp[i + 1]; ++k) {
-    const double* U = lu + size_t(k) * 9;
+    const T* U = lu + size_t(k) * 9;
     const int j = col[k];
-    const double x0 = __ldcg(x + 3 * j), x1 = __ldcg(x + 3 * j + 1), x2 = __ldcg(x + 3 * j + 2);
+    const T x0 = __ldcg(xt + 3 * j), x1 = __ldcg(xt + 3 * j + 1), x2 = __ldcg(xt + 3 * j + 2);
     b0 -= U[0] * x0 + U[1] * x1 + U[2] * x2;
     b1 -= U[3] * x0 + U[4] * x1 + U[5] * x2;
     b2 -= U[6] * x0 + U[7] * x1 + U[8] * x2;
   }
-  const double* D = dinv + size_t(i) * 9;
-  x[3 * i] = D[0] * b0 + D[1] * b1 + D[2] * b2;
-  x[3 * i + 1] = D[3] * b0 + D[4] * b1 + D[5] * b2;
-  x[3 * i + 2] = D[6] * b0 + D[7] * b1 + D[8] * b2;
+  const T* D = dinv + size_t(i) * 9;
+  const T o0 = D[0] * b0 + D[1] * b1 + D[2] * b2;
+  const T o1 = D[3] * b0 + D[4] * b1 + D[5] * b2;
+  const T o2 = D[6] * b0 + D[7] * b1 + D[8] * b2;
+  xt[3 * i] = o0;
+  xt[3 * i + 1] = o1;
+  xt[3 * i + 2] = o2;
+  if (x != nullptr && (const void*)x != (const void*)xt) {
+    x[3 * i] = double(o0);
+    x[3 * i + 1] = double(o1);
+    x[3 * i + 2] = double(o2);
+  }
 }
 
-// x = BlockILU(cr)   [one cluster: forward levels, then backward levels]
-__global__ void __launch_bounds__(kCBlock, 1) k_block_sweep_cluster(LevelSched L, const double* __restrict__ lu,
-                                                                     const double* __restrict__ dinv,
-                                                                     const double* __restrict__ cr, double* y,
+// x = BlockILU(cr)   [one cluster: forward levels, then backward levels].  For T = double the
+// backward sweep works in x itself (xt == x); for T = float it works in xt and writes x too.
+template <class T>
+__global__ void __launch_bounds__(kCBlock, 1) k_block_sweep_cluster(LevelSched L, const T* __restrict__ lu,
+                                                                     const T* __restrict__ dinv,
+                                                                     const double* __restrict__ cr, T* y, T* xt,
                                                                      double* x) {
   __shared__ int s_ptr[kSmemLevels];
   const int* lp = stage_levels(L, s_ptr);
@@ -664,46 +680,49 @@ __global__ void __launch_bounds__(kCBlock, 1) k_block_sweep_cluster(LevelSched L
   }
   for (int l = L.n_levels - 1; l >= 0; --l) {
     for (int q = lp[l] + tid; q < lp[l + 1]; q += nth)
-      block_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, dinv, y, x);
+      block_bwd_row(L.lvl_rows[q], L.rp, L.col, L.diag, lu, dinv, y, xt, x);
     if (l > 0) cluster_barrier();
   }
 }
 
 // scalar pressure ILU rows
-__device__ __forceinline__ void p_fwd_row(int r, const int* rp, const int* col, const int* diag, const double* plu,
-                                          const double* rhs, double* y) {
-  double s = __ldcg(rhs + r);
+template <class T>
+__device__ __forceinline__ void p_fwd_row(int r, const int* rp, const int* col, const int* diag, const T* plu,
+                                          const T* rhs, T* y) {
+  T s = __ldcg(rhs + r);
   for (int k = rp[r]; k < diag[r]; ++k) s -= plu[k] * __ldcg(y + col[k]);
   y[r] = s;
 }
-__device__ __forceinline__ void p_bwd_row(int r, const int* rp, const int* col, const int* diag, const double* plu,
-                                          const double* pdiag, const double* y, double* x) {
-  double s = __ldcg(y + r);
+template <class T>
+__device__ __forceinline__ void p_bwd_row(int r, const int* rp, const int* col, const int* diag, const T* plu,
+                                          const T* pdiag, const T* y, T* x) {
+  T s = __ldcg(y + r);
   for (int k = diag[r] + 1; k < rp[r + 1]; ++k) s -= plu[k] * __ldcg(x + col[k]);
-  const double d = pdiag[r];
-  x[r] = fabs(d) > kEps ? s / d : s;
+  const T d = pdiag[r];
+  x[r] = fabs(double(d)) > kEps ? s / d : s;
 }
 
 // ============================================================================================
 // BiCGStab on the pressure system (solve_pressure_with_bicgstab), one cluster
 // ============================================================================================
+template <class T>
 struct BicgArgs {
   LevelSched L;
   int n;
-  const double* pval;
-  const double* plu;
-  const double* pdiag;
+  const T* pval;
+  const T* plu;
+  const T* pdiag;
   const double* rhs;
   double* x;
-  double* r;
-  double* rh;
-  double* p;
-  double* v;
-  double* ph;
-  double* s;
-  double* sh;
-  double* t;
-  double* y;
+  T* r;
+  T* rh;
+  T* p;
+  T* v;
+  T* ph;
+  T* s;
+  T* sh;
+  T* t;
+  T* y;
   int max_iters;
   long long* iter_counter;  // incremented by the iterations this solve ran
 };
@@ -742,11 +761,11 @@ __device__ void cluster_sums(double* red /* shared [2][4] */, int& parity, int n
   __syncthreads();
 }
 
-__device__ __forceinline__ void pressure_spmv(const LevelSched& L, const double* pval, const double* x, double* y,
-                                              int n) {
+template <class T>
+__device__ __forceinline__ void pressure_spmv(const LevelSched& L, const T* pval, const T* x, T* y, int n) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int r = tid; r < n; r += nth) {
-    double s = 0.0;
+    T s = T(0);
     for (int k = L.rp[r]; k < L.rp[r + 1]; ++k) s += pval[k] * __ldcg(x + L.col[k]);
     y[r] = s;
   }
@@ -754,7 +773,8 @@ __device__ __forceinline__ void pressure_spmv(const LevelSched& L, const double*
 
 // out = PressureILU(rhs): forward levels, backward levels, each level ended by a cluster barrier
 // (the last one also publishes `out` to the SpMV that follows).
-__device__ void pressure_ilu_apply(const BicgArgs& a, const int* lp, const double* rhs, double* out) {
+template <class T>
+__device__ void pressure_ilu_apply(const BicgArgs<T>& a, const int* lp, const T* rhs, T* out) {
   const LevelSched& L = a.L;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int l = 0; l < L.n_levels; ++l) {
@@ -770,8 +790,10 @@ __device__ void pressure_ilu_apply(const BicgArgs& a, const int* lp, const doubl
 }
 
 // The whole BiCGStab solve in one launch.  tol = max(|rhs|, EPS) * 1e-6 is formed from the first
-// reduction (r0 = rhs - A*0 = rhs), as the reference forms it from the right-hand side.
-__global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
+// reduction (r0 = rhs - A*0 = rhs), as the reference forms it from the right-hand side.  Dot
+// products accumulate in double and the iterate x is kept in double for either storage type.
+template <class T>
+__global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs<T> a) {
   __shared__ double sh[32];
   __shared__ double red[8];
   __shared__ int s_ptr[kSmemLevels];
@@ -783,12 +805,13 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
   v3[0] = 0.0;
   for (int i = tid; i < n; i += nth) {
     const double ri = a.rhs[i] - 0.0;
+    const T rt = T(ri);
     a.x[i] = 0.0;
-    a.r[i] = ri;
-    a.rh[i] = ri;
-    a.v[i] = 0.0;
-    a.p[i] = 0.0;
-    v3[0] += ri * ri;
+    a.r[i] = rt;
+    a.rh[i] = rt;
+    a.v[i] = T(0);
+    a.p[i] = T(0);
+    v3[0] += double(rt) * double(rt);
   }
   cluster_sums(red, parity, 1, v3, o3, sh);
   const double rnorm0 = sqrt(o3[0]);
@@ -799,7 +822,7 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
   for (int it = 0; it < max_iters; ++it) {
     started = it + 1;
     v3[0] = 0.0;
-    for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.r[i];
+    for (int i = tid; i < n; i += nth) v3[0] += double(a.rh[i]) * double(a.r[i]);
     cluster_sums(red, parity, 1, v3, o3, sh);
     const double rho = o3[0];
     if (!isfinite(rho) || fabs(rho) < kEps) break;
@@ -807,26 +830,27 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
       for (int i = tid; i < n; i += nth) a.p[i] = a.r[i];
     } else {
       const double beta = (rho / rho_prev) * (alpha / omega);
-      for (int i = tid; i < n; i += nth) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+      for (int i = tid; i < n; i += nth)
+        a.p[i] = T(double(a.r[i]) + beta * (double(a.p[i]) - omega * double(a.v[i])));
     }
     cluster_barrier();
     pressure_ilu_apply(a, lp, a.p, a.ph);
     pressure_spmv(a.L, a.pval, a.ph, a.v, n);
     v3[0] = 0.0;
-    for (int i = tid; i < n; i += nth) v3[0] += a.rh[i] * a.v[i];
+    for (int i = tid; i < n; i += nth) v3[0] += double(a.rh[i]) * double(a.v[i]);
     cluster_sums(red, parity, 1, v3, o3, sh);
     const double vd = o3[0];
     if (!isfinite(vd) || fabs(vd) < kEps) break;
     alpha = rho / vd;
     v3[0] = 0.0;
     for (int i = tid; i < n; i += nth) {
-      const double si = a.r[i] - alpha * a.v[i];
+      const T si = T(double(a.r[i]) - alpha * double(a.v[i]));
       a.s[i] = si;
-      v3[0] += si * si;
+      v3[0] += double(si) * double(si);
     }
     cluster_sums(red, parity, 1, v3, o3, sh);
     if (sqrt(o3[0]) <= tol) {
-      for (int i = tid; i < n; i += nth) a.x[i] += alpha * __ldcg(a.ph + i);
+      for (int i = tid; i < n; i += nth) a.x[i] += alpha * double(__ldcg(a.ph + i));
       break;
     }
     pressure_ilu_apply(a, lp, a.s, a.sh);
@@ -834,8 +858,9 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
     v3[0] = 0.0;
     v3[1] = 0.0;
     for (int i = tid; i < n; i += nth) {
-      v3[0] += a.t[i] * a.t[i];
-      v3[1] += a.t[i] * a.s[i];
+      const double ti = double(a.t[i]);
+      v3[0] += ti * ti;
+      v3[1] += ti * double(a.s[i]);
     }
     cluster_sums(red, parity, 2, v3, o3, sh);
     const double tt = o3[0];
@@ -844,10 +869,10 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
     if (!isfinite(omega) || fabs(omega) < kEps) break;
     v3[0] = 0.0;
     for (int i = tid; i < n; i += nth) {
-      a.x[i] += alpha * __ldcg(a.ph + i) + omega * __ldcg(a.sh + i);
-      const double ri = a.s[i] - omega * a.t[i];
+      a.x[i] += alpha * double(__ldcg(a.ph + i)) + omega * double(__ldcg(a.sh + i));
+      const T ri = T(double(a.s[i]) - omega * double(a.t[i]));
       a.r[i] = ri;
-      v3[0] += ri * ri;
+      v3[0] += double(ri) * double(ri);
     }
     cluster_sums(red, parity, 1, v3, o3, sh);
     if (sqrt(o3[0]) <= tol) break;
@@ -857,6 +882,24 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs a) {
     atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
   // no CTA may leave while another can still read its shared partials
   cluster_barrier();
+}
+
+// FP32 copies of the factors and the pressure matrix for the mixed form (one pass over each).
+__global__ void k_factors_to_f32(long long n_lu, const double* __restrict__ lu, float* __restrict__ lu32,
+                                 long long n_dinv, const double* __restrict__ dinv, float* __restrict__ dinv32,
+                                 long long nnzb, const double* __restrict__ plu, float* __restrict__ plu32,
+                                 const double* __restrict__ pval, float* __restrict__ pval32, long long nb,
+                                 const double* __restrict__ pdiag, float* __restrict__ pdiag32) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_lu; i += stride) lu32[i] = float(lu[i]);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_dinv; i += stride)
+    dinv32[i] = float(dinv[i]);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nnzb; i += stride) {
+    plu32[i] = float(plu[i]);
+    pval32[i] = float(pval[i]);
+  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nb; i += stride)
+    pdiag32[i] = float(pdiag[i]);
 }
 
 // ============================================================================================
@@ -1065,6 +1108,12 @@ static void cpr_build(Ctx& c) {
   double* pdiag = c.d_pdiag.p;
   void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
   cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
+  if (c.precision == 1) {
+    k_factors_to_f32<<<4 * c.num_sms, kBlock, 0, c.stream>>>(
+        9ll * c.nnzb, c.d_lu.p, c.d_lu32.p, 9ll * n, c.d_dinv.p, c.d_dinv32.p, c.nnzb, c.d_plu.p, c.d_plu32.p,
+        c.d_pval.p, c.d_pval32.p, n, c.d_pdiag.p, c.d_pdiag32.p);
+    c.launches++;
+  }
   c.dense_ok = 0;
   if (n <= 299) {
     k_dense_build<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_col.p, c.d_pval.p, c.d_tmp2.p);
@@ -1075,6 +1124,33 @@ static void cpr_build(Ctx& c) {
     RF_CUDA(cudaStreamSynchronize(c.stream));
     c.dense_ok = ok;
   }
+}
+
+template <class T>
+static void launch_bicgstab(Ctx& c, const T* pval, const T* plu, const T* pdiag, const double* rhs, double* x,
+                            T* base) {
+  const size_t n = c.n;
+  BicgArgs<T> a;
+  a.L = level_sched(c);
+  a.n = c.n;
+  a.pval = pval;
+  a.plu = plu;
+  a.pdiag = pdiag;
+  a.rhs = rhs;
+  a.x = x;
+  a.r = base;
+  a.rh = base + n;
+  a.p = base + 2 * n;
+  a.v = base + 3 * n;
+  a.ph = base + 4 * n;
+  a.s = base + 5 * n;
+  a.sh = base + 6 * n;
+  a.t = base + 7 * n;
+  a.y = base + 8 * n;
+  a.max_iters = 50;
+  a.iter_counter = c.d_bicg_iters;
+  void* args[] = {&a};
+  cluster_launch(c, (const void*)k_bicgstab_cluster<T>, kCBlock, args);
 }
 
 // z = CPR(v)
@@ -1090,29 +1166,11 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
     k_dense_matvec<<<blocks_for(n, 64), 64, 0, c.stream>>>(n, c.d_dense.p, prhs, corr);
     c.launches++;
   } else {
-    BicgArgs a;
-    a.L = level_sched(c);
-    a.n = n;
-    a.pval = c.d_pval.p;
-    a.plu = c.d_plu.p;
-    a.pdiag = c.d_pdiag.p;
-    a.rhs = prhs;
-    a.x = corr;
-    double* base = c.d_pvec.p;
-    a.r = base;
-    a.rh = base + n;
-    a.p = base + 2 * size_t(n);
-    a.v = base + 3 * size_t(n);
-    a.ph = base + 4 * size_t(n);
-    a.s = base + 5 * size_t(n);
-    a.sh = base + 6 * size_t(n);
-    a.t = base + 7 * size_t(n);
-    a.y = base + 8 * size_t(n);
-    a.max_iters = 50;
-    a.iter_counter = c.d_bicg_iters;
-    void* args[] = {&a};
     PhaseScope pk(c, kPhBicgKernel);
-    cluster_launch(c, (const void*)k_bicgstab_cluster, kCBlock, args);
+    if (c.precision == 1)
+      launch_bicgstab<float>(c, c.d_pval32.p, c.d_plu32.p, c.d_pdiag32.p, prhs, corr, c.d_pvec32.p);
+    else
+      launch_bicgstab<double>(c, c.d_pval.p, c.d_plu.p, c.d_pdiag.p, prhs, corr, c.d_pvec.p);
   }
   k_prolong<<<blocks_for(n), kBlock, 0, c.stream>>>(n, corr, z);
   c.launches++;
@@ -1123,12 +1181,21 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
   double* ysw = c.d_tmp2.p;
   spmv_res(c, z, v, cr);
   LevelSched L = level_sched(c);
-  const double* lu = c.d_lu.p;
-  const double* dinv = c.d_dinv.p;
   const double* crp = cr;
   double* xo = c.d_w.p;
-  void* args[] = {&L, (void*)&lu, (void*)&dinv, (void*)&crp, &ysw, &xo};
-  cluster_launch(c, (const void*)k_block_sweep_cluster, kCBlock, args);
+  if (c.precision == 1) {
+    const float* lu = c.d_lu32.p;
+    const float* dinv = c.d_dinv32.p;
+    float* y32 = c.d_sweep32.p;
+    float* x32 = c.d_sweep32.p + 3 * size_t(n);
+    void* args[] = {&L, (void*)&lu, (void*)&dinv, (void*)&crp, &y32, &x32, &xo};
+    cluster_launch(c, (const void*)k_block_sweep_cluster<float>, kCBlock, args);
+  } else {
+    const double* lu = c.d_lu.p;
+    const double* dinv = c.d_dinv.p;
+    void* args[] = {&L, (void*)&lu, (void*)&dinv, (void*)&crp, &ysw, &xo, &xo};
+    cluster_launch(c, (const void*)k_block_sweep_cluster<double>, kCBlock, args);
+  }
   k_add_inplace<<<reduce_blocks(c, 3ll * n), kBlock, 0, c.stream>>>(3ll * n, c.d_w.p, z);
   c.launches++;
 }
@@ -1387,6 +1454,55 @@ void build_levels(Ctx& c) {
                      cudaMemcpyHostToDevice));
 }
 
+// The largest cluster size <= `want` (a power of two, 1..16) that every level-scheduled kernel
+// can launch with (16 needs the non-portable cluster attribute).
+int set_cluster_size(Ctx& c, int want) {
+  const void* fns[5] = {(const void*)k_factor_cluster, (const void*)k_block_sweep_cluster<double>,
+                        (const void*)k_bicgstab_cluster<double>, (const void*)k_block_sweep_cluster<float>,
+                        (const void*)k_bicgstab_cluster<float>};
+  const int blocks[5] = {kFBlock, kCBlock, kCBlock, kCBlock, kCBlock};
+  for (int cs = 16; cs >= 1; cs /= 2) {
+    if (cs > want) continue;
+    bool ok = true;
+    for (int f = 0; f < 5 && ok; ++f) {
+      if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(blocks[f]);
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cs;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, fns[f], &cfg) != cudaSuccess || nclusters < 1) ok = false;
+    }
+    cudaGetLastError();
+    if (ok) {
+      c.cluster_size = cs;
+      return cs;
+    }
+  }
+  throw CudaError("no thread-block cluster shape fits the level-scheduled kernels");
+}
+
+// FP32 factors and work vectors of the mixed form, allocated on first use.
+void set_linear_precision(Ctx& c, int mode) {
+  if (mode == 1 && c.d_lu32.p == nullptr) {
+    const size_t n = c.n;
+    c.d_lu32.alloc(size_t(c.nnzb) * 9);
+    c.d_dinv32.alloc(n * 9);
+    c.d_plu32.alloc(c.nnzb);
+    c.d_pval32.alloc(c.nnzb);
+    c.d_pdiag32.alloc(n);
+    c.d_pvec32.alloc(10 * n);
+    c.d_sweep32.alloc(6 * n);
+  }
+  c.precision = mode;
+}
+
 void setup_linear_workspace(Ctx& c) {
   const size_t n = c.n, n3 = 3 * n;
   const int R = Ctx::kRestart;
@@ -1417,34 +1533,13 @@ void setup_linear_workspace(Ctx& c) {
   RF_CUDA(cudaMalloc(&c.d_bicg_iters, sizeof(long long)));
   RF_CUDA(cudaMemset(c.d_bicg_iters, 0, sizeof(long long)));
   // the largest cluster (16 CTAs, non-portable; else 8) that every level-scheduled kernel can run
-  const void* fns[3] = {(const void*)k_factor_cluster, (const void*)k_block_sweep_cluster,
-                        (const void*)k_bicgstab_cluster};
-  const int blocks[3] = {kFBlock, kCBlock, kCBlock};
-  c.cluster_size = 0;
-  for (int cs : {16, 8, 4, 2, 1}) {
-    bool ok = true;
-    for (int f = 0; f < 3 && ok; ++f) {
-      if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(cs);
-      cfg.blockDim = dim3(blocks[f]);
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = cs;
-      at[0].val.clusterDim.y = 1;
-      at[0].val.clusterDim.z = 1;
-      cfg.attrs = at;
-      cfg.numAttrs = 1;
-      int nclusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&nclusters, fns[f], &cfg) != cudaSuccess || nclusters < 1) ok = false;
-    }
-    cudaGetLastError();
-    if (ok) {
-      c.cluster_size = cs;
-      break;
-    }
-  }
-  if (c.cluster_size == 0) throw CudaError("no thread-block cluster shape fits the level-scheduled kernels");
+  // automatic cluster size: enough CTAs to give every row of the widest level its own thread
+  int widest = 1;
+  for (int l = 0; l < c.levels.n_levels; ++l)
+    widest = std::max(widest, c.levels.h_ptr[l + 1] - c.levels.h_ptr[l]);
+  int want = 1;
+  while (want < 16 && want * kCBlock < widest) want *= 2;
+  set_cluster_size(c, want);
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
   if (smem > 48 * 1024) RF_CUDA(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));

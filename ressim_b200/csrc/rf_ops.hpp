@@ -29,5 +29,10 @@ LinResult linear_solve_reduced(Ctx& c);
 // Build-once helpers
 void build_levels(Ctx& c);
 void setup_linear_workspace(Ctx& c);
+// 0: FP64 throughout; 1: FP32 block-ILU0 factors, FP32 pressure stage, FP64 FGMRES.
+void set_linear_precision(Ctx& c, int mode);
+// CTAs of the cluster that runs the level-scheduled kernels: the largest launchable power of two
+// <= want (1..16); returns it.
+int set_cluster_size(Ctx& c, int want);
 
 }  // namespace rf

@@ -1,0 +1,90 @@
+"""`Ensemble`: many independent decks (sensitivity variants of uneven sizes) stepped together.
+
+Each variant has its own device context; `step(dt)` advances every variant by one report step
+through `rf_batch_step`, which drives the variants from a pool of host threads so their kernels
+run concurrently on the GPU.  The reference simulator steps one deck per object; this is the
+batched form of the same step API.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, _lib
+from .deck import Deck
+from .simulator import DeviceError, _ptr
+
+
+class Ensemble:
+    def __init__(self, decks: list[Deck], host_threads: int = 0, precision: str = "fp64"):
+        L = _lib.load()
+        self.decks = list(decks)
+        self._abis = [d.to_abi() for d in self.decks]
+        arr = (C.POINTER(_abi.RfDeck) * len(self.decks))(*[C.pointer(a[0]) for a in self._abis])
+        h = C.c_void_p()
+        rc = L.rf_batch_create(arr, len(self.decks), int(host_threads), C.byref(h))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_batch_create failed ({rc}): {_lib.last_error(None)}")
+        self._h = h
+        self._ctx = [L.rf_batch_context(h, i) for i in range(len(self.decks))]
+        codes = {"fp64": _abi.RF_PRECISION_FP64, "mixed": _abi.RF_PRECISION_MIXED}
+        for i, d in enumerate(self.decks):
+            p = np.ascontiguousarray(d.pressure, dtype=np.float64)
+            sw = np.ascontiguousarray(d.sat_water, dtype=np.float64)
+            rc = L.rf_set_state(self._ctx[i], _ptr(p), _ptr(sw), None, None, 0.0)
+            if rc != _abi.RF_OK:
+                raise DeviceError(f"rf_set_state failed for variant {i}: {_lib.last_error(self._ctx[i])}")
+            rc = L.rf_set_linear_precision(self._ctx[i], codes[precision])
+            if rc != _abi.RF_OK:
+                raise DeviceError(f"rf_set_linear_precision failed for variant {i}")
+
+    def __len__(self):
+        return len(self.decks)
+
+    @property
+    def cells(self) -> int:
+        return sum(d.n_cells for d in self.decks)
+
+    def step(self, target_dt_days: float) -> list[dict]:
+        n = len(self.decks)
+        reps = (_abi.RfStepReport * n)()
+        rc = _lib.load().rf_batch_step(self._h, float(target_dt_days), reps)
+        if rc < 0:
+            raise DeviceError(f"rf_batch_step failed ({rc})")
+        return [r.as_dict() for r in reps]
+
+    def state(self, i: int) -> dict:
+        n = self.decks[i].n_cells
+        p, sw, so = np.zeros(n), np.zeros(n), np.zeros(n)
+        t = C.c_double()
+        rc = _lib.load().rf_get_state(self._ctx[i], _ptr(p), _ptr(sw), _ptr(so), None, None, C.byref(t))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_get_state failed for variant {i}: {_lib.last_error(self._ctx[i])}")
+        return {"pressure": p, "sat_water": sw, "sat_oil": so, "time": t.value}
+
+    def kernel_launches(self) -> int:
+        L = _lib.load()
+        return sum(int(L.rf_kernel_launches(c)) for c in self._ctx)
+
+    def profile(self, i: int, enable=None, reset=False) -> dict:
+        out = np.zeros(len(_lib.PHASES) + 3)
+        en = -1 if enable is None else int(bool(enable))
+        _lib.load().rf_profile(self._ctx[i], en, int(reset), _ptr(out), len(out))
+        d = {k: float(v) for k, v in zip(_lib.PHASES, out)}
+        k = len(_lib.PHASES)
+        d["bicgstab_iterations"] = int(out[k])
+        d["bicgstab_launches"] = int(out[k + 1])
+        d["nnzb"] = int(out[k + 2])
+        return d
+
+    def close(self):
+        if self._h is not None:
+            _lib.load().rf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -145,6 +145,24 @@ class ReservoirSimulator(Deck):
         d["nnzb"] = int(out[k + 2])
         return d
 
+    def set_linear_precision(self, mode: str) -> None:
+        """"fp64" (default, the reference's arithmetic) or "mixed" (FP32 block-ILU0 and pressure
+        stage under the FP64 FGMRES)."""
+        codes = {"fp64": _abi.RF_PRECISION_FP64, "mixed": _abi.RF_PRECISION_MIXED}
+        if mode not in codes:
+            raise ValueError(f"precision must be one of {sorted(codes)}")
+        rc = _lib.load().rf_set_linear_precision(self._context(), codes[mode])
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_set_linear_precision failed ({rc}): {_lib.last_error(self._context())}")
+
+    def set_cluster_size(self, ctas: int = 0) -> int:
+        """CTAs of the cluster running the level-scheduled kernels (0: automatic); returns the size
+        in use."""
+        rc = _lib.load().rf_set_cluster_size(self._context(), int(ctas))
+        if rc <= 0:
+            raise DeviceError(f"rf_set_cluster_size failed ({rc}): {_lib.last_error(self._context())}")
+        return rc
+
     def kernel_launches(self) -> int:
         return int(_lib.load().rf_kernel_launches(self._context()))
 

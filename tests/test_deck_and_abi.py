@@ -17,7 +17,7 @@ def test_library_exports_every_declared_symbol():
     declared = set()
     for line in open(HEADER):
         line = line.strip()
-        if line.startswith(("int32_t rf_", "int64_t rf_")):
+        if line.startswith(("int32_t rf_", "int64_t rf_", "RfCtx* rf_")):
             declared.add(line.split("(")[0].split()[-1])
     assert declared == set(_lib.EXPORTED_SYMBOLS)
     for name in declared:
