@@ -881,6 +881,8 @@ static void free_ctx(Ctx& c) {
                   &c.d_perf_well, &c.d_perf_inj, &c.d_perf_has_wi, &c.d_well_ptr, &c.d_well_perfs, &c.d_tinv_off,
                   &c.d_perf_row_off, &c.d_flag_dense, &c.d_dense_perm})
     b->free();
+  for (auto* b : {&c.d_own_rows, &c.d_own_ptr})
+    b->free();
   for (auto* b : {&c.d_lu32, &c.d_dinv32, &c.d_plu32, &c.d_pval32, &c.d_pdiag32, &c.d_pvec32, &c.d_sweep32})
     b->free();
   c.d_bmask.free();
@@ -1071,15 +1073,7 @@ int64_t rf_kernel_launches(const RfCtx* ctx) { return ctx ? ctx->c.launches : 0;
 int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas) {
   if (!ctx || ctas < 0 || ctas > 16) return RF_ERR_INVALID;
   return guarded(ctx, [&]() -> int32_t {
-    if (ctas == 0) {
-      int widest = 1;
-      const auto& hp = ctx->c.levels.h_ptr;
-      for (size_t l = 0; l + 1 < hp.size(); ++l) widest = std::max(widest, hp[l + 1] - hp[l]);
-      int want = 1;
-      while (want < 16 && want * 1024 < widest) want *= 2;
-      return rf::set_cluster_size(ctx->c, want);
-    }
-    return rf::set_cluster_size(ctx->c, ctas);
+    return rf::set_cluster_size(ctx->c, ctas == 0 ? rf::auto_cluster_size(ctx->c) : ctas);
   });
 }
 

@@ -35,6 +35,7 @@ struct Topology {
 struct Levels {
   int n_levels = 0;
   std::vector<int> h_ptr;
+  std::vector<int> h_rows;
   int* d_rows = nullptr;
   int* d_ptr = nullptr;
 };
@@ -124,6 +125,10 @@ struct Ctx {
   DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
   DBuf<double> d_partials, d_scal;
   int cluster_size = 0;  // CTAs in the one cluster that runs the level-scheduled kernels
+  // slice ownership schedule of the distributed-shared-memory BiCGStab (built for cluster_size)
+  int own_slice = 0;
+  size_t dsm_bytes[2] = {0, 0};  // dynamic shared memory per CTA for double / float; 0: does not fit
+  DBuf<int> d_own_rows, d_own_ptr;
   // linear-solver precision: 0 FP64; 1 mixed (FP32 block-ILU0 and pressure stage under FP64 FGMRES)
   int precision = 0;
   DBuf<float> d_lu32, d_dinv32, d_plu32, d_pval32, d_pdiag32, d_pvec32, d_sweep32;

@@ -733,12 +733,13 @@ struct BicgArgs {
 // advanced identically by every CTA): a CTA may run ahead into the next reduction and overwrite
 // its own slot while a slower CTA is still reading this reduction's partials, but it cannot reach
 // the reduction after that before the slower CTA has passed the barrier in between.
+template <int BLOCK = kCBlock>
 __device__ void cluster_sums(double* red /* shared [2][4] */, int& parity, int nq, const double* vals, double* out,
                              double* sh) {
   double* buf = red + (parity & 1) * 4;
   ++parity;
   for (int q = 0; q < nq; ++q) {
-    const double r = block_sum<kCBlock>(vals[q], sh);
+    const double r = block_sum<BLOCK>(vals[q], sh);
     if (threadIdx.x == 0) buf[q] = r;
   }
   cluster_barrier();
@@ -881,6 +882,215 @@ __global__ void __launch_bounds__(kCBlock, 1) k_bicgstab_cluster(BicgArgs<T> a) 
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.iter_counter)
     atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
   // no CTA may leave while another can still read its shared partials
+  cluster_barrier();
+}
+
+// ============================================================================================
+// BiCGStab with the vectors the level sweeps exchange held in distributed shared memory
+// ============================================================================================
+// Used when the pressure system fits the cluster's shared memory.  CTA b of the cluster owns the
+// contiguous rows [b*S, b*S + S) ("slice"): it computes every row of its slice in every phase, so
+// all vectors that are only read at a row's own index (r, rh, p, v, s, t, x) stay in global memory
+// touched by one SM, and the three vectors read at neighbour indices (the forward-sweep result y
+// and the sweep outputs ph and sh, which the SpMV reads next) live in the owners' shared memory.
+// A neighbour in another slice is read through the cluster's distributed shared memory
+// (mapa + ld.shared::cluster), so a level costs a cluster barrier plus one on-chip round trip
+// instead of an L2 round trip after a release of global stores.  Within each slice the rows keep
+// the level order, so every row still sees exactly the values the sequential sweep would.
+constexpr int kDBlock = 256;
+
+struct OwnedLevels {
+  int slice;        // rows per CTA (the last CTA may own fewer)
+  const int* rows;  // [n]: CTA b's rows in level order at [b*slice, b*slice + count_b)
+  const int* ptr;   // [cs * (n_levels + 1)]: per-CTA level pointers, relative to b*slice
+};
+
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned v;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(v));
+  return v;
+}
+__device__ __forceinline__ double dsm_load(const double* p, unsigned rank) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  unsigned r;
+  double v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r) : "memory");
+  return v;
+}
+__device__ __forceinline__ float dsm_load(const float* p, unsigned rank) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  unsigned r;
+  float v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(r) : "memory");
+  return v;
+}
+// element `idx` of a slice-distributed vector whose local slice starts at `local`
+template <class T>
+__device__ __forceinline__ T slice_read(const T* local, int idx, int slice, unsigned me) {
+  const unsigned owner = unsigned(idx / slice);
+  const T* p = local + (idx - int(owner) * slice);
+  return owner == me ? *p : dsm_load(p, owner);
+}
+
+template <class T>
+struct DsmBicgArgs {
+  int n, n_levels;
+  OwnedLevels own;
+  const int* rp;
+  const int* col;
+  const int* diag;
+  const T* pval;
+  const T* plu;
+  const T* pdiag;
+  const double* rhs;
+  double* x;
+  T* r;
+  T* rh;
+  T* p;
+  T* v;
+  T* s;
+  T* t;
+  int max_iters;
+  long long* iter_counter;
+};
+
+template <class T>
+__device__ void dsm_ilu_apply(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr, int base, unsigned me,
+                              const T* rhs, T* y_s, T* out_s) {
+  const int S = a.own.slice;
+  for (int l = 0; l < a.n_levels; ++l) {
+    for (int q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
+      const int r = lrows[q];
+      T s = rhs[r];
+      for (int k = a.rp[r]; k < a.diag[r]; ++k) s -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
+      y_s[r - base] = s;
+    }
+    cluster_barrier();
+  }
+  for (int l = a.n_levels - 1; l >= 0; --l) {
+    for (int q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
+      const int r = lrows[q];
+      T s = y_s[r - base];
+      for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) s -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+      const T d = a.pdiag[r];
+      out_s[r - base] = fabs(double(d)) > kEps ? s / d : s;
+    }
+    cluster_barrier();
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void dsm_spmv(const DsmBicgArgs<T>& a, int base, int cnt, unsigned me, const T* in_s,
+                                         T* out) {
+  const int S = a.own.slice;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const int r = base + i;
+    T s = T(0);
+    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) s += a.pval[k] * slice_read(in_s, a.col[k], S, me);
+    out[r] = s;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char dsm_raw[];
+  __shared__ double sh[32];
+  __shared__ double red[8];
+  const int S = a.own.slice, n = a.n;
+  T* y_s = reinterpret_cast<T*>(dsm_raw);
+  T* ph_s = y_s + S;
+  T* sh_s = ph_s + S;
+  int* lrows = reinterpret_cast<int*>(sh_s + S);
+  int* lptr = lrows + S;
+  const unsigned me = cluster_rank();
+  const int base = int(me) * S;
+  const int cnt = max(0, min(S, n - base));
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) lrows[i] = a.own.rows[base + i];
+  for (int l = threadIdx.x; l <= a.n_levels; l += blockDim.x) lptr[l] = a.own.ptr[size_t(me) * (a.n_levels + 1) + l];
+  double v3[3], o3[3];
+  int parity = 0;
+  v3[0] = 0.0;
+  for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) {
+    const double ri = a.rhs[i] - 0.0;
+    const T rt = T(ri);
+    a.x[i] = 0.0;
+    a.r[i] = rt;
+    a.rh[i] = rt;
+    a.v[i] = T(0);
+    a.p[i] = T(0);
+    v3[0] += double(rt) * double(rt);
+  }
+  cluster_sums<kDBlock>(red, parity, 1, v3, o3, sh);
+  const double rnorm0 = sqrt(o3[0]);
+  const double tol = fmax(rnorm0, kEps) * 1e-6;
+  const int max_iters = rnorm0 <= tol ? 0 : a.max_iters;
+  double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  int started = 0;
+  for (int it = 0; it < max_iters; ++it) {
+    started = it + 1;
+    v3[0] = 0.0;
+    for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) v3[0] += double(a.rh[i]) * double(a.r[i]);
+    cluster_sums<kDBlock>(red, parity, 1, v3, o3, sh);
+    const double rho = o3[0];
+    if (!isfinite(rho) || fabs(rho) < kEps) break;
+    if (it == 0) {
+      for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) a.p[i] = a.r[i];
+    } else {
+      const double beta = (rho / rho_prev) * (alpha / omega);
+      for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x)
+        a.p[i] = T(double(a.r[i]) + beta * (double(a.p[i]) - omega * double(a.v[i])));
+    }
+    __syncthreads();
+    dsm_ilu_apply(a, lrows, lptr, base, me, a.p, y_s, ph_s);
+    dsm_spmv(a, base, cnt, me, ph_s, a.v);
+    v3[0] = 0.0;
+    for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) v3[0] += double(a.rh[i]) * double(a.v[i]);
+    cluster_sums<kDBlock>(red, parity, 1, v3, o3, sh);
+    const double vd = o3[0];
+    if (!isfinite(vd) || fabs(vd) < kEps) break;
+    alpha = rho / vd;
+    v3[0] = 0.0;
+    for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) {
+      const T si = T(double(a.r[i]) - alpha * double(a.v[i]));
+      a.s[i] = si;
+      v3[0] += double(si) * double(si);
+    }
+    cluster_sums<kDBlock>(red, parity, 1, v3, o3, sh);
+    if (sqrt(o3[0]) <= tol) {
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) a.x[base + i] += alpha * double(ph_s[i]);
+      break;
+    }
+    dsm_ilu_apply(a, lrows, lptr, base, me, a.s, y_s, sh_s);
+    dsm_spmv(a, base, cnt, me, sh_s, a.t);
+    v3[0] = 0.0;
+    v3[1] = 0.0;
+    for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) {
+      const double ti = double(a.t[i]);
+      v3[0] += ti * ti;
+      v3[1] += ti * double(a.s[i]);
+    }
+    cluster_sums<kDBlock>(red, parity, 2, v3, o3, sh);
+    const double tt = o3[0];
+    if (!isfinite(tt) || tt <= kEps) break;
+    omega = o3[1] / tt;
+    if (!isfinite(omega) || fabs(omega) < kEps) break;
+    v3[0] = 0.0;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const int g = base + i;
+      a.x[g] += alpha * double(ph_s[i]) + omega * double(sh_s[i]);
+      const T ri = T(double(a.s[g]) - omega * double(a.t[g]));
+      a.r[g] = ri;
+      v3[0] += double(ri) * double(ri);
+    }
+    cluster_sums<kDBlock>(red, parity, 1, v3, o3, sh);
+    if (sqrt(o3[0]) <= tol) break;
+    rho_prev = rho;
+  }
+  if (me == 0 && threadIdx.x == 0 && a.iter_counter)
+    atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
+  // no CTA may leave while another can still read its shared memory
   cluster_barrier();
 }
 
@@ -1127,8 +1337,55 @@ static void cpr_build(Ctx& c) {
 }
 
 template <class T>
+static bool launch_bicgstab_dsmem(Ctx& c, const T* pval, const T* plu, const T* pdiag, const double* rhs, double* x,
+                                  T* base) {
+  const size_t bytes = c.dsm_bytes[sizeof(T) == 4 ? 1 : 0];
+  if (bytes == 0) return false;
+  const size_t n = c.n;
+  DsmBicgArgs<T> a;
+  a.n = c.n;
+  a.n_levels = c.levels.n_levels;
+  a.own.slice = c.own_slice;
+  a.own.rows = c.d_own_rows.p;
+  a.own.ptr = c.d_own_ptr.p;
+  a.rp = c.d_row_ptr.p;
+  a.col = c.d_col.p;
+  a.diag = c.d_diag.p;
+  a.pval = pval;
+  a.plu = plu;
+  a.pdiag = pdiag;
+  a.rhs = rhs;
+  a.x = x;
+  a.r = base;
+  a.rh = base + n;
+  a.p = base + 2 * n;
+  a.v = base + 3 * n;
+  a.s = base + 5 * n;
+  a.t = base + 7 * n;
+  a.max_iters = 50;
+  a.iter_counter = c.d_bicg_iters;
+  void* args[] = {&a};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(c.cluster_size);
+  cfg.blockDim = dim3(kDBlock);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = c.stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = c.cluster_size;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  RF_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_bicgstab_dsmem<T>, args));
+  c.launches++;
+  return true;
+}
+
+template <class T>
 static void launch_bicgstab(Ctx& c, const T* pval, const T* plu, const T* pdiag, const double* rhs, double* x,
                             T* base) {
+  if (launch_bicgstab_dsmem<T>(c, pval, plu, pdiag, rhs, x, base)) return;
   const size_t n = c.n;
   BicgArgs<T> a;
   a.L = level_sched(c);
@@ -1447,11 +1704,79 @@ void build_levels(Ctx& c) {
   for (int l = 0; l < c.levels.n_levels; ++l) c.levels.h_ptr[l + 1] += c.levels.h_ptr[l];
   std::vector<int> rows(n), fillp(c.levels.h_ptr.begin(), c.levels.h_ptr.end() - 1);
   for (int i = 0; i < n; ++i) rows[fillp[lvl[i]]++] = i;
+  c.levels.h_rows = rows;
   RF_CUDA(cudaMalloc(&c.levels.d_rows, sizeof(int) * n));
   RF_CUDA(cudaMalloc(&c.levels.d_ptr, sizeof(int) * (c.levels.n_levels + 1)));
   RF_CUDA(cudaMemcpy(c.levels.d_rows, rows.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   RF_CUDA(cudaMemcpy(c.levels.d_ptr, c.levels.h_ptr.data(), sizeof(int) * (c.levels.n_levels + 1),
                      cudaMemcpyHostToDevice));
+}
+
+// Automatic cluster size: the smallest power of two (<= 16) whose slices hold at most 4608 rows,
+// so the distributed-shared-memory BiCGStab applies, and at least enough 1024-thread CTAs to give
+// every row of the widest level its own thread.
+int auto_cluster_size(const Ctx& c) {
+  int widest = 1;
+  for (int l = 0; l < c.levels.n_levels; ++l)
+    widest = std::max(widest, c.levels.h_ptr[l + 1] - c.levels.h_ptr[l]);
+  int want = 1;
+  while (want < 16 && ((c.n + want - 1) / want > 4608 || want * kCBlock < widest)) want *= 2;
+  return want;
+}
+
+// Slice ownership for the distributed-shared-memory BiCGStab at the current cluster size: CTA b
+// owns rows [b*S, b*S + S), listed in level order (ties in row order), with per-CTA level
+// pointers.  Records, per value type, the dynamic shared memory the kernel needs, or 0 when the
+// slices do not fit (the global-memory cluster kernel runs instead).
+static void build_owned_levels(Ctx& c) {
+  const int n = c.n, cs = c.cluster_size, L = c.levels.n_levels;
+  const int S = (n + cs - 1) / cs;
+  std::vector<int> lvl(n);
+  for (int l = 0; l < L; ++l)
+    for (int q = c.levels.h_ptr[l]; q < c.levels.h_ptr[l + 1]; ++q) lvl[c.levels.h_rows[q]] = l;
+  std::vector<int> rows(n), ptr(size_t(cs) * (L + 1), 0);
+  for (int b = 0; b < cs; ++b) {
+    const int lo = b * S, hi = std::min(n, lo + S);
+    int* bp = ptr.data() + size_t(b) * (L + 1);
+    for (int r = lo; r < hi; ++r) bp[lvl[r] + 1]++;
+    for (int l = 0; l < L; ++l) bp[l + 1] += bp[l];
+    std::vector<int> fill(bp, bp + L);
+    for (int r = lo; r < hi; ++r) rows[lo + fill[lvl[r]]++] = r;
+  }
+  c.own_slice = S;
+  c.d_own_rows.free();
+  c.d_own_ptr.free();
+  c.d_own_rows.alloc(n);
+  c.d_own_ptr.alloc(ptr.size());
+  RF_CUDA(cudaMemcpy(c.d_own_rows.p, rows.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.d_own_ptr.p, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice));
+  int optin = 0;
+  RF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+  const void* fns[2] = {(const void*)k_bicgstab_dsmem<double>, (const void*)k_bicgstab_dsmem<float>};
+  const size_t tsz[2] = {sizeof(double), sizeof(float)};
+  for (int f = 0; f < 2; ++f) {
+    c.dsm_bytes[f] = 0;
+    cudaFuncAttributes fa;
+    RF_CUDA(cudaFuncGetAttributes(&fa, fns[f]));
+    const size_t bytes = 3 * size_t(S) * tsz[f] + sizeof(int) * (size_t(S) + L + 1);
+    if (bytes + fa.sharedSizeBytes > size_t(optin)) continue;
+    RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kDBlock);
+    cfg.dynamicSmemBytes = bytes;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, fns[f], &cfg) == cudaSuccess && ncl >= 1) c.dsm_bytes[f] = bytes;
+    cudaGetLastError();
+  }
 }
 
 // The largest cluster size <= `want` (a power of two, 1..16) that every level-scheduled kernel
@@ -1482,6 +1807,7 @@ int set_cluster_size(Ctx& c, int want) {
     cudaGetLastError();
     if (ok) {
       c.cluster_size = cs;
+      build_owned_levels(c);
       return cs;
     }
   }
@@ -1533,13 +1859,7 @@ void setup_linear_workspace(Ctx& c) {
   RF_CUDA(cudaMalloc(&c.d_bicg_iters, sizeof(long long)));
   RF_CUDA(cudaMemset(c.d_bicg_iters, 0, sizeof(long long)));
   // the largest cluster (16 CTAs, non-portable; else 8) that every level-scheduled kernel can run
-  // automatic cluster size: enough CTAs to give every row of the widest level its own thread
-  int widest = 1;
-  for (int l = 0; l < c.levels.n_levels; ++l)
-    widest = std::max(widest, c.levels.h_ptr[l + 1] - c.levels.h_ptr[l]);
-  int want = 1;
-  while (want < 16 && want * kCBlock < widest) want *= 2;
-  set_cluster_size(c, want);
+  set_cluster_size(c, auto_cluster_size(c));
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
   if (smem > 48 * 1024) RF_CUDA(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));

@@ -34,5 +34,6 @@ void set_linear_precision(Ctx& c, int mode);
 // CTAs of the cluster that runs the level-scheduled kernels: the largest launchable power of two
 // <= want (1..16); returns it.
 int set_cluster_size(Ctx& c, int want);
+int auto_cluster_size(const Ctx& c);
 
 }  // namespace rf

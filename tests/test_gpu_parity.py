@@ -8,18 +8,13 @@ is three times the oracle-vs-oracle difference under a changed summation order, 
 import numpy as np
 import pytest
 
+from _parity import check_within_floor, oracle_runs, rel_err
 from oracle.oracle_py import OracleSimulator, linear_solve_csr
 from ressim_b200 import ReservoirSimulator, decks, linear_solve_bsr
 
 pytestmark = pytest.mark.gpu
 
 FIELD_RTOL = 1e-6
-
-
-def rel_err(a, b):
-    a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
-    scale = np.maximum(np.abs(b), 1.0)
-    return float(np.max(np.abs(a - b) / scale)) if a.size else 0.0
 
 
 def run_pair(deck, dt, steps):
@@ -84,35 +79,14 @@ def test_waterflood_3d_mid_parity_at_rounding_floor():
     The oracle run twice, with the reference's left-to-right dot products and with interleaved
     partial sums, measures that rounding floor; the device path must stay within it (x3, plus
     1e-6), with Newton counts within one."""
-    from oracle.oracle_py import lib
-
     deck = decks.waterflood_3d(30, 30, 10, seed=7)
     dt, steps = 10.0, 3
-    runs = {}
-    try:
-        for mode in (0, 1):
-            lib().orc_set_sum_order(mode)
-            o = OracleSimulator(deck)
-            runs[mode] = []
-            for _ in range(steps):
-                rc, r = o.step(dt)
-                assert rc == 0
-                st = o.state()
-                runs[mode].append((st["pressure"].copy(), st["sat_water"].copy(), r.newton_iterations))
-            o.close()
-    finally:
-        lib().orc_set_sum_order(0)
+    runs = oracle_runs(deck, dt, steps)
     gpu = ReservoirSimulator.from_deck(deck)
     for s in range(steps):
         rg = gpu.step(dt)
         gs = gpu.state()
-        p0, sw0, n0 = runs[0][s]
-        p1, sw1, _ = runs[1][s]
-        floor_p = rel_err(p1, p0)
-        floor_sw = rel_err(sw1, sw0)
-        assert rel_err(gs["pressure"], p0) <= 3 * floor_p + FIELD_RTOL, (s, rel_err(gs["pressure"], p0), floor_p)
-        assert rel_err(gs["sat_water"], sw0) <= 3 * floor_sw + FIELD_RTOL, (s, rel_err(gs["sat_water"], sw0), floor_sw)
-        assert abs(rg["newton_iterations"] - n0) <= 1, (s, rg["newton_iterations"], n0)
+        check_within_floor(s, gs["pressure"], gs["sat_water"], rg["newton_iterations"], runs)
 
 
 def _csr_to_bsr(n_cells, ptr, col, val):
