@@ -397,19 +397,20 @@ inline void csr_matvec(const Csr& m, const std::vector<double>& x, std::vector<d
 }
 
 // Summation order of the vector dots and norms: 0 is the reference's left-to-right order.  A
-// test hook sets 1 (256 interleaved partial sums, then added in order), which changes only the
+// test hook sets w >= 2 (w interleaved partial sums, then added in order), which changes only the
 // rounding, to measure how far rounding alone moves a run.
 inline int g_sum_order = 0;
 inline double vdot_n(size_t n, const double* a, const double* b) {
-  if (g_sum_order == 0) {
+  if (g_sum_order < 2) {
     double s = 0.0;
     for (size_t i = 0; i < n; ++i) s += a[i] * b[i];
     return s;
   }
-  double part[256] = {0.0};
-  for (size_t i = 0; i < n; ++i) part[i & 255] += a[i] * b[i];
+  const size_t w = size_t(g_sum_order);
+  std::vector<double> part(w, 0.0);
+  for (size_t i = 0; i < n; ++i) part[i % w] += a[i] * b[i];
   double s = 0.0;
-  for (int k = 0; k < 256; ++k) s += part[k];
+  for (size_t k = 0; k < w; ++k) s += part[k];
   return s;
 }
 inline double vnorm(const std::vector<double>& x) { return std::sqrt(vdot_n(x.size(), x.data(), x.data())); }

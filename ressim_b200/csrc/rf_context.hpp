@@ -129,6 +129,9 @@ struct Ctx {
   int own_slice = 0;
   size_t dsm_bytes[2] = {0, 0};  // dynamic shared memory per CTA for double / float; 0: does not fit
   DBuf<int> d_own_rows, d_own_ptr;
+  DBuf<int> d_fcnt, d_bcnt, d_fdep, d_bdep;  // packed sweep structure (ownership order)
+  DBuf<double> d_fval, d_bval, d_dval;       // packed factor values, FP64
+  DBuf<float> d_fval32, d_bval32, d_dval32;  // packed factor values, mixed form
   // linear-solver precision: 0 FP64; 1 mixed (FP32 block-ILU0 and pressure stage under FP64 FGMRES)
   int precision = 0;
   DBuf<float> d_lu32, d_dinv32, d_plu32, d_pval32, d_pdiag32, d_pvec32, d_sweep32;

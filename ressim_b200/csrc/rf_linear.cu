@@ -934,6 +934,19 @@ __device__ __forceinline__ T slice_read(const T* local, int idx, int slice, unsi
   return owner == me ? *p : dsm_load(p, owner);
 }
 
+// Level-ordered packed rows of each CTA's slice (index g = position in the ownership order,
+// the same order as OwnedLevels::rows): for the forward (L) and backward (U) parts, the number of
+// entries (-1 when more than kPackK: that row takes the CSR path), each entry's column as
+// (owner CTA << 24) | index within the owner's slice, and the factor values in column order.
+// The structure is fixed per pattern; the values are repacked after every factorisation.
+constexpr int kPackK = 4;
+template <class T>
+struct PackedSweep {
+  const int* cnt;  // [n]
+  const int* dep;  // [kPackK][n]
+  const T* val;    // [kPackK][n]
+};
+
 template <class T>
 struct DsmBicgArgs {
   int n, n_levels;
@@ -944,6 +957,8 @@ struct DsmBicgArgs {
   const T* pval;
   const T* plu;
   const T* pdiag;
+  PackedSweep<T> fw, bw;
+  const T* dval;  // [n] pivots in ownership order
   const double* rhs;
   double* x;
   T* r;
@@ -956,29 +971,149 @@ struct DsmBicgArgs {
   long long* iter_counter;
 };
 
+__device__ __forceinline__ void cluster_arrive_release() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <class T>
+__device__ __forceinline__ T dep_read(const T* slice_base, int dep, unsigned me) {
+  const unsigned owner = unsigned(dep) >> 24;
+  const T* p = slice_base + (dep & 0xffffff);
+  return owner == me ? *p : dsm_load(p, owner);
+}
+
+// One row's packed data, loaded one level ahead.
+template <class T>
+struct PackedRow {
+  int g, r, cnt;
+  int dep[kPackK];
+  T val[kPackK];
+  T extra;  // forward: rhs[r]; backward: pivot
+};
+
+template <class T>
+__device__ __forceinline__ void load_packed(PackedRow<T>& pr, const PackedSweep<T>& ps, int n, int g, int r,
+                                            const T* extra_src, int extra_idx) {
+  pr.g = g;
+  pr.r = r;
+  pr.cnt = ps.cnt[g];
+#pragma unroll
+  for (int j = 0; j < kPackK; ++j) {
+    pr.dep[j] = ps.dep[size_t(j) * n + g];
+    pr.val[j] = ps.val[size_t(j) * n + g];
+  }
+  pr.extra = extra_src[extra_idx];
+}
+
+// s - sum_j val_j * src[dep_j] over the row's entries in column order; the dependency loads are
+// issued together, the subtractions keep the sequential order.
+template <class T>
+__device__ __forceinline__ T packed_subtract(T s, const PackedRow<T>& pr, const T* src, unsigned me) {
+  T d[kPackK];
+#pragma unroll
+  for (int j = 0; j < kPackK; ++j) d[j] = j < pr.cnt ? dep_read(src, pr.dep[j], me) : T(0);
+#pragma unroll
+  for (int j = 0; j < kPackK; ++j)
+    if (j < pr.cnt) s -= pr.val[j] * d[j];
+  return s;
+}
+
+// out = PressureILU(rhs) on slices: forward levels into y_s, backward levels into out_s.  Each
+// thread handles one row per level from data loaded during the previous level's barrier (between
+// arrive and wait, so the loads overlap the barrier); further rows of a wide level and rows with
+// more than kPackK entries take the CSR path.
 template <class T>
 __device__ void dsm_ilu_apply(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr, int base, unsigned me,
                               const T* rhs, T* y_s, T* out_s) {
-  const int S = a.own.slice;
-  for (int l = 0; l < a.n_levels; ++l) {
-    for (int q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
-      const int r = lrows[q];
-      T s = rhs[r];
-      for (int k = a.rp[r]; k < a.diag[r]; ++k) s -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
-      y_s[r - base] = s;
-    }
-    cluster_barrier();
+  const int S = a.own.slice, n = a.n, L = a.n_levels, t = threadIdx.x, B = blockDim.x;
+  PackedRow<T> cur, nxt;
+  cur.cnt = -2;
+  if (lptr[0] + t < lptr[1]) {
+    const int q = lptr[0] + t;
+    load_packed(cur, a.fw, n, base + q, lrows[q], rhs, lrows[q]);
   }
-  for (int l = a.n_levels - 1; l >= 0; --l) {
-    for (int q = lptr[l] + threadIdx.x; q < lptr[l + 1]; q += blockDim.x) {
+  for (int l = 0; l < L; ++l) {
+    const int q0 = lptr[l] + t, qe = lptr[l + 1];
+    if (q0 < qe) {
+      if (cur.cnt >= 0) {
+        y_s[cur.r - base] = packed_subtract(cur.extra, cur, y_s, me);
+      } else {
+        const int r = cur.r;
+        T sum = cur.extra;
+        for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
+        y_s[r - base] = sum;
+      }
+    }
+    for (int q = q0 + B; q < qe; q += B) {
       const int r = lrows[q];
-      T s = y_s[r - base];
-      for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) s -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+      T sum = rhs[r];
+      for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
+      y_s[r - base] = sum;
+    }
+    cluster_arrive_release();
+    nxt.cnt = -2;
+    if (l + 1 < L && lptr[l + 1] + t < lptr[l + 2]) {
+      const int q = lptr[l + 1] + t;
+      load_packed(nxt, a.fw, n, base + q, lrows[q], rhs, lrows[q]);
+    }
+    cluster_wait_acquire();
+    cur = nxt;
+  }
+  cur.cnt = -2;
+  if (lptr[L - 1] + t < lptr[L]) {
+    const int q = lptr[L - 1] + t;
+    load_packed(cur, a.bw, n, base + q, lrows[q], a.dval, base + q);
+  }
+  for (int l = L - 1; l >= 0; --l) {
+    const int q0 = lptr[l] + t, qe = lptr[l + 1];
+    if (q0 < qe) {
+      const int r = cur.r;
+      T sum = y_s[r - base];
+      if (cur.cnt >= 0) {
+        sum = packed_subtract(sum, cur, out_s, me);
+      } else {
+        for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+      }
+      const T d = cur.extra;
+      out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
+    }
+    for (int q = q0 + B; q < qe; q += B) {
+      const int r = lrows[q];
+      T sum = y_s[r - base];
+      for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
       const T d = a.pdiag[r];
-      out_s[r - base] = fabs(double(d)) > kEps ? s / d : s;
+      out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
     }
-    cluster_barrier();
+    cluster_arrive_release();
+    nxt.cnt = -2;
+    if (l > 0 && lptr[l - 1] + t < lptr[l]) {
+      const int q = lptr[l - 1] + t;
+      load_packed(nxt, a.bw, n, base + q, lrows[q], a.dval, base + q);
+    }
+    cluster_wait_acquire();
+    cur = nxt;
   }
+}
+
+// Values of the packed sweeps after a factorisation (ownership order, column order per row).
+template <class T>
+__global__ void k_pack_sweeps(int n, const int* __restrict__ own_rows, const int* __restrict__ rp,
+                              const int* __restrict__ diag, const int* __restrict__ fcnt, const int* __restrict__ bcnt,
+                              const double* __restrict__ plu, const double* __restrict__ pdiag, T* __restrict__ fval,
+                              T* __restrict__ bval, T* __restrict__ dval) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const int r = own_rows[g];
+  const int fc = fcnt[g], bc = bcnt[g];
+#pragma unroll
+  for (int j = 0; j < kPackK; ++j) {
+    fval[size_t(j) * n + g] = j < fc ? T(plu[rp[r] + j]) : T(0);
+    bval[size_t(j) * n + g] = j < bc ? T(plu[diag[r] + 1 + j]) : T(0);
+  }
+  dval[g] = T(pdiag[r]);
 }
 
 template <class T>
@@ -1318,6 +1453,17 @@ static void cpr_build(Ctx& c) {
   double* pdiag = c.d_pdiag.p;
   void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
   cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
+  if (c.dsm_bytes[c.precision == 1 ? 1 : 0] != 0) {
+    if (c.precision == 1)
+      k_pack_sweeps<float><<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_own_rows.p, c.d_row_ptr.p, c.d_diag.p,
+                                                                   c.d_fcnt.p, c.d_bcnt.p, c.d_plu.p, c.d_pdiag.p,
+                                                                   c.d_fval32.p, c.d_bval32.p, c.d_dval32.p);
+    else
+      k_pack_sweeps<double><<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_own_rows.p, c.d_row_ptr.p, c.d_diag.p,
+                                                                    c.d_fcnt.p, c.d_bcnt.p, c.d_plu.p, c.d_pdiag.p,
+                                                                    c.d_fval.p, c.d_bval.p, c.d_dval.p);
+    c.launches++;
+  }
   if (c.precision == 1) {
     k_factors_to_f32<<<4 * c.num_sms, kBlock, 0, c.stream>>>(
         9ll * c.nnzb, c.d_lu.p, c.d_lu32.p, 9ll * n, c.d_dinv.p, c.d_dinv32.p, c.nnzb, c.d_plu.p, c.d_plu32.p,
@@ -1354,6 +1500,19 @@ static bool launch_bicgstab_dsmem(Ctx& c, const T* pval, const T* plu, const T* 
   a.pval = pval;
   a.plu = plu;
   a.pdiag = pdiag;
+  a.fw.cnt = c.d_fcnt.p;
+  a.fw.dep = c.d_fdep.p;
+  a.bw.cnt = c.d_bcnt.p;
+  a.bw.dep = c.d_bdep.p;
+  if constexpr (sizeof(T) == 4) {
+    a.fw.val = c.d_fval32.p;
+    a.bw.val = c.d_bval32.p;
+    a.dval = c.d_dval32.p;
+  } else {
+    a.fw.val = c.d_fval.p;
+    a.bw.val = c.d_bval.p;
+    a.dval = c.d_dval.p;
+  }
   a.rhs = rhs;
   a.x = x;
   a.r = base;
@@ -1743,13 +1902,43 @@ static void build_owned_levels(Ctx& c) {
     std::vector<int> fill(bp, bp + L);
     for (int r = lo; r < hi; ++r) rows[lo + fill[lvl[r]]++] = r;
   }
+  // packed sweep structure: entry counts (-1 above kPackK) and (owner << 24 | local) columns
+  std::vector<int> fcnt(n), bcnt(n), fdep(size_t(kPackK) * n, 0), bdep(size_t(kPackK) * n, 0);
+  auto packdep = [&](int col) { return ((col / S) << 24) | (col - (col / S) * S); };
+  for (int g = 0; g < n; ++g) {
+    const int r = rows[g];
+    const int lo = c.h_row_ptr[r], d = c.h_diag[r], hi = c.h_row_ptr[r + 1];
+    fcnt[g] = d - lo <= kPackK ? d - lo : -1;
+    bcnt[g] = hi - d - 1 <= kPackK ? hi - d - 1 : -1;
+    for (int j = 0; j < kPackK; ++j) {
+      if (j < fcnt[g]) fdep[size_t(j) * n + g] = packdep(c.h_col[lo + j]);
+      if (j < bcnt[g]) bdep[size_t(j) * n + g] = packdep(c.h_col[d + 1 + j]);
+    }
+  }
   c.own_slice = S;
-  c.d_own_rows.free();
-  c.d_own_ptr.free();
+  for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep}) b->free();
   c.d_own_rows.alloc(n);
   c.d_own_ptr.alloc(ptr.size());
+  c.d_fcnt.alloc(n);
+  c.d_bcnt.alloc(n);
+  c.d_fdep.alloc(size_t(kPackK) * n);
+  c.d_bdep.alloc(size_t(kPackK) * n);
   RF_CUDA(cudaMemcpy(c.d_own_rows.p, rows.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   RF_CUDA(cudaMemcpy(c.d_own_ptr.p, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.d_fcnt.p, fcnt.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.d_bcnt.p, bcnt.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.d_fdep.p, fdep.data(), sizeof(int) * fdep.size(), cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.d_bdep.p, bdep.data(), sizeof(int) * bdep.size(), cudaMemcpyHostToDevice));
+  if (c.d_fval.p == nullptr) {
+    c.d_fval.alloc(size_t(kPackK) * n);
+    c.d_bval.alloc(size_t(kPackK) * n);
+    c.d_dval.alloc(n);
+  }
+  if (c.precision == 1 && c.d_fval32.p == nullptr) {
+    c.d_fval32.alloc(size_t(kPackK) * n);
+    c.d_bval32.alloc(size_t(kPackK) * n);
+    c.d_dval32.alloc(n);
+  }
   int optin = 0;
   RF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
   const void* fns[2] = {(const void*)k_bicgstab_dsmem<double>, (const void*)k_bicgstab_dsmem<float>};
@@ -1816,6 +2005,12 @@ int set_cluster_size(Ctx& c, int want) {
 
 // FP32 factors and work vectors of the mixed form, allocated on first use.
 void set_linear_precision(Ctx& c, int mode) {
+  if (mode == 1 && c.d_fval32.p == nullptr) {
+    const size_t n = c.n;
+    c.d_fval32.alloc(size_t(kPackK) * n);
+    c.d_bval32.alloc(size_t(kPackK) * n);
+    c.d_dval32.alloc(n);
+  }
   if (mode == 1 && c.d_lu32.p == nullptr) {
     const size_t n = c.n;
     c.d_lu32.alloc(size_t(c.nnzb) * 9);

@@ -24,6 +24,7 @@ def test_mixed_precision_field_error(dims, steps):
     gpu = ReservoirSimulator.from_deck(deck)
     gpu.set_linear_precision("mixed")
     cpu = OracleSimulator(deck)
+    same_path = True
     for s in range(steps):
         rg = gpu.step(dt)
         rc, rep = cpu.step(dt)
@@ -34,7 +35,8 @@ def test_mixed_precision_field_error(dims, steps):
         print(f"{dims} step {s}: pressure rel {ep:.2e}, sw abs {es:.2e}, newton {rg['newton_iterations']} "
               f"vs {rep.newton_iterations}")
         assert rc == 0 and rg["warning"] == 0
-        if rg["newton_iterations"] == rep.newton_iterations and rg["substeps"] == rep.substeps:
+        same_path = same_path and rg["newton_iterations"] == rep.newton_iterations and rg["substeps"] == rep.substeps
+        if same_path:
             assert ep < 1e-4 and es < 1e-3, (s, ep, es)
         else:
             assert ep < 1e-2 and es < 5e-2, (s, ep, es)
