@@ -35,13 +35,29 @@ def oracle_runs(deck, dt, steps, orders=FLOOR_ORDERS):
     return runs
 
 
-def check_within_floor(step, p, sw, newton, runs, rtol=1e-6):
-    """Device fields within three times the rounding floor plus `rtol`; Newton count within one."""
+# Once a report step ends after a different number of Newton iterations (one more or one fewer,
+# which the parity bar allows), the runs stop at different points inside the Newton tolerance and
+# the next substep sizes differ; from then on the fields agree to the Newton tolerance, not to the
+# rounding floor.
+NEWTON_TOL_P, NEWTON_TOL_SW = 1e-4, 2e-3
+
+
+def check_within_floor(step, p, sw, newton, runs, rtol=1e-6, state=None):
+    """Device fields within three times the rounding floor plus `rtol` while every report step so
+    far took the oracle's Newton count; within the Newton tolerance after a step that did not.
+    Newton count within one.  `state` (a dict carried across steps) records the divergence."""
+    state = {} if state is None else state
     p0, sw0, n0 = runs[0][step]
     fp = max(rel_err(runs[m][step][0], p0) for m in runs if m != 0)
     fs = max(rel_err(runs[m][step][1], sw0) for m in runs if m != 0)
-    print(f"step {step}: pressure {rel_err(p, p0):.2e} (floor {fp:.2e}), sw {rel_err(sw, sw0):.2e} "
-          f"(floor {fs:.2e}), newton {newton} vs {n0}")
-    assert rel_err(p, p0) <= 3 * fp + rtol, (step, "pressure", rel_err(p, p0), fp)
-    assert rel_err(sw, sw0) <= 3 * fs + rtol, (step, "sat_water", rel_err(sw, sw0), fs)
+    ep, es = rel_err(p, p0), rel_err(sw, sw0)
+    print(f"step {step}: pressure {ep:.2e} (floor {fp:.2e}), sw {es:.2e} (floor {fs:.2e}), "
+          f"newton {newton} vs {n0}")
     assert abs(newton - n0) <= 1, (step, newton, n0)
+    if state.get("diverged"):
+        assert ep <= NEWTON_TOL_P and es <= NEWTON_TOL_SW, (step, ep, es)
+    else:
+        assert ep <= 3 * fp + rtol, (step, "pressure", ep, fp)
+        assert es <= 3 * fs + rtol, (step, "sat_water", es, fs)
+    if newton != n0:
+        state["diverged"] = True

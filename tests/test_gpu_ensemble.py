@@ -33,8 +33,9 @@ def test_batch_variant_matches_oracle():
     d = decks.ensemble_variant(SMALL_VARIANTS[0])
     runs = oracle_runs(d, 10.0, 2)
     ens = Ensemble([d, decks.ensemble_variant(SMALL_VARIANTS[1])], host_threads=2)
+    state = {}
     for s in range(2):
         reps = ens.step(10.0)
         g = ens.state(0)
-        check_within_floor(s, g["pressure"], g["sat_water"], reps[0]["newton_iterations"], runs)
+        check_within_floor(s, g["pressure"], g["sat_water"], reps[0]["newton_iterations"], runs, state=state)
     ens.close()

@@ -78,15 +78,17 @@ def test_waterflood_3d_mid_parity_at_rounding_floor():
     different summation order alone moves the Newton end state by more than 1e-6 in saturation.
     The oracle run twice, with the reference's left-to-right dot products and with interleaved
     partial sums, measures that rounding floor; the device path must stay within it (x3, plus
-    1e-6), with Newton counts within one."""
+    1e-6), with Newton counts within one.  After a report step that took one Newton iteration
+    more or fewer than the oracle, the bound is the Newton tolerance (tests/_parity.py)."""
     deck = decks.waterflood_3d(30, 30, 10, seed=7)
     dt, steps = 10.0, 3
     runs = oracle_runs(deck, dt, steps)
     gpu = ReservoirSimulator.from_deck(deck)
+    state = {}
     for s in range(steps):
         rg = gpu.step(dt)
         gs = gpu.state()
-        check_within_floor(s, gs["pressure"], gs["sat_water"], rg["newton_iterations"], runs)
+        check_within_floor(s, gs["pressure"], gs["sat_water"], rg["newton_iterations"], runs, state=state)
 
 
 def _csr_to_bsr(n_cells, ptr, col, val):
