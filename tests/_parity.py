@@ -54,10 +54,10 @@ def check_within_floor(step, p, sw, newton, runs, rtol=1e-6, state=None):
     print(f"step {step}: pressure {ep:.2e} (floor {fp:.2e}), sw {es:.2e} (floor {fs:.2e}), "
           f"newton {newton} vs {n0}")
     assert abs(newton - n0) <= 1, (step, newton, n0)
+    if newton != n0:
+        state["diverged"] = True
     if state.get("diverged"):
         assert ep <= NEWTON_TOL_P and es <= NEWTON_TOL_SW, (step, ep, es)
     else:
         assert ep <= 3 * fp + rtol, (step, "pressure", ep, fp)
         assert es <= 3 * fs + rtol, (step, "sat_water", es, fs)
-    if newton != n0:
-        state["diverged"] = True
