@@ -195,6 +195,22 @@ int64_t rf_kernel_launches(const RfCtx* ctx);
  * enable > 0 switches the profiler on, 0 off, < 0 leaves it as is; reset != 0 zeroes the totals. */
 int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n);
 
+/* ---- Dense pressure solve that allocates nothing.  No counterpart in the reference, where the
+ * dense inverse of a pressure block of at most 299 rows runs inside the preconditioner
+ * (gmres_block_jacobi.rs:903-917); this exposes that solve alone for callers that may not call
+ * cudaMalloc (a host that reserves its device memory up front for its own pool, an embedding
+ * framework that owns the allocator, a loop that must not block on an allocation).
+ * x = A^{-1} b, A dense row-major n x n; a, b and x are device memory owned by the caller; the
+ * call runs on `stream` (a cudaStream_t, NULL for the default stream) and synchronises it before
+ * returning.  n must lie in 1..RF_NOALLOC_MAX_ROWS, otherwise RF_ERR_INVALID; an exactly zero
+ * pivot also returns RF_ERR_INVALID.  Its scratch is one fixed device array of about 1.4 MB that
+ * every GPU loading the library keeps until exit.  The first call on a device looks up that
+ * array's address, so make it before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race.  On failure a message is written to err (may be NULL, err_len bytes). */
+#define RF_NOALLOC_MAX_ROWS 299
+int32_t rf_dense_solve_noalloc(int32_t n, const double* a, const double* b, double* x, void* stream,
+                               char* err, size_t err_len);
+
 /* ---- Ensemble batch (sensitivity variants of uneven sizes); no counterpart in the reference, whose
  * simulator object steps one deck.  Each variant gets its own context (the rf_* calls above work on
  * rf_batch_context(b, i)); rf_batch_step advances every variant by one report step, driving the

@@ -186,3 +186,14 @@ def linear_solve_bsr(sim: ReservoirSimulator, row_ptr, cols, vals, rhs):
     if rc != _abi.RF_OK:
         raise DeviceError(f"rf_linear_solve_bsr failed ({rc}): {_lib.last_error(h)}")
     return x, rep
+
+
+def dense_solve_noalloc(n: int, a_ptr: int, b_ptr: int, x_ptr: int, stream: int = 0) -> None:
+    """x = A^{-1} b through rf_dense_solve_noalloc, for callers that may not allocate device
+    memory.  `a_ptr` (dense row-major n x n), `b_ptr` and `x_ptr` are device addresses of float64
+    data owned by the caller; n <= 299.  The call allocates nothing; calls must not overlap."""
+    err = C.create_string_buffer(256)
+    rc = _lib.load().rf_dense_solve_noalloc(int(n), C.c_void_p(a_ptr), C.c_void_p(b_ptr), C.c_void_p(x_ptr),
+                                            C.c_void_p(stream or None), err, len(err))
+    if rc != _abi.RF_OK:
+        raise DeviceError(f"rf_dense_solve_noalloc failed ({rc}): {err.value.decode(errors='replace')}")
