@@ -881,7 +881,9 @@ static void free_ctx(Ctx& c) {
                   &c.d_perf_well, &c.d_perf_inj, &c.d_perf_has_wi, &c.d_well_ptr, &c.d_well_perfs, &c.d_tinv_off,
                   &c.d_perf_row_off, &c.d_flag_dense, &c.d_dense_perm})
     b->free();
-  for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep}) b->free();
+  for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep, &c.d_pipe_status}) b->free();
+  c.d_reqf.free();
+  c.d_reqb.free();
   for (auto* b : {&c.d_fval, &c.d_bval, &c.d_dval}) b->free();
   for (auto* b : {&c.d_fval32, &c.d_bval32, &c.d_dval32}) b->free();
   for (auto* b : {&c.d_lu32, &c.d_dinv32, &c.d_plu32, &c.d_pval32, &c.d_pdiag32, &c.d_pvec32, &c.d_sweep32})

@@ -959,6 +959,10 @@ struct DsmBicgArgs {
   const T* pdiag;
   PackedSweep<T> fw, bw;
   const T* dval;  // [n] pivots in ownership order
+  // [cs][L][cs]: progress (in positions) CTA b needs from CTA b' before a position, 0 = none
+  const unsigned short* reqf;
+  const unsigned short* reqb;
+  int* status;
   const double* rhs;
   double* x;
   T* r;
@@ -1021,81 +1025,148 @@ __device__ __forceinline__ T packed_subtract(T s, const PackedRow<T>& pr, const 
   return s;
 }
 
-// out = PressureILU(rhs) on slices: forward levels into y_s, backward levels into out_s.  Each
-// thread handles one row per level from data loaded during the previous level's barrier (between
-// arrive and wait, so the loads overlap the barrier); further rows of a wide level and rows with
-// more than kPackK entries take the CSR path.
-template <class T>
-__device__ void dsm_ilu_apply(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr, int base, unsigned me,
-                              const T* rhs, T* y_s, T* out_s) {
-  const int S = a.own.slice, n = a.n, L = a.n_levels, t = threadIdx.x, B = blockDim.x;
-  PackedRow<T> cur, nxt;
-  cur.cnt = -2;
-  if (lptr[0] + t < lptr[1]) {
-    const int q = lptr[0] + t;
-    load_packed(cur, a.fw, n, base + q, lrows[q], rhs, lrows[q]);
-  }
-  for (int l = 0; l < L; ++l) {
-    const int q0 = lptr[l] + t, qe = lptr[l + 1];
-    if (q0 < qe) {
-      if (cur.cnt >= 0) {
-        y_s[cur.r - base] = packed_subtract(cur.extra, cur, y_s, me);
-      } else {
-        const int r = cur.r;
-        T sum = cur.extra;
-        for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
-        y_s[r - base] = sum;
+// Pipelined triangular sweeps on slices.  A CTA walks its own rows in level order ("positions":
+// the levels for the forward sweep, the levels from the top for the backward one), separating
+// its positions with __syncthreads only.  After each position it publishes how far it has got in
+// a progress word in its shared memory (st.release.cluster); before a position it waits, through
+// distributed shared memory (ld.acquire.cluster), only for the CTAs its rows read from, and only
+// up to the position those rows need (a per-CTA table built with the schedule).  A CTA whose
+// inputs are ready runs ahead instead of meeting every other CTA at a barrier each level.
+// Progress words only grow within a launch: sweep number k counts from k * (L + 1).  Every wait
+// is bounded; a wait that gives up sets the status word (2) and marks the CTA so it waits no more,
+// which ends the launch with wrong values that the host then rejects.
+constexpr long long kProgressPollLimit = 1ll << 22;
+
+struct PipeSync {
+  unsigned* prog;         // this CTA's progress word (shared memory)
+  volatile int* abort_s;  // shared: a wait of this CTA gave up
+  int* status;            // global status word, read by the host after the solve
+  unsigned known;         // warp 0, lane j: the last progress value seen from CTA j
+  unsigned epoch;         // progress value at the start of the current sweep
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void publish_progress(unsigned* prog, unsigned v) {
+  asm volatile("st.release.cluster.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(prog)), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned read_progress(unsigned cluster_addr) {
+  unsigned v;
+  asm volatile("ld.acquire.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(cluster_addr) : "memory");
+  return v;
+}
+
+// Warp 0 waits until every CTA that position `pos` of this CTA reads from has published the
+// progress the table asks for; the other threads meet it at the __syncthreads that follows.
+__device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* req_s, int pos, int cs, unsigned me) {
+  const int j = threadIdx.x;
+  if (j < cs && j != int(me) && !*ps.abort_s) {
+    const unsigned need = req_s[pos * cs + j];
+    if (need != 0) {
+      const unsigned target = ps.epoch + need;
+      if (ps.known < target) {
+        unsigned addr;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(smem_u32(ps.prog)), "r"(j));
+        long long polls = 0;
+        while (ps.known < target) {
+          ps.known = read_progress(addr);
+          if (++polls > kProgressPollLimit) {
+            *ps.abort_s = 1;
+            atomicExch(ps.status, 2);
+            break;
+          }
+        }
       }
     }
-    for (int q = q0 + B; q < qe; q += B) {
-      const int r = lrows[q];
-      T sum = rhs[r];
-      for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
-      y_s[r - base] = sum;
-    }
-    cluster_arrive_release();
-    nxt.cnt = -2;
-    if (l + 1 < L && lptr[l + 1] + t < lptr[l + 2]) {
-      const int q = lptr[l + 1] + t;
-      load_packed(nxt, a.fw, n, base + q, lrows[q], rhs, lrows[q]);
-    }
-    cluster_wait_acquire();
-    cur = nxt;
   }
-  cur.cnt = -2;
-  if (lptr[L - 1] + t < lptr[L]) {
-    const int q = lptr[L - 1] + t;
-    load_packed(cur, a.bw, n, base + q, lrows[q], a.dval, base + q);
-  }
-  for (int l = L - 1; l >= 0; --l) {
+  __syncthreads();
+}
+
+template <class T, bool FWD>
+__device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr, const unsigned short* req_s,
+                           int base, unsigned me, int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s) {
+  const int S = a.own.slice, n = a.n, L = a.n_levels, t = threadIdx.x, B = blockDim.x;
+  const PackedSweep<T>& pk = FWD ? a.fw : a.bw;
+  auto level_of = [&](int pos) { return FWD ? pos : L - 1 - pos; };
+  auto empty = [&](int pos) {
+    const int l = level_of(pos);
+    return lptr[l] == lptr[l + 1];
+  };
+  auto prefetch = [&](PackedRow<T>& pr, int pos) {
+    pr.cnt = -2;
+    if (pos >= L) return;
+    const int l = level_of(pos);
+    const int q = lptr[l] + t;
+    if (q < lptr[l + 1]) {
+      if (FWD)
+        load_packed(pr, pk, n, base + q, lrows[q], rhs, lrows[q]);
+      else
+        load_packed(pr, pk, n, base + q, lrows[q], a.dval, base + q);
+    }
+  };
+  int pos = 0;
+  while (pos < L && empty(pos)) ++pos;
+  if (t == 0) publish_progress(ps.prog, ps.epoch + unsigned(pos));
+  PackedRow<T> cur;
+  prefetch(cur, pos);
+  while (pos < L) {
+    wait_inputs(ps, req_s, pos, cs, me);
+    const int l = level_of(pos);
     const int q0 = lptr[l] + t, qe = lptr[l + 1];
     if (q0 < qe) {
       const int r = cur.r;
-      T sum = y_s[r - base];
-      if (cur.cnt >= 0) {
-        sum = packed_subtract(sum, cur, out_s, me);
+      if (FWD) {
+        if (cur.cnt >= 0) {
+          y_s[r - base] = packed_subtract(cur.extra, cur, y_s, me);
+        } else {
+          T sum = cur.extra;
+          for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
+          y_s[r - base] = sum;
+        }
       } else {
-        for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+        T sum = y_s[r - base];
+        if (cur.cnt >= 0) {
+          sum = packed_subtract(sum, cur, out_s, me);
+        } else {
+          for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+        }
+        const T d = cur.extra;
+        out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
       }
-      const T d = cur.extra;
-      out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
     }
     for (int q = q0 + B; q < qe; q += B) {
       const int r = lrows[q];
-      T sum = y_s[r - base];
-      for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
-      const T d = a.pdiag[r];
-      out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
+      if (FWD) {
+        T sum = rhs[r];
+        for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
+        y_s[r - base] = sum;
+      } else {
+        T sum = y_s[r - base];
+        for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+        const T d = a.pdiag[r];
+        out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
+      }
     }
-    cluster_arrive_release();
-    nxt.cnt = -2;
-    if (l > 0 && lptr[l - 1] + t < lptr[l]) {
-      const int q = lptr[l - 1] + t;
-      load_packed(nxt, a.bw, n, base + q, lrows[q], a.dval, base + q);
-    }
-    cluster_wait_acquire();
-    cur = nxt;
+    int next = pos + 1;
+    while (next < L && empty(next)) ++next;
+    __syncthreads();
+    if (t == 0) publish_progress(ps.prog, ps.epoch + unsigned(next));
+    prefetch(cur, next);
+    pos = next;
   }
+  ps.epoch += unsigned(L) + 1u;
+}
+
+// out = PressureILU(rhs) on slices: the pipelined forward sweep into y_s, the pipelined backward
+// sweep into out_s, then one cluster barrier so the SpMV that follows sees all of out_s.
+template <class T>
+__device__ void dsm_ilu_apply(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr,
+                              const unsigned short* reqf_s, const unsigned short* reqb_s, int base, unsigned me,
+                              int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s) {
+  pipe_sweep<T, true>(a, lrows, lptr, reqf_s, base, me, cs, ps, rhs, y_s, out_s);
+  pipe_sweep<T, false>(a, lrows, lptr, reqb_s, base, me, cs, ps, rhs, y_s, out_s);
+  cluster_barrier();
 }
 
 // Values of the packed sweeps after a factorisation (ownership order, column order per row).
@@ -1139,11 +1210,31 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
   T* sh_s = ph_s + S;
   int* lrows = reinterpret_cast<int*>(sh_s + S);
   int* lptr = lrows + S;
+  const int L = a.n_levels;
+  const int cs = int(cluster_nblocks());
+  unsigned short* reqf_s = reinterpret_cast<unsigned short*>(lptr + L + 1);
+  unsigned short* reqb_s = reqf_s + size_t(L) * cs;
+  __shared__ unsigned s_prog;
+  __shared__ int s_abort;
   const unsigned me = cluster_rank();
   const int base = int(me) * S;
   const int cnt = max(0, min(S, n - base));
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) lrows[i] = a.own.rows[base + i];
-  for (int l = threadIdx.x; l <= a.n_levels; l += blockDim.x) lptr[l] = a.own.ptr[size_t(me) * (a.n_levels + 1) + l];
+  for (int l = threadIdx.x; l <= L; l += blockDim.x) lptr[l] = a.own.ptr[size_t(me) * (L + 1) + l];
+  for (int i = threadIdx.x; i < L * cs; i += blockDim.x) {
+    reqf_s[i] = a.reqf[size_t(me) * L * cs + i];
+    reqb_s[i] = a.reqb[size_t(me) * L * cs + i];
+  }
+  if (threadIdx.x == 0) {
+    s_prog = 0;
+    s_abort = 0;
+  }
+  PipeSync ps;
+  ps.prog = &s_prog;
+  ps.abort_s = &s_abort;
+  ps.status = a.status;
+  ps.known = 0;
+  ps.epoch = 0;
   double v3[3], o3[3];
   int parity = 0;
   v3[0] = 0.0;
@@ -1178,7 +1269,7 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
         a.p[i] = T(double(a.r[i]) + beta * (double(a.p[i]) - omega * double(a.v[i])));
     }
     __syncthreads();
-    dsm_ilu_apply(a, lrows, lptr, base, me, a.p, y_s, ph_s);
+    dsm_ilu_apply(a, lrows, lptr, reqf_s, reqb_s, base, me, cs, ps, a.p, y_s, ph_s);
     dsm_spmv(a, base, cnt, me, ph_s, a.v);
     v3[0] = 0.0;
     for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) v3[0] += double(a.rh[i]) * double(a.v[i]);
@@ -1197,7 +1288,7 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
       for (int i = threadIdx.x; i < cnt; i += blockDim.x) a.x[base + i] += alpha * double(ph_s[i]);
       break;
     }
-    dsm_ilu_apply(a, lrows, lptr, base, me, a.s, y_s, sh_s);
+    dsm_ilu_apply(a, lrows, lptr, reqf_s, reqb_s, base, me, cs, ps, a.s, y_s, sh_s);
     dsm_spmv(a, base, cnt, me, sh_s, a.t);
     v3[0] = 0.0;
     v3[1] = 0.0;
@@ -1500,6 +1591,9 @@ static bool launch_bicgstab_dsmem(Ctx& c, const T* pval, const T* plu, const T* 
   a.pval = pval;
   a.plu = plu;
   a.pdiag = pdiag;
+  a.reqf = c.d_reqf.p;
+  a.reqb = c.d_reqb.p;
+  a.status = c.d_pipe_status.p;
   a.fw.cnt = c.d_fcnt.p;
   a.fw.dep = c.d_fdep.p;
   a.bw.cnt = c.d_bcnt.p;
@@ -1733,6 +1827,12 @@ LinResult linear_solve_reduced(Ctx& c) {
     }
   }
   RF_CUDA(cudaGetLastError());
+  if (c.d_pipe_status.p) {
+    int st = 0;
+    RF_CUDA(cudaMemcpyAsync(&st, c.d_pipe_status.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    if (st != 0) throw CudaError("device status " + std::to_string(st) + ": a pressure-sweep wait gave up");
+  }
   return out;
 }
 
@@ -1915,8 +2015,37 @@ static void build_owned_levels(Ctx& c) {
       if (j < bcnt[g]) bdep[size_t(j) * n + g] = packdep(c.h_col[d + 1 + j]);
     }
   }
+  // progress tables of the pipelined sweeps: before position p (forward: level p; backward:
+  // level L-1-p) CTA b needs, from each other CTA b', every position that holds a column its rows
+  // at that level read, i.e. progress >= (forward) level(col) + 1 or (backward) L - level(col)
+  std::vector<unsigned short> reqf(size_t(cs) * L * cs, 0), reqb(size_t(cs) * L * cs, 0);
+  bool req_fits = L + 1 <= 65535;
+  for (int r = 0; r < n && req_fits; ++r) {
+    const int b = r / S, l = lvl[r];
+    for (int k = c.h_row_ptr[r]; k < c.h_row_ptr[r + 1]; ++k) {
+      const int col = c.h_col[k], ob = col / S;
+      if (ob == b || col == r) continue;
+      if (k < c.h_diag[r]) {
+        unsigned short& q = reqf[(size_t(b) * L + l) * cs + ob];
+        q = std::max<unsigned short>(q, static_cast<unsigned short>(lvl[col] + 1));
+      } else {
+        unsigned short& q = reqb[(size_t(b) * L + (L - 1 - l)) * cs + ob];
+        q = std::max<unsigned short>(q, static_cast<unsigned short>(L - lvl[col]));
+      }
+    }
+  }
   c.own_slice = S;
   for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep}) b->free();
+  c.d_reqf.free();
+  c.d_reqb.free();
+  c.d_reqf.alloc(reqf.size());
+  c.d_reqb.alloc(reqb.size());
+  RF_CUDA(cudaMemcpy(c.d_reqf.p, reqf.data(), sizeof(unsigned short) * reqf.size(), cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.d_reqb.p, reqb.data(), sizeof(unsigned short) * reqb.size(), cudaMemcpyHostToDevice));
+  if (c.d_pipe_status.p == nullptr) {
+    c.d_pipe_status.alloc(1);
+    RF_CUDA(cudaMemset(c.d_pipe_status.p, 0, sizeof(int)));
+  }
   c.d_own_rows.alloc(n);
   c.d_own_ptr.alloc(ptr.size());
   c.d_fcnt.alloc(n);
@@ -1947,8 +2076,9 @@ static void build_owned_levels(Ctx& c) {
     c.dsm_bytes[f] = 0;
     cudaFuncAttributes fa;
     RF_CUDA(cudaFuncGetAttributes(&fa, fns[f]));
-    const size_t bytes = 3 * size_t(S) * tsz[f] + sizeof(int) * (size_t(S) + L + 1);
-    if (bytes + fa.sharedSizeBytes > size_t(optin)) continue;
+    const size_t bytes = 3 * size_t(S) * tsz[f] + sizeof(int) * (size_t(S) + L + 1) +
+                         2 * sizeof(unsigned short) * size_t(L) * cs;
+    if (!req_fits || bytes + fa.sharedSizeBytes > size_t(optin)) continue;
     RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
     if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
