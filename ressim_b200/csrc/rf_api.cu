@@ -884,6 +884,7 @@ static void free_ctx(Ctx& c) {
   for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep, &c.d_pipe_status}) b->free();
   c.d_reqf.free();
   c.d_reqb.free();
+  c.d_cons.free();
   for (auto* b : {&c.d_fval, &c.d_bval, &c.d_dval}) b->free();
   for (auto* b : {&c.d_fval32, &c.d_bval32, &c.d_dval32}) b->free();
   for (auto* b : {&c.d_lu32, &c.d_dinv32, &c.d_plu32, &c.d_pval32, &c.d_pdiag32, &c.d_pvec32, &c.d_sweep32})

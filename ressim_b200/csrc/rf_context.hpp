@@ -131,6 +131,7 @@ struct Ctx {
   DBuf<int> d_own_rows, d_own_ptr;
   DBuf<int> d_fcnt, d_bcnt, d_fdep, d_bdep;  // packed sweep structure (ownership order)
   DBuf<unsigned short> d_reqf, d_reqb;       // per-CTA, per-position progress needed from each CTA
+  DBuf<unsigned> d_cons;                     // [2][cs] consumer masks of the forward / backward sweeps
   DBuf<int> d_pipe_status;                   // nonzero: a pipelined sweep's bounded wait gave up
   DBuf<double> d_fval, d_bval, d_dval;       // packed factor values, FP64
   DBuf<float> d_fval32, d_bval32, d_dval32;  // packed factor values, mixed form

@@ -962,6 +962,8 @@ struct DsmBicgArgs {
   // [cs][L][cs]: progress (in positions) CTA b needs from CTA b' before a position, 0 = none
   const unsigned short* reqf;
   const unsigned short* reqb;
+  const unsigned* cons_f;  // [cs]: bit j set when CTA j reads this CTA's rows in the forward sweep
+  const unsigned* cons_b;  // [cs]: the same for the backward sweep
   int* status;
   const double* rhs;
   double* x;
@@ -1027,37 +1029,46 @@ __device__ __forceinline__ T packed_subtract(T s, const PackedRow<T>& pr, const 
 
 // Pipelined triangular sweeps on slices.  A CTA walks its own rows in level order ("positions":
 // the levels for the forward sweep, the levels from the top for the backward one), separating
-// its positions with __syncthreads only.  After each position it publishes how far it has got in
-// a progress word in its shared memory (st.release.cluster); before a position it waits, through
-// distributed shared memory (ld.acquire.cluster), only for the CTAs its rows read from, and only
-// up to the position those rows need (a per-CTA table built with the schedule).  A CTA whose
-// inputs are ready runs ahead instead of meeting every other CTA at a barrier each level.
-// Progress words only grow within a launch: sweep number k counts from k * (L + 1).  Every wait
+// its positions with __syncthreads only.  After each position it pushes how far it has got into
+// an inbox word in the shared memory of each CTA that reads its rows (st.release.cluster to
+// distributed shared memory); before a position it waits on its own inbox (ld.acquire.cluster on
+// local shared memory) for the CTAs its rows read from, up to the position those rows need (a
+// per-CTA table built with the schedule).  A CTA whose inputs are ready runs ahead instead of
+// meeting every other CTA at a barrier each level, and the waits poll on-chip local memory.
+// Progress values only grow within a launch: sweep number k counts from k * (L + 1).  Every wait
 // is bounded; a wait that gives up sets the status word (2) and marks the CTA so it waits no more,
 // which ends the launch with wrong values that the host then rejects.
-constexpr long long kProgressPollLimit = 1ll << 22;
+constexpr long long kProgressPollLimit = 1ll << 24;
 
 struct PipeSync {
-  unsigned* prog;         // this CTA's progress word (shared memory)
+  unsigned* inbox;        // [cs] in this CTA's shared memory: progress pushed by each producer
   volatile int* abort_s;  // shared: a wait of this CTA gave up
   int* status;            // global status word, read by the host after the solve
-  unsigned known;         // warp 0, lane j: the last progress value seen from CTA j
   unsigned epoch;         // progress value at the start of the current sweep
+  unsigned cons_f, cons_b;  // CTAs that read this CTA's rows in the forward / backward sweep
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void publish_progress(unsigned* prog, unsigned v) {
-  asm volatile("st.release.cluster.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(prog)), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned read_progress(unsigned cluster_addr) {
+__device__ __forceinline__ unsigned read_inbox(const unsigned* p) {
   unsigned v;
-  asm volatile("ld.acquire.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(cluster_addr) : "memory");
+  asm volatile("ld.acquire.cluster.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
   return v;
 }
 
-// Warp 0 waits until every CTA that position `pos` of this CTA reads from has published the
+// Warp 0, lane j: push `value` into inbox[me] of consumer CTA j (after the CTA's rows of this
+// position are written and a __syncthreads has ordered them before this store).
+__device__ __forceinline__ void push_progress(const PipeSync& ps, unsigned consumers, unsigned me, unsigned value) {
+  const unsigned j = threadIdx.x;
+  if (j < 32 && ((consumers >> j) & 1u)) {
+    unsigned addr;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(smem_u32(ps.inbox + me)), "r"(j));
+    asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(value) : "memory");
+  }
+}
+
+// Warp 0 waits until every CTA that position `pos` of this CTA reads from has pushed the
 // progress the table asks for; the other threads meet it at the __syncthreads that follows.
 __device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* req_s, int pos, int cs, unsigned me) {
   const int j = threadIdx.x;
@@ -1065,17 +1076,12 @@ __device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* 
     const unsigned need = req_s[pos * cs + j];
     if (need != 0) {
       const unsigned target = ps.epoch + need;
-      if (ps.known < target) {
-        unsigned addr;
-        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(smem_u32(ps.prog)), "r"(j));
-        long long polls = 0;
-        while (ps.known < target) {
-          ps.known = read_progress(addr);
-          if (++polls > kProgressPollLimit) {
-            *ps.abort_s = 1;
-            atomicExch(ps.status, 2);
-            break;
-          }
+      long long polls = 0;
+      while (read_inbox(ps.inbox + j) < target) {
+        if (++polls > kProgressPollLimit) {
+          *ps.abort_s = 1;
+          atomicExch(ps.status, 2);
+          break;
         }
       }
     }
@@ -1105,9 +1111,10 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
         load_packed(pr, pk, n, base + q, lrows[q], a.dval, base + q);
     }
   };
+  const unsigned consumers = FWD ? ps.cons_f : ps.cons_b;
   int pos = 0;
   while (pos < L && empty(pos)) ++pos;
-  if (t == 0) publish_progress(ps.prog, ps.epoch + unsigned(pos));
+  push_progress(ps, consumers, me, ps.epoch + unsigned(pos));
   PackedRow<T> cur;
   prefetch(cur, pos);
   while (pos < L) {
@@ -1151,7 +1158,7 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
     int next = pos + 1;
     while (next < L && empty(next)) ++next;
     __syncthreads();
-    if (t == 0) publish_progress(ps.prog, ps.epoch + unsigned(next));
+    push_progress(ps, consumers, me, ps.epoch + unsigned(next));
     prefetch(cur, next);
     pos = next;
   }
@@ -1214,7 +1221,7 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
   const int cs = int(cluster_nblocks());
   unsigned short* reqf_s = reinterpret_cast<unsigned short*>(lptr + L + 1);
   unsigned short* reqb_s = reqf_s + size_t(L) * cs;
-  __shared__ unsigned s_prog;
+  __shared__ unsigned s_inbox[16];
   __shared__ int s_abort;
   const unsigned me = cluster_rank();
   const int base = int(me) * S;
@@ -1225,16 +1232,15 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
     reqf_s[i] = a.reqf[size_t(me) * L * cs + i];
     reqb_s[i] = a.reqb[size_t(me) * L * cs + i];
   }
-  if (threadIdx.x == 0) {
-    s_prog = 0;
-    s_abort = 0;
-  }
+  if (threadIdx.x < 16) s_inbox[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_abort = 0;
   PipeSync ps;
-  ps.prog = &s_prog;
+  ps.inbox = s_inbox;
   ps.abort_s = &s_abort;
   ps.status = a.status;
-  ps.known = 0;
   ps.epoch = 0;
+  ps.cons_f = a.cons_f[me];
+  ps.cons_b = a.cons_b[me];
   double v3[3], o3[3];
   int parity = 0;
   v3[0] = 0.0;
@@ -1593,6 +1599,8 @@ static bool launch_bicgstab_dsmem(Ctx& c, const T* pval, const T* plu, const T* 
   a.pdiag = pdiag;
   a.reqf = c.d_reqf.p;
   a.reqb = c.d_reqb.p;
+  a.cons_f = c.d_cons.p;
+  a.cons_b = c.d_cons.p + c.cluster_size;
   a.status = c.d_pipe_status.p;
   a.fw.cnt = c.d_fcnt.p;
   a.fw.dep = c.d_fdep.p;
@@ -2036,6 +2044,17 @@ static void build_owned_levels(Ctx& c) {
   }
   c.own_slice = S;
   for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep}) b->free();
+  // consumers of each CTA: the CTAs whose progress tables wait on it
+  std::vector<unsigned> cons(2 * size_t(cs), 0u);
+  for (int b = 0; b < cs; ++b)
+    for (int p = 0; p < L; ++p)
+      for (int ob = 0; ob < cs; ++ob) {
+        if (reqf[(size_t(b) * L + p) * cs + ob]) cons[ob] |= 1u << b;
+        if (reqb[(size_t(b) * L + p) * cs + ob]) cons[cs + ob] |= 1u << b;
+      }
+  c.d_cons.free();
+  c.d_cons.alloc(cons.size());
+  RF_CUDA(cudaMemcpy(c.d_cons.p, cons.data(), sizeof(unsigned) * cons.size(), cudaMemcpyHostToDevice));
   c.d_reqf.free();
   c.d_reqb.free();
   c.d_reqf.alloc(reqf.size());
