@@ -910,12 +910,15 @@ __device__ __forceinline__ unsigned cluster_rank() {
   asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(v));
   return v;
 }
+// Remote shared-memory loads.  They carry no "memory" clobber, so the compiler may overlap them
+// with other loads; they stay ordered against the barriers and progress waits, which are volatile
+// asm statements with a memory clobber.
 __device__ __forceinline__ double dsm_load(const double* p, unsigned rank) {
   const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
   unsigned r;
   double v;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
-  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r) : "memory");
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r));
   return v;
 }
 __device__ __forceinline__ float dsm_load(const float* p, unsigned rank) {
@@ -923,7 +926,7 @@ __device__ __forceinline__ float dsm_load(const float* p, unsigned rank) {
   unsigned r;
   float v;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
-  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(r) : "memory");
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(r));
   return v;
 }
 // element `idx` of a slice-distributed vector whose local slice starts at `local`
@@ -946,6 +949,46 @@ struct PackedSweep {
   const int* dep;  // [kPackK][n]
   const T* val;    // [kPackK][n]
 };
+
+// sum -= plu[k] * src[col[k]] for k in [k0, k1), in k order, with the loads of each batch of
+// eight entries issued together (rows of a well's clique have up to ~20 entries)
+template <class T>
+__device__ __noinline__ T csr_subtract(T sum, int k0, int k1, const int* col, const T* val, const T* src, int slice,
+                                       unsigned me) {
+  for (int k = k0; k < k1; k += 8) {
+    T v[8], d[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (k + j < k1) {
+        v[j] = val[k + j];
+        d[j] = slice_read(src, col[k + j], slice, me);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (k + j < k1) sum -= v[j] * d[j];
+  }
+  return sum;
+}
+template <class T>
+__device__ __forceinline__ T csr_dot(int k0, int k1, const int* col, const T* val, const T* src, int slice,
+                                     unsigned me) {
+  T s = T(0);
+  for (int k = k0; k < k1; k += 8) {
+    T v[8], d[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (k + j < k1) {
+        v[j] = val[k + j];
+        d[j] = slice_read(src, col[k + j], slice, me);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (k + j < k1) s += v[j] * d[j];
+  }
+  return s;
+}
 
 template <class T>
 struct DsmBicgArgs {
@@ -1127,17 +1170,14 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
         if (cur.cnt >= 0) {
           y_s[r - base] = packed_subtract(cur.extra, cur, y_s, me);
         } else {
-          T sum = cur.extra;
-          for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
-          y_s[r - base] = sum;
+          y_s[r - base] = csr_subtract(cur.extra, a.rp[r], a.diag[r], a.col, a.plu, y_s, S, me);
         }
       } else {
         T sum = y_s[r - base];
-        if (cur.cnt >= 0) {
+        if (cur.cnt >= 0)
           sum = packed_subtract(sum, cur, out_s, me);
-        } else {
-          for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
-        }
+        else
+          sum = csr_subtract(sum, a.diag[r] + 1, a.rp[r + 1], a.col, a.plu, out_s, S, me);
         const T d = cur.extra;
         out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
       }
@@ -1145,12 +1185,9 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
     for (int q = q0 + B; q < qe; q += B) {
       const int r = lrows[q];
       if (FWD) {
-        T sum = rhs[r];
-        for (int k = a.rp[r]; k < a.diag[r]; ++k) sum -= a.plu[k] * slice_read(y_s, a.col[k], S, me);
-        y_s[r - base] = sum;
+        y_s[r - base] = csr_subtract(rhs[r], a.rp[r], a.diag[r], a.col, a.plu, y_s, S, me);
       } else {
-        T sum = y_s[r - base];
-        for (int k = a.diag[r] + 1; k < a.rp[r + 1]; ++k) sum -= a.plu[k] * slice_read(out_s, a.col[k], S, me);
+        const T sum = csr_subtract(y_s[r - base], a.diag[r] + 1, a.rp[r + 1], a.col, a.plu, out_s, S, me);
         const T d = a.pdiag[r];
         out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
       }
@@ -1200,9 +1237,7 @@ __device__ __forceinline__ void dsm_spmv(const DsmBicgArgs<T>& a, int base, int 
   const int S = a.own.slice;
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
     const int r = base + i;
-    T s = T(0);
-    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) s += a.pval[k] * slice_read(in_s, a.col[k], S, me);
-    out[r] = s;
+    out[r] = csr_dot(a.rp[r], a.rp[r + 1], a.col, a.pval, in_s, S, me);
   }
 }
 
