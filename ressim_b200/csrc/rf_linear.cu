@@ -20,6 +20,7 @@
 // fill.  Pressure-matrix entries with |v| <= 1e-14 are dropped, as the reference does.
 
 #include <algorithm>
+#include <mutex>
 #include <cstdio>
 
 #include "rf_ops.hpp"
@@ -2026,6 +2027,18 @@ int auto_cluster_size(const Ctx& c) {
   return want;
 }
 
+// Dynamic shared memory limits are attributes of a kernel, shared by every context in the process:
+// only ever raise them, so a context created later with smaller needs cannot undercut an earlier
+// one's launches.
+static void raise_dynamic_smem(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  cudaFuncAttributes fa;
+  RF_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if (size_t(fa.maxDynamicSharedSizeBytes) < bytes)
+    RF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
 // Slice ownership for the distributed-shared-memory BiCGStab at the current cluster size: CTA b
 // owns rows [b*S, b*S + S), listed in level order (ties in row order), with per-CTA level
 // pointers.  Records, per value type, the dynamic shared memory the kernel needs, or 0 when the
@@ -2133,7 +2146,7 @@ static void build_owned_levels(Ctx& c) {
     const size_t bytes = 3 * size_t(S) * tsz[f] + sizeof(int) * (size_t(S) + L + 1) +
                          2 * sizeof(unsigned short) * size_t(L) * cs;
     if (!req_fits || bytes + fa.sharedSizeBytes > size_t(optin)) continue;
-    RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    raise_dynamic_smem(fns[f], bytes);
     if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cs);
@@ -2241,7 +2254,7 @@ void setup_linear_workspace(Ctx& c) {
   set_cluster_size(c, auto_cluster_size(c));
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
-  if (smem > 48 * 1024) RF_CUDA(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (smem > 48 * 1024) raise_dynamic_smem((const void*)k_schur, smem);
 }
 
 }  // namespace rf

@@ -51,7 +51,8 @@ class Ensemble:
         reps = (_abi.RfStepReport * n)()
         rc = _lib.load().rf_batch_step(self._h, float(target_dt_days), reps)
         if rc < 0:
-            raise DeviceError(f"rf_batch_step failed ({rc})")
+            msgs = [f"variant {i}: {m}" for i, m in ((i, _lib.last_error(c)) for i, c in enumerate(self._ctx)) if m]
+            raise DeviceError(f"rf_batch_step failed ({rc}): " + "; ".join(msgs[:3]))
         return [r.as_dict() for r in reps]
 
     def state(self, i: int) -> dict:

@@ -39,3 +39,13 @@ def test_batch_variant_matches_oracle():
         g = ens.state(0)
         check_within_floor(s, g["pressure"], g["sat_water"], reps[0]["newton_iterations"], runs, state=state)
     ens.close()
+
+
+def test_batch_with_larger_variant_created_first():
+    """Contexts created later with smaller shared-memory needs must not break the launches of a
+    larger context created before them (kernel launch limits are process-wide)."""
+    ds = [decks.ensemble_variant(i) for i in (206, 142)]  # 4,050 then 3,300 cells
+    ens = Ensemble(ds, host_threads=2)
+    reps = ens.step(10.0)
+    assert all(r["newton_iterations"] > 0 for r in reps)
+    ens.close()
