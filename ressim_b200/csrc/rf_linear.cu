@@ -2015,16 +2015,25 @@ void build_levels(Ctx& c) {
                      cudaMemcpyHostToDevice));
 }
 
-// Automatic cluster size: the smallest power of two (<= 16) whose slices hold at most 4608 rows,
-// so the distributed-shared-memory BiCGStab applies, and at least enough 1024-thread CTAs to give
-// every row of the widest level its own thread.
+// Automatic cluster size: the smallest power of two (<= 16) whose slices fit the FP64
+// distributed-shared-memory BiCGStab (three vectors, the row list and the level and progress
+// tables per CTA) and that gives every row of the widest level its own thread in the
+// global-memory kernels (1024 threads per CTA); 16 when no size fits.  Fewer CTAs per cluster
+// leave more SMs to other work, which matters when many decks run at once.
 int auto_cluster_size(const Ctx& c) {
   int widest = 1;
   for (int l = 0; l < c.levels.n_levels; ++l)
     widest = std::max(widest, c.levels.h_ptr[l + 1] - c.levels.h_ptr[l]);
-  int want = 1;
-  while (want < 16 && ((c.n + want - 1) / want > 4608 || want * kCBlock < widest)) want *= 2;
-  return want;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device) != cudaSuccess) optin = 0;
+  const size_t budget = optin > 4096 ? size_t(optin) - 4096 : 0;  // static shared memory and slack
+  const size_t L = size_t(c.levels.n_levels);
+  for (int cs = 1; cs <= 16; cs *= 2) {
+    const size_t S = (size_t(c.n) + cs - 1) / cs;
+    const size_t bytes = 3 * S * sizeof(double) + sizeof(int) * (S + L + 1) + 2 * sizeof(unsigned short) * L * cs;
+    if (bytes <= budget && cs * kCBlock >= widest) return cs;
+  }
+  return 16;
 }
 
 // Dynamic shared memory limits are attributes of a kernel, shared by every context in the process:
