@@ -247,8 +247,8 @@ static void tail_norms(Ctx& c, const WellState& ws, FamNorms& fam) {
   const int W = c.topo.n_wells, P = c.topo.n_perfs;
   if (W + P == 0) return;
   std::vector<double> rt(W + P);
-  RF_CUDA(cudaMemcpyAsync(rt.data(), c.d_res_tail.p, sizeof(double) * rt.size(), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, rt.data(), c.d_res_tail.p, sizeof(double) * rt.size());
+  d2h_wait(c);
   double fw = 0.0, fp = 0.0;
   for (int w = 0; w < W; ++w) {
     const WellControlH k = well_control(c, w);
@@ -807,6 +807,9 @@ static void setup_device(Ctx& c) {
   RF_CUDA(cudaGetDevice(&c.device));
   RF_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device));
   RF_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  c.h_pin_bytes = sizeof(double) * (16 * size_t(c.topo.n_wells + c.topo.n_perfs) + 4096);
+  RF_CUDA(cudaMallocHost(&c.h_pin, c.h_pin_bytes));
+  c.pin_pending.reserve(64);
   RF_CUDA(cudaEventCreate(&c.ev0));
   RF_CUDA(cudaEventCreate(&c.ev1));
   const int n = c.n, nx = c.nx, ny = c.ny, nz = c.nz, nxy = nx * ny;
@@ -899,6 +902,8 @@ static void free_ctx(Ctx& c) {
   c.d_bicg_iters = nullptr;
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
+  if (c.h_pin) cudaFreeHost(c.h_pin);
+  c.h_pin = nullptr;
   if (c.stream) cudaStreamDestroy(c.stream);
 }
 

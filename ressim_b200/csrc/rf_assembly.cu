@@ -361,8 +361,8 @@ void launch_norms(Ctx& c, double dt, double* h_out /* kNormQ + 1 */) {
   k_cnv_violation<<<nb, kBlock, 0, c.stream>>>(n, c.d_pv.p, c.d_res.p, c.d_scal.p, c.d_partials.p);
   k_sum_final<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, c.d_scal.p + kNormQ);
   c.launches += 4;
-  RF_CUDA(cudaMemcpyAsync(h_out, c.d_scal.p, sizeof(double) * (kNormQ + 1), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, h_out, c.d_scal.p, sizeof(double) * (kNormQ + 1));
+  d2h_wait(c);
 }
 
 }  // namespace rf

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <cstring>
 #include <vector>
 
 #include "../../include/ressim_fim.h"
@@ -124,6 +125,15 @@ struct Ctx {
   int dense_ok = 0;
   DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
   DBuf<double> d_partials, d_scal;
+  // pinned staging for the step path's small device-to-host readbacks (d2h / d2h_wait below):
+  // pageable copies stage through the driver and serialise when many contexts step at once
+  unsigned char* h_pin = nullptr;
+  size_t h_pin_bytes = 0, h_pin_used = 0;
+  struct PinCopy {
+    void* dst;
+    size_t off, bytes;
+  };
+  std::vector<PinCopy> pin_pending;
   int cluster_size = 0;  // CTAs in the one cluster that runs the level-scheduled kernels
   // slice ownership schedule of the distributed-shared-memory BiCGStab (built for cluster_size)
   int own_slice = 0;
@@ -151,6 +161,31 @@ struct Ctx {
   long long phase_count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   long long* d_bicg_iters = nullptr;  // device counter of BiCGStab iterations
 };
+
+// Queue a device-to-host copy through the context's pinned staging buffer; the bytes reach `dst`
+// at the next d2h_wait.  A copy larger than the buffer goes directly (and synchronously).
+inline void d2h_wait(Ctx& c);
+inline void d2h(Ctx& c, void* dst, const void* src, size_t bytes) {
+  if (c.h_pin == nullptr || bytes > c.h_pin_bytes) {
+    RF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+    return;
+  }
+  size_t off = (c.h_pin_used + 15) & ~size_t(15);
+  if (off + bytes > c.h_pin_bytes) {
+    d2h_wait(c);
+    off = 0;
+  }
+  RF_CUDA(cudaMemcpyAsync(c.h_pin + off, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+  c.pin_pending.push_back({dst, off, bytes});
+  c.h_pin_used = off + bytes;
+}
+// Synchronise the context's stream and deliver the queued readbacks.
+inline void d2h_wait(Ctx& c) {
+  RF_CUDA(cudaStreamSynchronize(c.stream));
+  for (const auto& q : c.pin_pending) std::memcpy(q.dst, c.h_pin + q.off, q.bytes);
+  c.pin_pending.clear();
+  c.h_pin_used = 0;
+}
 
 // Phases of one Newton iteration reported by rf_profile.
 enum Phase {

@@ -1609,8 +1609,8 @@ static void cpr_build(Ctx& c) {
     k_dense_invert<<<1, 1024, 0, c.stream>>>(n, c.d_tmp2.p, c.d_dense.p, c.d_dense_perm.p, c.d_flag_dense.p);
     c.launches += 2;
     int ok = 0;
-    RF_CUDA(cudaMemcpyAsync(&ok, c.d_flag_dense.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
+    d2h(c, &ok, c.d_flag_dense.p, sizeof(int));
+    d2h_wait(c);
     c.dense_ok = ok;
   }
 }
@@ -1776,8 +1776,8 @@ LinResult linear_solve_reduced(Ctx& c) {
   cpr_build(c);
   dot_dev(c, n3, b, nullptr, c.d_scal.p + 21, true);
   double rhs_norm = 0.0;
-  RF_CUDA(cudaMemcpyAsync(&rhs_norm, c.d_scal.p + 21, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, &rhs_norm, c.d_scal.p + 21, sizeof(double));
+  d2h_wait(c);
   out.rhs_norm = rhs_norm;
   const double tol = 1e-12 + 5e-3 * fmax(rhs_norm, kEps);
   // x0 = 0: r = b - A*0, computed explicitly as the reference does
@@ -1785,8 +1785,8 @@ LinResult linear_solve_reduced(Ctx& c) {
   spmv_res(c, c.d_x.p, b, c.d_cres.p);
   dot_dev(c, n3, c.d_cres.p, nullptr, c.d_scal.p + 22, true);
   double rn = 0.0;
-  RF_CUDA(cudaMemcpyAsync(&rn, c.d_scal.p + 22, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, &rn, c.d_scal.p + 22, sizeof(double));
+  d2h_wait(c);
   if (rn <= tol) {
     out.converged = true;
     out.iterations = 0;
@@ -1814,8 +1814,8 @@ LinResult linear_solve_reduced(Ctx& c) {
       c.launches++;
     }
     dot_dev(c, n3, w, nullptr, hbuf + j + 1, true);
-    RF_CUDA(cudaMemcpyAsync(hcol.data(), hbuf, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
+    d2h(c, hcol.data(), hbuf, sizeof(double) * (j + 2));
+    d2h_wait(c);
     const double nn = hcol[j + 1];
     auto Hc = [&](int r, int cc) -> double& { return H[size_t(r) * R + cc]; };
     for (int p = 0; p <= j + 1; ++p) Hc(p, j) = hcol[p];
@@ -1855,8 +1855,8 @@ LinResult linear_solve_reduced(Ctx& c) {
     dot_dev(c, n3, c.d_cres.p, nullptr, c.d_scal.p + 23, true);
     c.launches++;
     double trn = 0.0;
-    RF_CUDA(cudaMemcpyAsync(&trn, c.d_scal.p + 23, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
+    d2h(c, &trn, c.d_scal.p + 23, sizeof(double));
+    d2h_wait(c);
     if (trn <= tol) {
       out.converged = true;
       out.iterations = iters;
@@ -1873,8 +1873,8 @@ LinResult linear_solve_reduced(Ctx& c) {
   RF_CUDA(cudaGetLastError());
   if (c.d_pipe_status.p) {
     int st = 0;
-    RF_CUDA(cudaMemcpyAsync(&st, c.d_pipe_status.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
+    d2h(c, &st, c.d_pipe_status.p, sizeof(int));
+    d2h_wait(c);
     if (st != 0) throw CudaError("device status " + std::to_string(st) + ": a pressure-sweep wait gave up");
   }
   return out;
@@ -1951,30 +1951,29 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
     r.tail_sq = c.d_scal.p + 4096;
     k_recover<<<W, 32, 0, c.stream>>>(r);
     c.launches++;
-    RF_CUDA(cudaMemcpyAsync(h_dx_tail.data(), c.d_dx_tail.p, sizeof(double) * h_dx_tail.size(),
-                            cudaMemcpyDeviceToHost, c.stream));
+    d2h(c, h_dx_tail.data(), c.d_dx_tail.p, sizeof(double) * h_dx_tail.size());
     std::vector<double> tsq(W);
-    RF_CUDA(cudaMemcpyAsync(tsq.data(), c.d_scal.p + 4096, sizeof(double) * W, cudaMemcpyDeviceToHost, c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
+    d2h(c, tsq.data(), c.d_scal.p + 4096, sizeof(double) * W);
+    d2h_wait(c);
     for (double v : tsq) tail_sq_sum += v;
   }
   dot_dev(c, n3, c.d_full.p, nullptr, c.d_scal.p + 24, false);
   double sq = 0.0;
-  RF_CUDA(cudaMemcpyAsync(&sq, c.d_scal.p + 24, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  d2h(c, &sq, c.d_scal.p + 24, sizeof(double));
   // rhs norm of the full system: |[-res; -res_tail]|
   dot_dev(c, n3, c.d_res.p, nullptr, c.d_scal.p + 25, false);
   double rsq = 0.0;
-  RF_CUDA(cudaMemcpyAsync(&rsq, c.d_scal.p + 25, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  d2h(c, &rsq, c.d_scal.p + 25, sizeof(double));
   std::vector<double> rt(size_t(W) + c.topo.n_perfs);
   if (!rt.empty())
-    RF_CUDA(cudaMemcpyAsync(rt.data(), c.d_res_tail.p, sizeof(double) * rt.size(), cudaMemcpyDeviceToHost, c.stream));
+    d2h(c, rt.data(), c.d_res_tail.p, sizeof(double) * rt.size());
   // finiteness of the solution
   RF_CUDA(cudaMemsetAsync(c.d_flag_dense.p + 1, 0, sizeof(int), c.stream));
   k_count_nonfinite<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_x.p, c.d_flag_dense.p + 1);
   c.launches++;
   int nonfinite = 0;
-  RF_CUDA(cudaMemcpyAsync(&nonfinite, c.d_flag_dense.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, &nonfinite, c.d_flag_dense.p + 1, sizeof(int));
+  d2h_wait(c);
   for (double v : rt) rsq += v * v;
   for (double v : h_dx_tail)
     if (!std::isfinite(v)) nonfinite = 1;

@@ -128,8 +128,8 @@ void apply_cell_update(Ctx& c, double relax, double& pmax, bool& finite) {
   k_max2_final<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, c.d_scal.p + 200);
   c.launches += 2;
   double h[2];
-  RF_CUDA(cudaMemcpyAsync(h, c.d_scal.p + 200, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, h, c.d_scal.p + 200, sizeof(h));
+  d2h_wait(c);
   pmax = h[0];
   finite = h[1] == 0.0;
 }
@@ -140,8 +140,8 @@ void state_sums(Ctx& c, const double* ap, const double* asw, const double* ahc, 
   k_state_sums<<<nb, kBlock, 0, c.stream>>>(c.fluid, c.n, c.d_pv.p, ap, asw, ahc, bp, bsw, bhc, c.d_partials.p);
   k_state_final<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, c.d_scal.p + 210);
   c.launches += 2;
-  RF_CUDA(cudaMemcpyAsync(out, c.d_scal.p + 210, sizeof(double) * kStateQ, cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, out, c.d_scal.p + 210, sizeof(double) * kStateQ);
+  d2h_wait(c);
 }
 
 void gather_perf_cells(Ctx& c, const double* p, const double* sw, const double* hc, std::vector<double>& out) {
@@ -151,8 +151,8 @@ void gather_perf_cells(Ctx& c, const double* p, const double* sw, const double* 
   double* d = c.d_scal.p + 1024;  // 3P <= 3072 doubles (checked at setup)
   k_gather_perf<<<blocks_for(P, 64), 64, 0, c.stream>>>(P, c.d_perf_cell.p, p, sw, hc, d);
   c.launches++;
-  RF_CUDA(cudaMemcpyAsync(out.data(), d, sizeof(double) * 3 * P, cudaMemcpyDeviceToHost, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  d2h(c, out.data(), d, sizeof(double) * 3 * P);
+  d2h_wait(c);
 }
 
 }  // namespace rf
