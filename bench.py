@@ -37,6 +37,8 @@ import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
+# many contexts' streams at once: give them their own hardware queues (read at CUDA start-up)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 HBM_FALLBACK_GBS = 6650.0
 
@@ -49,6 +51,11 @@ WORKLOADS = {
     "2m": (200, 200, 50, 10.0,
            "waterflood_3d 200x200x50 (2,000,000 cells), same statistics and wells, dt 10 d report steps, FP64"),
     "1d": (200, 1, 1, 10.0, "waterflood_1d 200x1x1, rate injector cell 0, BHP producer cell 199, dt 10 d, FP64"),
+    "ensemble": (0, 0, 0, 10.0,
+                 "sensitivity ensemble: {nv} two-phase waterflood variants per GPU (decks.ensemble_variant: nx, ny "
+                 "in 20..64, nz in 5..16, sigma ln k 0.5..1.5, mobility ratio 0.5..10, Corey exponents 1.5..4, kv/kh "
+                 "0.01..1, quarter five-spot), one context per variant stepped concurrently (rf_batch_step), "
+                 "dt 10 d report steps"),
 }
 
 
@@ -62,6 +69,7 @@ def parse():
     ap.add_argument("--dt", type=float, default=None)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="linear-solver precision of the device path (mixed: FP32 ILU and pressure stage)")
+    ap.add_argument("--variants", type=int, default=256, help="ensemble variants per GPU (--workload ensemble)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="wall budget of the CPU baseline sample")
     return ap.parse_args()
@@ -71,6 +79,8 @@ def make_deck(workload):
     from ressim_b200 import decks
 
     nx, ny, nz, dt, desc = WORKLOADS[workload]
+    if workload == "ensemble":  # the CPU legs time variant 0 of the ensemble
+        return decks.ensemble_variant(0), dt, desc
     if workload == "1d":
         deck, _, _ = decks.waterflood_1d()
     else:
@@ -239,7 +249,10 @@ def run_reference(args):
     _, dt_default, desc = make_deck(args.workload)
     dt = args.dt if args.dt is not None else dt_default
     v, k, el, newton, _ = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
-    n = WORKLOADS[args.workload][0] * WORKLOADS[args.workload][1] * WORKLOADS[args.workload][2]
+    n = make_deck(args.workload)[0].n_cells
+    if args.workload == "ensemble":
+        desc = desc.format(nv=args.variants) + "; the reference steps one deck per simulator, so its arm times " \
+               "variant 0 (" + str(n) + " cells)"
     line = {
         "metric": "FIM cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * el / k,
@@ -255,11 +268,165 @@ def run_reference(args):
     return 0
 
 
+def run_ensemble(args, rank, world):
+    """`--workload ensemble`: every rank steps its own `--variants` variants (weak scaling, no
+    collective on the data path); value = all ranks' cells x K / the slowest rank's device time."""
+    cpu_job = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import multiprocessing as mp
+
+        pool = mp.get_context("spawn").Pool(1)
+        cpu_job = (pool, pool.apply_async(cpu_leg, ("ensemble", args.dt, args.warmup, 1, args.cpu_sample_s)))
+    import ctypes as C
+
+    import torch
+
+    from ressim_b200 import Ensemble, _abi, _lib, decks
+
+    if not torch.cuda.is_available():
+        print(json.dumps({"error": "no CUDA device"}))
+        return 1
+    torch.cuda.set_device(0)
+    dev_index = (os.environ.get("CUDA_VISIBLE_DEVICES", "") or "0").split(",")[0].strip() or "0"
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", 0))
+        pg = dist
+    dt_default, desc = WORKLOADS["ensemble"][3], WORKLOADS["ensemble"][4]
+    dt = args.dt if args.dt is not None else dt_default
+    nv = args.variants
+    ds = [decks.ensemble_variant(rank * nv + i) for i in range(nv)]
+    cells = sum(d.n_cells for d in ds)
+    ens = Ensemble(ds, precision=args.precision)
+    L = _lib.load()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def l2_flush():
+        flush.zero_()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        ens.step(dt)
+    for i in range(nv):
+        ens.profile(i, enable=True, reset=True)
+    launches0 = ens.kernel_launches()
+    l2_flush()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev_index)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dev_ms = 0.0
+    newton = 0
+    for _ in range(args.steps):
+        ev0.record()
+        reps = ens.step(dt)  # returns once every variant's stream has finished the report step
+        ev1.record()
+        ev1.synchronize()
+        dev_ms += ev0.elapsed_time(ev1)
+        newton += sum(r["newton_iterations"] for r in reps)
+        l2_flush()
+    clk = clocks.stop()
+    launches = ens.kernel_launches() - launches0
+    profs = [ens.profile(i, enable=False, reset=True) for i in range(nv)]
+    dev_ms_max = max_over_ranks(dev_ms, pg, "cuda")
+    value = world * cells * args.steps / (dev_ms_max / 1e3)
+
+    # e2e: the next K report steps with every variant's state uploaded from pinned host memory
+    # before the step and read back after it
+    hosts = []
+    for i, d in enumerate(ds):
+        st = ens.state(i)
+        p_h = torch.tensor(st["pressure"]).pin_memory()
+        s_h = torch.tensor(st["sat_water"]).pin_memory()
+        hosts.append((p_h, s_h, C.cast(p_h.data_ptr(), C.POINTER(C.c_double)),
+                      C.cast(s_h.data_ptr(), C.POINTER(C.c_double))))
+    tt = C.c_double()
+    l2_flush()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e2e_s = 0.0
+    times = [r["time_days"] for r in reps]
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for i in range(nv):
+            if L.rf_set_state(ens._ctx[i], hosts[i][2], hosts[i][3], None, None, C.c_double(times[i])) != 0:
+                raise RuntimeError(f"rf_set_state failed for variant {i}")
+        reps = ens.step(dt)
+        times = [r["time_days"] for r in reps]
+        for i in range(nv):
+            if L.rf_get_state(ens._ctx[i], hosts[i][2], hosts[i][3], None, None, None, C.byref(tt)) != 0:
+                raise RuntimeError(f"rf_get_state failed for variant {i}")
+        e2e_s += time.perf_counter() - t0
+        l2_flush()
+    e2e_s = max_over_ranks(e2e_s, pg, "cuda")
+    e2e_value = world * cells * args.steps / e2e_s
+
+    peak, peak_kind = measured_hbm_peak()
+    it = sum(p["bicgstab_iterations"] for p in profs)
+    nl = sum(p["bicgstab_launches"] for p in profs)
+    kms = sum(p["bicgstab_kernel"] for p in profs)
+    byts = sum(bicgstab_bytes_per_iteration(d.n_cells, p["nnzb"]) * p["bicgstab_iterations"] for d, p in zip(ds, profs))
+    roof = None
+    if nl > 0 and kms > 0:
+        achieved_one = byts / (kms / 1e3) / 1e9  # per kernel, launches of all variants pooled
+        achieved_all = byts / (dev_ms / 1e3) / 1e9  # all variants' kernels over the step time
+        roof = {"kernel": "k_bicgstab_dsmem (all variants)", "bound": "hbm", "achieved": achieved_all, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved_all / peak, "traffic": None,
+                "achieved_per_kernel": achieved_one, "iterations_per_launch": it / nl,
+                "share_of_kernel_time": kms / max(sum(sum(p[k] for k in _lib.PHASES if k != "bicgstab_kernel")
+                                                      for p in profs), 1e-9)}
+    cpu = None
+    if cpu_job is not None:
+        pool, job = cpu_job
+        try:
+            v, k, el, cnewton, _ = job.get(timeout=900)
+            cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                   "sample": f"variant 0 ({ds[0].n_cells} cells), report step(s) {args.warmup}..{args.warmup + k - 1} "
+                             f"after {args.warmup} untimed ones ({cnewton} Newton iterations, {el:.1f} s), C++ "
+                             f"restatement of the reference FIM, 1 thread"}
+        except Exception as e:  # noqa: BLE001 - reported in the line
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+        pool.terminate()
+    if rank == 0:
+        line = {
+            "metric": "FIM cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded deck generator)",
+            "config": {"workload": desc.format(nv=nv), "variants_per_gpu": nv, "cells_per_gpu": cells,
+                       "dt_days": dt, "parallelism": f"variants sharded over {world} GPU(s)",
+                       "l2": "flushed (256 MB write) between timed report steps; state alone exceeds L2",
+                       "newton_iterations": newton,
+                       "e2e_steps": "the K report steps after the timed ones"},
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * cells,
+                    "d2h_bytes_per_step": 2 * 8 * cells},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
+            "precision": args.precision,
+        }
+        print(json.dumps(line), flush=True)
+    ens.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     rank, world, local = dist_setup(args)
+    if args.workload == "ensemble":
+        return run_ensemble(args, rank, world)
     cpu_job = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "2m":
         import multiprocessing as mp

@@ -214,8 +214,11 @@ int32_t rf_dense_solve_noalloc(int32_t n, const double* a, const double* b, doub
 /* ---- Ensemble batch (sensitivity variants of uneven sizes); no counterpart in the reference, whose
  * simulator object steps one deck.  Each variant gets its own context (the rf_* calls above work on
  * rf_batch_context(b, i)); rf_batch_step advances every variant by one report step, driving the
- * variants from `host_threads` host threads (<= 0: one per hardware thread, at most n) so their
- * kernels run concurrently on the device from separate streams.  Returns the first negative
+ * variants from `host_threads` host threads (<= 0: max(32, hardware threads), at most n) so their
+ * kernels run concurrently on the device from separate streams.  Set the environment variable
+ * CUDA_DEVICE_MAX_CONNECTIONS=32 before CUDA initialises in the process: with the default of 8
+ * hardware queues the variants' streams alias and short kernels wait behind long pressure solves
+ * (the Python package sets it on import).  Returns the first negative
  * status of any variant, else the largest positive one; per-variant reports go to reports[n]. */
 typedef struct RfBatch RfBatch;
 int32_t rf_batch_create(const RfDeck* const* decks, int32_t n, int32_t host_threads, RfBatch** out);

@@ -1157,8 +1157,10 @@ int32_t rf_batch_create(const RfDeck* const* decks, int32_t n, int32_t host_thre
   for (int32_t i = 0; i < n; ++i) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(),
                    [&](int x, int y) { return b->ctx[x]->c.n > b->ctx[y]->c.n; });
+  // the host threads mostly wait on their variant's stream: up to 32 (the most hardware queues
+  // CUDA_DEVICE_MAX_CONNECTIONS can give the streams) even on fewer cores
   const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
-  b->threads = host_threads > 0 ? host_threads : std::min<int>(n, hw);
+  b->threads = host_threads > 0 ? host_threads : std::min<int>(n, std::max(hw, 32));
   *out = b;
   return RF_OK;
 }
