@@ -5,24 +5,36 @@ assembly, well Schur elimination, CPR-FGMRES and the update, including any subst
 on a seeded synthetic waterflood deck, run through the C ABI (`rf_step`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload 72k|2m|1d] [--dt DAYS] [--no-cpu-baseline]
+                    [--workload ensemble|72k|2m|1d] [--variants V] [--precision fp64|mixed]
+                    [--dt DAYS] [--no-cpu-baseline]
 
-Legs of the default (`--impl ours`) run, all on the same deck:
-  value     device time of K report steps with the state resident in HBM (CUDA events recorded
-            by the library on its own stream around each `rf_step`; L2 flushed between steps);
-  e2e       the same K report steps (a second simulator of the deck after the same warm-up)
-            through the public API with host buffers: every step uploads the state from pinned
-            host memory (`rf_set_state`), steps, and reads the state back (`rf_get_state`); each
-            step is timed from before the upload to after the read-back (host clock around
-            synchronous calls, so it covers the device work and the copies);
-  roofline  the cooperative BiCGStab kernel (the pressure stage, the dominant kernel): algorithmic
-            bytes per iteration x iterations per launch / mean launch time (CUDA events);
-  cpu_baseline  the CPU restatement (C++, single thread, like the reference) on the same deck and
-            the same report steps (after the same warm-up steps), in a spawned process beside the
-            GPU legs, bounded to about `--cpu-sample-s` seconds of timed work.
+The default workload is the sensitivity ensemble: 256 two-phase waterflood variants of uneven
+size (3,300 to 64,512 cells, 4.9M cells in all) per GPU, all advanced together one report step at
+a time (rf_batch_step).  `--workload 72k` is the single 60x60x20 deck of the plain FP64 form.
 
-Multi-GPU: the report step does not shard across GPUs in this build, so `--gpus N` under torchrun
-runs N independent replicas of the same deck (weak scaling); timing is the max over ranks.
+Legs of the `--impl ours` run:
+  value     device time of K report steps with the state resident in HBM, L2 flushed (256 MB
+            write) between steps.  Single deck: CUDA events recorded by the library on its own
+            stream around each `rf_step`.  Ensemble: CUDA events on the caller's stream around each
+            `rf_batch_step`, which returns when every variant's stream has finished;
+  e2e       the same metric through the public API with host buffers: every step uploads each
+            state from pinned host memory (`rf_set_state`), steps, and reads it back
+            (`rf_get_state`), timed from before the uploads to after the read-backs.  Single deck:
+            the same K steps on a second simulator after the same warm-up; ensemble: the K steps
+            after the timed ones;
+  roofline  the pressure BiCGStab kernel (the dominant kernel): algorithmic bytes per iteration
+            x iterations / kernel time (CUDA events), against the measured HBM copy bandwidth;
+  cpu_baseline  the CPU restatement (C++, single thread, like the reference) on the same deck
+            (ensemble: variant 0) and the same report steps after the same warm-up, in a spawned
+            process beside the GPU legs.
+
+The reference arm (`--impl reference`) times the CPU restatement on the host cores: the single
+deck on one core (the reference is single-threaded), the ensemble as one single-threaded process
+per core over the first `cores` variants.
+
+Multi-GPU (torchrun): a single deck does not shard, so each rank runs a replica; the ensemble
+shards by variant, every rank stepping its own `--variants` variants.  Both are weak scaling with
+no collective on the data path; timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -65,7 +77,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="72k")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ensemble")
     ap.add_argument("--dt", type=float, default=None)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="linear-solver precision of the device path (mixed: FP32 ILU and pressure stage)")
@@ -238,6 +250,61 @@ def cpu_leg(workload, dt, warmup, steps, budget_s):
     return n * k / el, k, el, newton, states
 
 
+def _ref_variant_worker(index, dt, warmup, steps):
+    """One reference-arm worker: variant `index` stepped `warmup` untimed and `steps` timed report
+    steps by the CPU restatement, single-threaded.  Returns (cells, seconds, Newton iterations)."""
+    sys.path.insert(0, HERE)
+    from oracle.oracle_py import OracleSimulator
+    from ressim_b200 import decks
+
+    d = decks.ensemble_variant(index)
+    sim = OracleSimulator(d)
+    for _ in range(warmup):
+        sim.step(dt)
+    t0 = time.perf_counter()
+    newton = 0
+    for _ in range(steps):
+        _, rep = sim.step(dt)
+        newton += rep.newton_iterations
+    el = time.perf_counter() - t0
+    sim.close()
+    return d.n_cells, el, newton
+
+
+def run_reference_ensemble(args):
+    """Reference arm of the ensemble: the reference steps one deck per simulator, single-threaded,
+    so a multi-core host runs one variant per core.  One process per host core (spawned) steps the
+    first `cores` variants (a bounded sample of the ensemble: W untimed and K timed report steps
+    each); throughput = cells x K summed over the sample / the slowest worker's timed seconds."""
+    import multiprocessing as mp
+
+    cores = max(1, min(os.cpu_count() or 1, args.variants))
+    dt = args.dt if args.dt is not None else WORKLOADS["ensemble"][3]
+    k = max(1, args.steps)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.starmap(_ref_variant_worker, [(i, dt, args.warmup, k) for i in range(cores)])
+    cells = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    newton = sum(r[2] for r in res)
+    v = cells * k / slowest
+    desc = WORKLOADS["ensemble"][4].format(nv=args.variants)
+    line = {
+        "metric": "FIM cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * slowest / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded deck generator)",
+        "config": {"workload": desc, "sample_variants": cores, "sample_cells": cells, "dt_days": dt,
+                   "newton_iterations": newton},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"variants 0..{cores - 1} ({cells} cells), one single-threaded process per "
+                                   f"core, report steps {args.warmup}..{args.warmup + k - 1} after {args.warmup} "
+                                   f"untimed ones; C++ restatement of the reference FIM"},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """Reference arm: the reference's FIM path on the host cores.  The reference (Rust/WASM) cannot
     be built in this image (no cargo, rustc or node), so its C++ restatement (oracle) is timed, one
@@ -246,6 +313,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "ensemble":
+        return run_reference_ensemble(args)
     _, dt_default, desc = make_deck(args.workload)
     dt = args.dt if args.dt is not None else dt_default
     v, k, el, newton, _ = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
