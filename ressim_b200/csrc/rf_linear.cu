@@ -1089,6 +1089,7 @@ struct PipeSync {
   volatile int* abort_s;  // shared: a wait of this CTA gave up
   int* status;            // global status word, read by the host after the solve
   unsigned epoch;         // progress value at the start of the current sweep
+  unsigned level;         // positions processed so far in this launch (selects the barrier pair)
   unsigned cons_f, cons_b;  // CTAs that read this CTA's rows in the forward / backward sweep
 };
 
@@ -1101,20 +1102,40 @@ __device__ __forceinline__ unsigned read_inbox(const unsigned* p) {
   return v;
 }
 
-// Warp 0, lane j: push `value` into inbox[me] of consumer CTA j (after the CTA's rows of this
-// position are written and a __syncthreads has ordered them before this store).
-__device__ __forceinline__ void push_progress(const PipeSync& ps, unsigned consumers, unsigned me, unsigned value) {
-  const unsigned j = threadIdx.x;
-  if (j < 32 && ((consumers >> j) & 1u)) {
+// Lane j of the signalling warp: push `value` into inbox[me] of consumer CTA j.  The compute
+// warps' rows of the positions it covers were ordered before this store by the named barrier the
+// signalling warp waited on.
+__device__ __forceinline__ void push_progress(const PipeSync& ps, unsigned consumers, unsigned me, unsigned lane,
+                                              unsigned value) {
+  if ((consumers >> lane) & 1u) {
     unsigned addr;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(smem_u32(ps.inbox + me)), "r"(j));
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(smem_u32(ps.inbox + me)), "r"(lane));
     asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(value) : "memory");
   }
 }
 
+// Named barriers of the pipelined sweeps (0 is __syncthreads), used in two alternating pairs by
+// the running count i of processed positions, so that no barrier instance can collect arrivals
+// from two positions:
+//   compute warps, position i: sync kBarCompute + (i & 1) (with the signalling warp's arrival),
+//     handle the rows, arrive (no wait) on kBarSignal + (i & 1);
+//   signalling warp, position i: sync kBarSignal + (i & 1), push the progress, arrive on
+//     kBarCompute + (i & 1) -- the compute barrier of position i + 2.
+// The signalling warp arrives on both compute barriers once at kernel start (for positions 0 and
+// 1), and the compute warps sync on both once at kernel end, which leaves every instance complete.
+constexpr int kBarCompute = 1;  // and 2
+constexpr int kBarSignal = 3;   // and 4
+__device__ __forceinline__ void named_sync(int id, int threads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int threads) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
 // Warp 0 waits until every CTA that position `pos` of this CTA reads from has pushed the
-// progress the table asks for; the other threads meet it at the __syncthreads that follows.
-__device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* req_s, int pos, int cs, unsigned me) {
+// progress the table asks for; the other compute warps meet it at the named barrier that follows.
+__device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* req_s, int pos, int cs, unsigned me,
+                                            int all_threads) {
   const int j = threadIdx.x;
   if (j < cs && j != int(me) && !*ps.abort_s) {
     const unsigned need = req_s[pos * cs + j];
@@ -1130,13 +1151,17 @@ __device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* 
       }
     }
   }
-  __syncthreads();
+  named_sync(kBarCompute + int(ps.level & 1u), all_threads);
 }
 
+// The last warp of the CTA only signals: it waits for the compute warps to finish each position
+// and pushes the progress, so the release stores stay off the compute warps' path.  The compute
+// warps (all but the last) handle the rows.
 template <class T, bool FWD>
 __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr, const unsigned short* req_s,
                            int base, unsigned me, int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s) {
-  const int S = a.own.slice, n = a.n, L = a.n_levels, t = threadIdx.x, B = blockDim.x;
+  const int S = a.own.slice, n = a.n, L = a.n_levels, t = threadIdx.x;
+  const int B = blockDim.x - 32;  // compute threads
   const PackedSweep<T>& pk = FWD ? a.fw : a.bw;
   auto level_of = [&](int pos) { return FWD ? pos : L - 1 - pos; };
   auto empty = [&](int pos) {
@@ -1158,11 +1183,26 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
   const unsigned consumers = FWD ? ps.cons_f : ps.cons_b;
   int pos = 0;
   while (pos < L && empty(pos)) ++pos;
-  push_progress(ps, consumers, me, ps.epoch + unsigned(pos));
+  if (t >= B) {
+    // signalling warp: the same sequence of positions as the compute warps
+    const unsigned lane = unsigned(t - B);
+    push_progress(ps, consumers, me, lane, ps.epoch + unsigned(pos));
+    while (pos < L) {
+      int next = pos + 1;
+      while (next < L && empty(next)) ++next;
+      named_sync(kBarSignal + int(ps.level & 1u), B + 32);
+      push_progress(ps, consumers, me, lane, ps.epoch + unsigned(next));
+      named_arrive(kBarCompute + int(ps.level & 1u), B + 32);
+      ++ps.level;
+      pos = next;
+    }
+    ps.epoch += unsigned(L) + 1u;
+    return;
+  }
   PackedRow<T> cur;
   prefetch(cur, pos);
   while (pos < L) {
-    wait_inputs(ps, req_s, pos, cs, me);
+    wait_inputs(ps, req_s, pos, cs, me, B + 32);
     const int l = level_of(pos);
     const int q0 = lptr[l] + t, qe = lptr[l + 1];
     if (q0 < qe) {
@@ -1195,8 +1235,8 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
     }
     int next = pos + 1;
     while (next < L && empty(next)) ++next;
-    __syncthreads();
-    push_progress(ps, consumers, me, ps.epoch + unsigned(next));
+    named_arrive(kBarSignal + int(ps.level & 1u), B + 32);
+    ++ps.level;
     prefetch(cur, next);
     pos = next;
   }
@@ -1275,8 +1315,13 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
   ps.abort_s = &s_abort;
   ps.status = a.status;
   ps.epoch = 0;
+  ps.level = 0;
   ps.cons_f = a.cons_f[me];
   ps.cons_b = a.cons_b[me];
+  if (threadIdx.x >= blockDim.x - 32) {  // signalling warp: release the compute barriers of positions 0 and 1
+    named_arrive(kBarCompute, blockDim.x);
+    named_arrive(kBarCompute + 1, blockDim.x);
+  }
   double v3[3], o3[3];
   int parity = 0;
   v3[0] = 0.0;
@@ -1358,6 +1403,10 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
   }
   if (me == 0 && threadIdx.x == 0 && a.iter_counter)
     atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
+  if (threadIdx.x < blockDim.x - 32) {  // complete the compute-barrier instances the signalling warp opened last
+    named_sync(kBarCompute + int(ps.level & 1u), blockDim.x);
+    named_sync(kBarCompute + int((ps.level + 1u) & 1u), blockDim.x);
+  }
   // no CTA may leave while another can still read its shared memory
   cluster_barrier();
 }
