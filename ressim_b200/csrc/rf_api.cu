@@ -885,7 +885,6 @@ static void free_ctx(Ctx& c) {
                   &c.d_perf_row_off, &c.d_flag_dense, &c.d_dense_perm})
     b->free();
   for (auto* b : {&c.d_own_rows, &c.d_own_ptr, &c.d_fcnt, &c.d_bcnt, &c.d_fdep, &c.d_bdep, &c.d_pipe_status}) b->free();
-  for (auto* b : {&c.d_fpc, &c.d_bpc, &c.d_fpt, &c.d_bpt}) b->free();
   c.d_reqf.free();
   c.d_reqb.free();
   c.d_cons.free();

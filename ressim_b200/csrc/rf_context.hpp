@@ -140,8 +140,6 @@ struct Ctx {
   size_t dsm_bytes[2] = {0, 0};  // dynamic shared memory per CTA for double / float; 0: does not fit
   DBuf<int> d_own_rows, d_own_ptr;
   DBuf<int> d_fcnt, d_bcnt, d_fdep, d_bdep;  // packed sweep structure (ownership order)
-  DBuf<int> d_fpc, d_bpc, d_fpt, d_bpt;      // halo push counts and targets per row
-  int halo_f = 0, halo_b = 0;                // halo slots per CTA
   DBuf<unsigned short> d_reqf, d_reqb;       // per-CTA, per-position progress needed from each CTA
   DBuf<unsigned> d_cons;                     // [2][cs] consumer masks of the forward / backward sweeps
   DBuf<int> d_pipe_status;                   // nonzero: a pipelined sweep's bounded wait gave up

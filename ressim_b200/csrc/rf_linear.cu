@@ -20,7 +20,6 @@
 // fill.  Pressure-matrix entries with |v| <= 1e-14 are dropped, as the reference does.
 
 #include <algorithm>
-#include <map>
 #include <mutex>
 #include <cstdio>
 
@@ -941,22 +940,15 @@ __device__ __forceinline__ T slice_read(const T* local, int idx, int slice, unsi
 
 // Level-ordered packed rows of each CTA's slice (index g = position in the ownership order,
 // the same order as OwnedLevels::rows): for the forward (L) and backward (U) parts, the number of
-// entries (-1 when more than kPackK: that row takes the CSR path), each entry's column and the
-// factor values in column order.  A column in this CTA's slice is (me << 24) | local index; a
-// column of another CTA that this CTA reads is a slot of its halo, a shared-memory copy that the
-// owner pushes as soon as it computes the value ((1 << 31) | slot); the rare column read by
-// more than kPushK other CTAs stays (owner << 24) | index and is read through distributed shared
-// memory.  Each row also lists the halos (consumer, slot) its value goes to.  The structure is
-// fixed per pattern; the values are repacked after every factorisation.
+// entries (-1 when more than kPackK: that row takes the CSR path), each entry's column as
+// (owner CTA << 24) | index within the owner's slice, and the factor values in column order.
+// The structure is fixed per pattern; the values are repacked after every factorisation.
 constexpr int kPackK = 4;
-constexpr int kPushK = 2;
 template <class T>
 struct PackedSweep {
-  const int* cnt;   // [n]
-  const int* dep;   // [kPackK][n]; negative: (1 << 31) | slot in this CTA's halo
-  const T* val;     // [kPackK][n]
-  const int* pcnt;  // [n]: other CTAs' halos this row's value is pushed to (0..kPushK)
-  const int* ptgt;  // [kPushK][n]: (consumer CTA << 24) | halo slot
+  const int* cnt;  // [n]
+  const int* dep;  // [kPackK][n]
+  const T* val;    // [kPackK][n]
 };
 
 // sum -= plu[k] * src[col[k]] for k in [k0, k1), in k order, with the loads of each batch of
@@ -1014,7 +1006,6 @@ struct DsmBicgArgs {
   // [cs][L][cs]: progress (in positions) CTA b needs from CTA b' before a position, 0 = none
   const unsigned short* reqf;
   const unsigned short* reqb;
-  int halo_f, halo_b;      // halo slots per CTA (forward / backward), a multiple of 2
   const unsigned* cons_f;  // [cs]: bit j set when CTA j reads this CTA's rows in the forward sweep
   const unsigned* cons_b;  // [cs]: the same for the backward sweep
   int* status;
@@ -1038,37 +1029,17 @@ __device__ __forceinline__ void cluster_wait_acquire() {
 }
 
 template <class T>
-__device__ __forceinline__ T dep_read(const T* slice_base, const T* halo, int dep, unsigned me) {
-  if (dep < 0) return halo[dep & 0x7fffffff];
+__device__ __forceinline__ T dep_read(const T* slice_base, int dep, unsigned me) {
   const unsigned owner = unsigned(dep) >> 24;
   const T* p = slice_base + (dep & 0xffffff);
   return owner == me ? *p : dsm_load(p, owner);
-}
-__device__ __forceinline__ void dsm_store(double* p, unsigned rank, double v) {
-  unsigned r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(static_cast<unsigned>(__cvta_generic_to_shared(p))), "r"(rank));
-  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(r), "d"(v) : "memory");
-}
-__device__ __forceinline__ void dsm_store(float* p, unsigned rank, float v) {
-  unsigned r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(static_cast<unsigned>(__cvta_generic_to_shared(p))), "r"(rank));
-  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(r), "f"(v) : "memory");
-}
-// Push a row's value into the halos of the CTAs that read it (before the position's progress is
-// signalled, so a consumer that sees the progress finds the value in its own shared memory).
-template <class T>
-__device__ __forceinline__ void halo_push(T v, int pc, const int* pt, T* halo_base) {
-#pragma unroll
-  for (int j = 0; j < kPushK; ++j)
-    if (j < pc) dsm_store(halo_base + (pt[j] & 0xffffff), unsigned(pt[j]) >> 24, v);
 }
 
 // One row's packed data, loaded one level ahead.
 template <class T>
 struct PackedRow {
-  int g, r, cnt, pc;
+  int g, r, cnt;
   int dep[kPackK];
-  int pt[kPushK];
   T val[kPackK];
   T extra;  // forward: rhs[r]; backward: pivot
 };
@@ -1079,24 +1050,21 @@ __device__ __forceinline__ void load_packed(PackedRow<T>& pr, const PackedSweep<
   pr.g = g;
   pr.r = r;
   pr.cnt = ps.cnt[g];
-  pr.pc = ps.pcnt[g];
 #pragma unroll
   for (int j = 0; j < kPackK; ++j) {
     pr.dep[j] = ps.dep[size_t(j) * n + g];
     pr.val[j] = ps.val[size_t(j) * n + g];
   }
-#pragma unroll
-  for (int j = 0; j < kPushK; ++j) pr.pt[j] = ps.ptgt[size_t(j) * n + g];
   pr.extra = extra_src[extra_idx];
 }
 
 // s - sum_j val_j * src[dep_j] over the row's entries in column order; the dependency loads are
 // issued together, the subtractions keep the sequential order.
 template <class T>
-__device__ __forceinline__ T packed_subtract(T s, const PackedRow<T>& pr, const T* src, const T* halo, unsigned me) {
+__device__ __forceinline__ T packed_subtract(T s, const PackedRow<T>& pr, const T* src, unsigned me) {
   T d[kPackK];
 #pragma unroll
-  for (int j = 0; j < kPackK; ++j) d[j] = j < pr.cnt ? dep_read(src, halo, pr.dep[j], me) : T(0);
+  for (int j = 0; j < kPackK; ++j) d[j] = j < pr.cnt ? dep_read(src, pr.dep[j], me) : T(0);
 #pragma unroll
   for (int j = 0; j < kPackK; ++j)
     if (j < pr.cnt) s -= pr.val[j] * d[j];
@@ -1191,7 +1159,7 @@ __device__ __forceinline__ void wait_inputs(PipeSync& ps, const unsigned short* 
 // warps (all but the last) handle the rows.
 template <class T, bool FWD>
 __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr, const unsigned short* req_s,
-                           int base, unsigned me, int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s, T* halo) {
+                           int base, unsigned me, int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s) {
   const int S = a.own.slice, n = a.n, L = a.n_levels, t = threadIdx.x;
   const int B = blockDim.x - 32;  // compute threads
   const PackedSweep<T>& pk = FWD ? a.fw : a.bw;
@@ -1239,42 +1207,31 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
     const int q0 = lptr[l] + t, qe = lptr[l + 1];
     if (q0 < qe) {
       const int r = cur.r;
-      T v;
       if (FWD) {
-        if (cur.cnt >= 0)
-          v = packed_subtract(cur.extra, cur, y_s, halo, me);
-        else
-          v = csr_subtract(cur.extra, a.rp[r], a.diag[r], a.col, a.plu, y_s, S, me);
-        y_s[r - base] = v;
+        if (cur.cnt >= 0) {
+          y_s[r - base] = packed_subtract(cur.extra, cur, y_s, me);
+        } else {
+          y_s[r - base] = csr_subtract(cur.extra, a.rp[r], a.diag[r], a.col, a.plu, y_s, S, me);
+        }
       } else {
         T sum = y_s[r - base];
         if (cur.cnt >= 0)
-          sum = packed_subtract(sum, cur, out_s, halo, me);
+          sum = packed_subtract(sum, cur, out_s, me);
         else
           sum = csr_subtract(sum, a.diag[r] + 1, a.rp[r + 1], a.col, a.plu, out_s, S, me);
         const T d = cur.extra;
-        v = fabs(double(d)) > kEps ? sum / d : sum;
-        out_s[r - base] = v;
+        out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
       }
-      halo_push(v, cur.pc, cur.pt, halo);
     }
     for (int q = q0 + B; q < qe; q += B) {
       const int r = lrows[q];
-      T v;
       if (FWD) {
-        v = csr_subtract(rhs[r], a.rp[r], a.diag[r], a.col, a.plu, y_s, S, me);
-        y_s[r - base] = v;
+        y_s[r - base] = csr_subtract(rhs[r], a.rp[r], a.diag[r], a.col, a.plu, y_s, S, me);
       } else {
         const T sum = csr_subtract(y_s[r - base], a.diag[r] + 1, a.rp[r + 1], a.col, a.plu, out_s, S, me);
         const T d = a.pdiag[r];
-        v = fabs(double(d)) > kEps ? sum / d : sum;
-        out_s[r - base] = v;
+        out_s[r - base] = fabs(double(d)) > kEps ? sum / d : sum;
       }
-      const int g = base + q;
-      int pt[kPushK];
-#pragma unroll
-      for (int j = 0; j < kPushK; ++j) pt[j] = pk.ptgt[size_t(j) * n + g];
-      halo_push(v, pk.pcnt[g], pt, halo);
     }
     int next = pos + 1;
     while (next < L && empty(next)) ++next;
@@ -1291,9 +1248,9 @@ __device__ void pipe_sweep(const DsmBicgArgs<T>& a, const int* lrows, const int*
 template <class T>
 __device__ void dsm_ilu_apply(const DsmBicgArgs<T>& a, const int* lrows, const int* lptr,
                               const unsigned short* reqf_s, const unsigned short* reqb_s, int base, unsigned me,
-                              int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s, T* hf_s, T* hb_s) {
-  pipe_sweep<T, true>(a, lrows, lptr, reqf_s, base, me, cs, ps, rhs, y_s, out_s, hf_s);
-  pipe_sweep<T, false>(a, lrows, lptr, reqb_s, base, me, cs, ps, rhs, y_s, out_s, hb_s);
+                              int cs, PipeSync& ps, const T* rhs, T* y_s, T* out_s) {
+  pipe_sweep<T, true>(a, lrows, lptr, reqf_s, base, me, cs, ps, rhs, y_s, out_s);
+  pipe_sweep<T, false>(a, lrows, lptr, reqb_s, base, me, cs, ps, rhs, y_s, out_s);
   cluster_barrier();
 }
 
@@ -1334,9 +1291,7 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
   T* y_s = reinterpret_cast<T*>(dsm_raw);
   T* ph_s = y_s + S;
   T* sh_s = ph_s + S;
-  T* hf_s = sh_s + S;        // forward-sweep halo
-  T* hb_s = hf_s + a.halo_f;  // backward-sweep halo
-  int* lrows = reinterpret_cast<int*>(hb_s + a.halo_b);
+  int* lrows = reinterpret_cast<int*>(sh_s + S);
   int* lptr = lrows + S;
   const int L = a.n_levels;
   const int cs = int(cluster_nblocks());
@@ -1401,7 +1356,7 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
         a.p[i] = T(double(a.r[i]) + beta * (double(a.p[i]) - omega * double(a.v[i])));
     }
     __syncthreads();
-    dsm_ilu_apply(a, lrows, lptr, reqf_s, reqb_s, base, me, cs, ps, a.p, y_s, ph_s, hf_s, hb_s);
+    dsm_ilu_apply(a, lrows, lptr, reqf_s, reqb_s, base, me, cs, ps, a.p, y_s, ph_s);
     dsm_spmv(a, base, cnt, me, ph_s, a.v);
     v3[0] = 0.0;
     for (int i = base + threadIdx.x; i < base + cnt; i += blockDim.x) v3[0] += double(a.rh[i]) * double(a.v[i]);
@@ -1420,7 +1375,7 @@ __global__ void __launch_bounds__(kDBlock, 1) k_bicgstab_dsmem(DsmBicgArgs<T> a)
       for (int i = threadIdx.x; i < cnt; i += blockDim.x) a.x[base + i] += alpha * double(ph_s[i]);
       break;
     }
-    dsm_ilu_apply(a, lrows, lptr, reqf_s, reqb_s, base, me, cs, ps, a.s, y_s, sh_s, hf_s, hb_s);
+    dsm_ilu_apply(a, lrows, lptr, reqf_s, reqb_s, base, me, cs, ps, a.s, y_s, sh_s);
     dsm_spmv(a, base, cnt, me, sh_s, a.t);
     v3[0] = 0.0;
     v3[1] = 0.0;
@@ -1732,12 +1687,6 @@ static bool launch_bicgstab_dsmem(Ctx& c, const T* pval, const T* plu, const T* 
   a.cons_f = c.d_cons.p;
   a.cons_b = c.d_cons.p + c.cluster_size;
   a.status = c.d_pipe_status.p;
-  a.halo_f = c.halo_f;
-  a.halo_b = c.halo_b;
-  a.fw.pcnt = c.d_fpc.p;
-  a.fw.ptgt = c.d_fpt.p;
-  a.bw.pcnt = c.d_bpc.p;
-  a.bw.ptgt = c.d_bpt.p;
   a.fw.cnt = c.d_fcnt.p;
   a.fw.dep = c.d_fdep.p;
   a.bw.cnt = c.d_bcnt.p;
@@ -2166,62 +2115,19 @@ static void build_owned_levels(Ctx& c) {
     std::vector<int> fill(bp, bp + L);
     for (int r = lo; r < hi; ++r) rows[lo + fill[lvl[r]]++] = r;
   }
-  // packed sweep structure: entry counts (-1 above kPackK); columns as (owner << 24 | local), or
-  // as halo slots for columns of other CTAs that the owner pushes (at most kPushK consumers per
-  // value: a value wanted by more CTAs is pushed to the first kPushK and read remotely by the rest)
+  // packed sweep structure: entry counts (-1 above kPackK) and (owner << 24 | local) columns
   std::vector<int> fcnt(n), bcnt(n), fdep(size_t(kPackK) * n, 0), bdep(size_t(kPackK) * n, 0);
-  std::vector<int> fpc(n, 0), bpc(n, 0), fpt(size_t(kPushK) * n, 0), bpt(size_t(kPushK) * n, 0);
-  std::vector<int> gpos(n);  // row -> ownership position
-  for (int g = 0; g < n; ++g) gpos[rows[g]] = g;
   auto packdep = [&](int col) { return ((col / S) << 24) | (col - (col / S) * S); };
-  std::vector<std::map<int, int>> hslot_f(cs), hslot_b(cs);  // per consumer CTA: column -> halo slot
   for (int g = 0; g < n; ++g) {
     const int r = rows[g];
     const int lo = c.h_row_ptr[r], d = c.h_diag[r], hi = c.h_row_ptr[r + 1];
     fcnt[g] = d - lo <= kPackK ? d - lo : -1;
     bcnt[g] = hi - d - 1 <= kPackK ? hi - d - 1 : -1;
-  }
-  // halo assignment: for every packed row of CTA b reading column col of another CTA
-  auto assign = [&](bool fwd) {
-    auto& hslot = fwd ? hslot_f : hslot_b;
-    auto& pc = fwd ? fpc : bpc;
-    auto& pt = fwd ? fpt : bpt;
-    auto& dep = fwd ? fdep : bdep;
-    const auto& cnt = fwd ? fcnt : bcnt;
-    for (int g = 0; g < n; ++g) {
-      const int r = rows[g], b = g / S;
-      const int k0 = fwd ? c.h_row_ptr[r] : c.h_diag[r] + 1;
-      for (int j = 0; j < cnt[g]; ++j) {
-        const int col = c.h_col[k0 + j], ob = col / S;
-        int code = packdep(col);
-        if (ob != b) {
-          auto it = hslot[b].find(col);
-          if (it != hslot[b].end()) {
-            code = int(0x80000000u | unsigned(it->second));
-          } else {
-            const int cg = gpos[col];
-            if (pc[cg] < kPushK) {
-              const int slot = int(hslot[b].size());
-              hslot[b][col] = slot;
-              pt[size_t(pc[cg]) * n + cg] = (b << 24) | slot;
-              pc[cg]++;
-              code = int(0x80000000u | unsigned(slot));
-            }
-          }
-        }
-        dep[size_t(j) * n + g] = code;
-      }
+    for (int j = 0; j < kPackK; ++j) {
+      if (j < fcnt[g]) fdep[size_t(j) * n + g] = packdep(c.h_col[lo + j]);
+      if (j < bcnt[g]) bdep[size_t(j) * n + g] = packdep(c.h_col[d + 1 + j]);
     }
-  };
-  assign(true);
-  assign(false);
-  size_t hf_max = 0, hb_max = 0;
-  for (int b = 0; b < cs; ++b) {
-    hf_max = std::max(hf_max, hslot_f[b].size());
-    hb_max = std::max(hb_max, hslot_b[b].size());
   }
-  c.halo_f = int((hf_max + 1) & ~size_t(1));
-  c.halo_b = int((hb_max + 1) & ~size_t(1));
   // progress tables of the pipelined sweeps: before position p (forward: level p; backward:
   // level L-1-p) CTA b needs, from each other CTA b', every position that holds a column its rows
   // at that level read, i.e. progress >= (forward) level(col) + 1 or (backward) L - level(col)
@@ -2270,15 +2176,6 @@ static void build_owned_levels(Ctx& c) {
   c.d_bcnt.alloc(n);
   c.d_fdep.alloc(size_t(kPackK) * n);
   c.d_bdep.alloc(size_t(kPackK) * n);
-  for (auto* b : {&c.d_fpc, &c.d_bpc, &c.d_fpt, &c.d_bpt}) b->free();
-  c.d_fpc.alloc(n);
-  c.d_bpc.alloc(n);
-  c.d_fpt.alloc(size_t(kPushK) * n);
-  c.d_bpt.alloc(size_t(kPushK) * n);
-  RF_CUDA(cudaMemcpy(c.d_fpc.p, fpc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-  RF_CUDA(cudaMemcpy(c.d_bpc.p, bpc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-  RF_CUDA(cudaMemcpy(c.d_fpt.p, fpt.data(), sizeof(int) * fpt.size(), cudaMemcpyHostToDevice));
-  RF_CUDA(cudaMemcpy(c.d_bpt.p, bpt.data(), sizeof(int) * bpt.size(), cudaMemcpyHostToDevice));
   RF_CUDA(cudaMemcpy(c.d_own_rows.p, rows.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   RF_CUDA(cudaMemcpy(c.d_own_ptr.p, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice));
   RF_CUDA(cudaMemcpy(c.d_fcnt.p, fcnt.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
@@ -2303,8 +2200,8 @@ static void build_owned_levels(Ctx& c) {
     c.dsm_bytes[f] = 0;
     cudaFuncAttributes fa;
     RF_CUDA(cudaFuncGetAttributes(&fa, fns[f]));
-    const size_t bytes = (3 * size_t(S) + size_t(c.halo_f) + size_t(c.halo_b)) * tsz[f] +
-                         sizeof(int) * (size_t(S) + L + 1) + 2 * sizeof(unsigned short) * size_t(L) * cs;
+    const size_t bytes = 3 * size_t(S) * tsz[f] + sizeof(int) * (size_t(S) + L + 1) +
+                         2 * sizeof(unsigned short) * size_t(L) * cs;
     if (!req_fits || bytes + fa.sharedSizeBytes > size_t(optin)) continue;
     raise_dynamic_smem(fns[f], bytes);
     if (cs > 8) RF_CUDA(cudaFuncSetAttribute(fns[f], cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
