@@ -61,6 +61,7 @@ def lib():
         L.orc_well_index.restype = C.c_double
         L.orc_ad_probe.argtypes = [C.c_int32, C.c_double, C.c_double, _dp]
         L.orc_set_sum_order.argtypes = [C.c_int32]
+        L.orc_head_offsets.argtypes = [C.c_void_p, _dp, C.c_int32]
         L.orc_assemble_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp, _ip, _ip, _dp, _ip, _ip, _dp]
         L.orc_topology.argtypes = [C.c_void_p, _ip, _ip]
         _lib = L
@@ -140,6 +141,12 @@ class OracleSimulator:
         lib().orc_assemble_current(self._h, dt, C.byref(nu), C.byref(nnz), ptr(res), iptr(ptr_), iptr(col),
                                    ptr(val))
         return res, ptr_, col, val
+
+    def head_offsets(self):
+        """Completion head offsets (bar) of the current state, one per deck well entry."""
+        out = np.zeros(len(self.deck.wells))
+        lib().orc_head_offsets(self._h, ptr(out), len(out))
+        return out
 
     def topology(self):
         w, p = C.c_int32(), C.c_int32()

@@ -473,9 +473,83 @@ static void record_step(Ctx& c, const WellState& ws, double dt, double water_cha
   c.rate_history.push_back(r);
 }
 
+// refresh_well_head_offsets (well_control.rs:192-276), on the state entering a report step: each
+// completion's head carries its physical well's datum BHP along the wellbore, density * g *
+// (depth(k) - datum) * 1e-5 bar.  Datum: the group's first explicit datum_depth_m, else its
+// shallowest completion.  Density: the first explicit wellbore_density_kg_m3, else the mean over
+// the group of the water density (injector) or the mobility-weighted mixture density (producer,
+// analytic Corey at the completion cell's state), each at the cell's pressure.  The per-completion
+// heads are copied to the device for the connection rows.
+static void refresh_head_offsets(Ctx& c) {
+  const Topology& t = c.topo;
+  c.head_offset.assign(c.wells.size(), 0.0);
+  if (c.fluid.gravity && t.n_perfs > 0) {
+    PerfCells pc;
+    gather_perf_cells(c, c.d_p.p, c.d_sw.p, c.d_hc.p, pc.v);
+    const Fluid& f = c.fluid;
+    for (int w = 0; w < t.n_wells; ++w) {
+      double datum = NAN, density = NAN;
+      for (int q = t.well_ptr[w]; q < t.well_ptr[w + 1]; ++q) {
+        const double d = c.wells[t.perf_entry[t.well_perfs[q]]].datum_depth_m;
+        if (std::isfinite(d)) {
+          datum = d;
+          break;
+        }
+      }
+      if (!std::isfinite(datum)) {
+        datum = INFINITY;
+        for (int q = t.well_ptr[w]; q < t.well_ptr[w + 1]; ++q)
+          datum = fmin(datum, c.depth_layer[c.wells[t.perf_entry[t.well_perfs[q]]].k]);
+      }
+      for (int q = t.well_ptr[w]; q < t.well_ptr[w + 1]; ++q) {
+        const double d = c.wells[t.perf_entry[t.well_perfs[q]]].wellbore_density_kg_m3;
+        if (std::isfinite(d) && d >= 0.0) {
+          density = d;
+          break;
+        }
+      }
+      if (!std::isfinite(density)) {
+        double total = 0.0, count = 0.0;
+        for (int q = t.well_ptr[w]; q < t.well_ptr[w + 1]; ++q) {
+          const int k = t.well_perfs[q];
+          const double p = pc.p(k), sw = pc.sw(k);
+          const double rho_w = inv_bw(f, p) * f.rho_w;
+          double rho;
+          if (t.perf_inj[k]) {
+            rho = rho_w;
+          } else {
+            const double lw = fmax(corey_krw(f, sw) / f.mu_w, 0.0), lo = fmax(corey_kro(f, sw) / f.mu_o, 0.0);
+            const double lt = fmax(lw + lo, kF64Eps);
+            const double fw = std::clamp(lw / lt, 0.0, 1.0), fo = std::clamp(lo / lt, 0.0, 1.0);
+            rho = fw * rho_w + fo * (f.rho_o / oil_fvf_plain(f, p));  // no gas phase
+          }
+          if (std::isfinite(rho) && rho > 0.0) {
+            total += rho;
+            count += 1.0;
+          }
+        }
+        density = count > 0.0 ? total / count : 0.0;
+      }
+      for (int q = t.well_ptr[w]; q < t.well_ptr[w + 1]; ++q) {
+        const int e = t.perf_entry[t.well_perfs[q]];
+        const double h = density * 9.80665 * (c.depth_layer[c.wells[e].k] - datum) * 1e-5;
+        c.head_offset[e] = std::isfinite(h) ? h : 0.0;
+      }
+    }
+  }
+  if (t.n_perfs > 0) {
+    std::vector<double> head(t.n_perfs);
+    for (int k = 0; k < t.n_perfs; ++k) head[k] = c.head_offset[t.perf_entry[k]];
+    RF_CUDA(cudaMemcpyAsync(c.d_perf_head.p, head.data(), sizeof(double) * head.size(), cudaMemcpyHostToDevice,
+                            c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+  }
+}
+
 static int step(Ctx& c, double target, RfStepReport* out) {
   RfStepReport rep{};
   RF_CUDA(cudaEventRecord(c.ev0, c.stream));
+  refresh_head_offsets(c);
   double stepped = 0.0;
   int substeps = 0, warning = 0;
   const int max_sub = 100000;
@@ -649,10 +723,6 @@ static int load(Ctx& c, const RfDeck* d) {
   c.tgt_prod_surf = d->target_producer_surface_rate_m3_day;
   c.bhp_min = d->well_bhp_min;
   c.bhp_max = d->well_bhp_max;
-  if (f.gravity && !c.wells.empty()) {
-    c.err = "gravity with wells (completion head offsets) is not implemented by the device path in this ABI version";
-    return RF_ERR_UNSUPPORTED;
-  }
   c.head_offset.assign(c.wells.size(), 0.0);
   // depth of each layer centre and pore volumes
   c.depth_layer.resize(c.nz);

@@ -56,11 +56,12 @@ def waterflood_1d(n_cells: int = 200, steps: int = 100, total_days: float = 1000
 
 def waterflood_3d(nx: int, ny: int, nz: int, seed: int = 7, dx: float = 20.0, dz: float = 2.0,
                   sigma: float = 1.0, corr_cells: float = 5.0, kv_kh: float = 0.1,
-                  rate_per_perf: float = 50.0) -> Deck:
+                  rate_per_perf: float = 50.0, gravity: bool = False) -> Deck:
     """Two-phase waterflood on an nx x ny x nz grid with the 1D deck's fluid and SCAL: ln kh ~
     N(ln 100 mD, sigma) smoothed to `corr_cells` correlation length, kv = kv_kh * kh,
     phi = clip(0.1 + 0.02 z, 0.05, 0.3), inverted five-spot (four corner rate injectors, one
-    centre BHP producer at 250 bar), every layer perforated, initial pressure 300 bar."""
+    centre BHP producer at 250 bar), every layer perforated, initial pressure 300 bar.  With
+    `gravity`, the BHPs are quoted at the shallowest completion and carried down each wellbore."""
     d = Deck(nx, ny, nz, 0.2)
     d.set_cell_dimensions(dx, dx, dz)
     kh, z = lognormal_field((nz, ny, nx), seed, math.log(100.0), sigma, corr_cells)
@@ -71,7 +72,7 @@ def waterflood_3d(nx: int, ny: int, nz: int, seed: int = 7, dx: float = 20.0, dz
     d.set_fluid_compressibilities(1e-5, 1e-5)
     d.set_rock_properties(0.0, 0.0, 1.0, 1.0)
     d.set_capillary_params(0.0, 2.0)
-    d.set_gravity_enabled(False)
+    d.set_gravity_enabled(gravity)
     d.set_initial_pressure(300.0)
     d.set_initial_saturation(0.2)
     d.set_well_control_modes("rate", "pressure")

@@ -73,6 +73,19 @@ def test_waterflood_3d_bicgstab_parity():
     check_rows(rows, hg, hc)
 
 
+def test_waterflood_3d_gravity_with_wells_parity():
+    """Gravity on, with fully perforated wells whose BHPs are quoted at the shallowest completion:
+    the completion heads are refreshed at every report step (12 x 10 x 4, dz 4 m)."""
+    deck = decks.waterflood_3d(12, 10, 4, seed=3, dz=4.0, rate_per_perf=20.0, gravity=True)
+    runs = oracle_runs(deck, 5.0, 3)
+    gpu = ReservoirSimulator.from_deck(deck)
+    state = {}
+    for s in range(3):
+        rg = gpu.step(5.0)
+        gs = gpu.state()
+        check_within_floor(s, gs["pressure"], gs["sat_water"], rg["newton_iterations"], runs, state=state)
+
+
 def test_waterflood_3d_mid_parity_at_rounding_floor():
     """30 x 30 x 10 (9,000 cells): the pressure BiCGStab stops at its 50-iteration cap, so a
     different summation order alone moves the Newton end state by more than 1e-6 in saturation.

@@ -317,3 +317,73 @@ def test_waterflood_1d_material_balance_and_front():
     assert sw[:front // 2].mean() > sw[front // 2:front].mean() > sw[front:].mean()
     last = sim.rate_history()[-1]
     assert last["material_balance_error_m3"] < 1e-6 * 20000.0
+
+
+# tests/physics/wellbore_datum.rs: a 1x1x4 water column in hydrostatic equilibrium with a fully
+# perforated producer; the completion heads carry the datum BHP down the wellbore.
+GRAVITY_M_S2 = 9.80665
+
+
+def _hydrostatic_water_column(gravity=True):
+    layers, dz = 4, 10.0
+    d = Deck(1, 1, layers, 0.2)
+    d.set_cell_dimensions_per_layer(20.0, 20.0, [dz] * layers)
+    d.set_fluid_densities(800.0, 1000.0)
+    d.set_initial_pressure(300.0)
+    d.set_initial_saturation(1.0)
+    d.set_capillary_params(0.0, 2.0)
+    d.set_gravity_enabled(gravity)
+    rho_w = lib().orc_water_inverse_fvf(300.0, 300.0, d.c_w, d.b_w) * 1000.0
+    depth = [d.depth_reference_m + dz * k + 0.5 * dz for k in range(layers)]
+    d.pressure = np.array([300.0 + rho_w * GRAVITY_M_S2 * (depth[k] - depth[0]) * 1e-5 for k in range(layers)])
+    for k in range(layers):
+        d.add_well_with_id(0, 0, k, 290.0, 0.1, 0.0, False, "prod")
+    return d, depth, rho_w
+
+
+def test_wellbore_datum_defaults_to_shallowest_completion():
+    d, depth, rho_w = _hydrostatic_water_column()
+    h = OracleSimulator(d).head_offsets()
+    assert h[0] == 0.0
+    for k in range(1, 4):
+        expected = rho_w * GRAVITY_M_S2 * (depth[k] - depth[0]) * 1e-5
+        assert abs(h[k] - expected) < 1e-4, (k, h[k], expected)
+
+
+def test_wellbore_datum_honours_explicit_datum_and_density():
+    d, depth, _ = _hydrostatic_water_column()
+    for w in d.wells:
+        w.datum_depth_m = depth[-1]
+        w.wellbore_density_kg_m3 = 500.0
+    h = OracleSimulator(d).head_offsets()
+    assert h[-1] == 0.0
+    for k in range(4):
+        assert abs(h[k] - 500.0 * GRAVITY_M_S2 * (depth[k] - depth[-1]) * 1e-5) < 1e-9
+    assert h[0] < 0.0
+
+
+def test_wellbore_datum_head_is_zero_without_gravity():
+    d, _, _ = _hydrostatic_water_column(gravity=False)
+    assert np.all(OracleSimulator(d).head_offsets() == 0.0)
+
+
+def test_jacobian_matches_finite_differences_gravity_with_wells():
+    """Gravity and wells together: the completion heads (refreshed on the assembled state, held
+    fixed through the Newton step as in the reference) enter the connection rows."""
+    d = Deck(3, 3, 4, 0.2)
+    d.set_cell_dimensions(15.0, 15.0, 4.0)
+    d.set_rel_perm_props(0.15, 0.15, 2.0, 2.0, 1.0, 1.0)
+    d.set_fim_corey_table_points(0)
+    d.set_capillary_params(0.0, 2.0)
+    d.set_gravity_enabled(True)
+    d.set_initial_pressure(250.0)
+    d.set_initial_saturation(0.35)
+    d.set_well_control_modes("rate", "pressure")
+    d.set_target_well_rates(20.0, 0.0)
+    for k in range(4):
+        d.add_well_with_id(0, 0, k, 320.0, 0.1, 0.0, True, "INJ")
+        d.add_well_with_id(2, 2, k, 200.0, 0.1, 0.0, False, "PROD")
+    sim = OracleSimulator(d)
+    h = sim.head_offsets()
+    assert h[0] == 0.0 and h[1] == 0.0 and np.all(h[2:] > 0.0)  # datum at the top completions
+    assert _fd_jacobian_check(d, 0.5, perturb_seed=5) < 1e-4
