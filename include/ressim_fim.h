@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define RF_ABI_VERSION 1
+#define RF_ABI_VERSION 2
 
 /* status codes */
 #define RF_OK 0
@@ -124,12 +124,18 @@ typedef struct RfTimePointRates {
   double injector_bhp_limited_fraction;
 } RfTimePointRates;
 
-/* Linear-solve report (FimLinearSolveReport, src/lib/ressim/src/fim/linear/mod.rs:213-230). */
+/* Linear-solve report (FimLinearSolveReport, src/lib/ressim/src/fim/linear/mod.rs:213-230).
+ * backend: RF_BACKEND_FGMRES_CPR or RF_BACKEND_SPARSE_LU (`backend_used`); used_fallback: the
+ * direct LU of a system of at most 512 rows did not converge and CPR-FGMRES ran instead. */
+#define RF_BACKEND_FGMRES_CPR 0
+#define RF_BACKEND_SPARSE_LU 1
 typedef struct RfLinearReport {
   int32_t converged;
   int32_t iterations;
   double rhs_norm;
   double final_residual_norm;
+  int32_t used_fallback;
+  int32_t backend;
 } RfLinearReport;
 
 typedef struct RfCtx RfCtx;
@@ -162,8 +168,9 @@ int32_t rf_rate_history_len(const RfCtx* ctx);
 int32_t rf_rate_history_get(const RfCtx* ctx, int32_t index, RfTimePointRates* out);
 
 /* Linear-solver seam replacing solve_linearized_system for a tail-free system
- * (src/lib/ressim/src/fim/linear/mod.rs:252-260): CPR-FGMRES with block-ILU0 on a 3x3 block
- * CSR matrix given on the host (block row pointers, block columns, row-major 3x3 values). */
+ * (src/lib/ressim/src/fim/linear/mod.rs:252-300): CPR-FGMRES with block-ILU0 on a 3x3 block
+ * CSR matrix given on the host (block row pointers, block columns, row-major 3x3 values).  A
+ * system of at most 512 rows goes to the dense direct LU first, as the reference's routing does. */
 int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* block_row_ptr,
                             const int32_t* block_cols, const double* block_vals,
                             const double* rhs, double* x, RfLinearReport* out);
@@ -190,7 +197,7 @@ int64_t rf_kernel_launches(const RfCtx* ctx);
  * src/lib/ressim/src/reporting.rs:191-243) measured with CUDA events on the context's stream.
  * out (may be NULL) receives up to n values, read before the enable/reset below take effect:
  * ms for assembly, well elimination, CPR build, pressure stage, block-ILU0 smoother, Krylov,
- * update, the BiCGStab kernel alone; then the BiCGStab iteration total, the number of BiCGStab
+ * update, the BiCGStab kernel alone, the direct LU route; then the BiCGStab iteration total, the number of BiCGStab
  * launches timed, and the block count of the reduced matrix.
  * enable > 0 switches the profiler on, 0 off, < 0 leaves it as is; reset != 0 zeroes the totals. */
 int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n);

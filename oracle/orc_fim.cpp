@@ -304,6 +304,8 @@ struct LinReport {
   bool converged = false;
   int iterations = 0;
   double rhs_norm = 0, final_residual_norm = 0;
+  bool used_fallback = false;  // direct route did not converge; CPR-FGMRES result
+  int backend = 0;             // 0: CPR-FGMRES, 1: direct LU
   double reduction() const { return final_residual_norm / rmax(rhs_norm, 1e-30); }
 };
 
@@ -784,6 +786,146 @@ static LinReport solve_with_wells(const Csr& J, const std::vector<double>& rhs, 
   rep.rhs_norm = rn;
   rep.final_residual_norm = frn;
   return rep;
+}
+
+// Direct route for small systems (fim/linear/mod.rs:15, 56-67, 262-300).  With the default
+// FgmresCpr kind on the native target, a full system (cells, well BHPs and perforation rates) of
+// at most 512 rows goes to the sparse direct LU of sparse_lu_debug.rs:148-232 (faer `sp_lu`,
+// then at most two refinement solves, each kept only when it cuts the residual below 95 % of the
+// previous one); when that does not converge, CPR-FGMRES with well elimination runs instead.
+// faer 0.24.4 (Cargo.lock; not part of the reference tree) factors with partial pivoting behind a
+// fill-reducing ordering.  This restatement factors densely with row partial pivoting (the first
+// largest |a_ik| of the column wins), which gives the same solution up to rounding; an exactly
+// zero pivot counts as a failed factorisation.  Storage is column-major and every element is
+// updated in the order of the device's direct solver, so both produce the same bits.
+constexpr int kDirectSolveRows = 512;
+
+struct DenseLu {
+  int n = 0;
+  std::vector<double> a;  // column-major: a[j * n + i]; unit-lower L below the diagonal, U on and above
+  std::vector<int> perm;  // row i of P A is row perm[i] of A
+  bool ok = false;
+};
+
+static DenseLu dense_lu(const Csr& J) {
+  DenseLu f;
+  const int n = J.n;
+  f.n = n;
+  f.a.assign(size_t(n) * n, 0.0);
+  f.perm.resize(n);
+  for (int i = 0; i < n; ++i) {
+    f.perm[i] = i;
+    for (int k = J.ptr[i]; k < J.ptr[i + 1]; ++k) f.a[size_t(J.col[k]) * n + i] += J.val[k];
+  }
+  double* a = f.a.data();
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = std::fabs(a[size_t(k) * n + k]);
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(a[size_t(k) * n + i]) > best) {
+        best = std::fabs(a[size_t(k) * n + i]);
+        p = i;
+      }
+    if (!(best > 0.0)) return f;  // zero (or NaN) pivot column
+    if (p != k) {
+      for (int j = 0; j < n; ++j) std::swap(a[size_t(j) * n + k], a[size_t(j) * n + p]);
+      std::swap(f.perm[k], f.perm[p]);
+    }
+    const double piv = a[size_t(k) * n + k];
+    for (int i = k + 1; i < n; ++i) a[size_t(k) * n + i] = a[size_t(k) * n + i] / piv;
+    for (int j = k + 1; j < n; ++j) {
+      const double u = a[size_t(j) * n + k];
+      if (u == 0.0) continue;
+      for (int i = k + 1; i < n; ++i) {
+        const double l = a[size_t(k) * n + i];
+        if (l != 0.0) a[size_t(j) * n + i] = a[size_t(j) * n + i] - l * u;
+      }
+    }
+  }
+  f.ok = true;
+  return f;
+}
+
+// x = U^-1 L^-1 P b, both triangular solves column by column
+static std::vector<double> dense_lu_solve(const DenseLu& f, const std::vector<double>& b) {
+  const int n = f.n;
+  const double* a = f.a.data();
+  std::vector<double> y(n);
+  for (int i = 0; i < n; ++i) y[i] = b[f.perm[i]];
+  for (int k = 0; k < n; ++k) {
+    const double yk = y[k];
+    if (yk == 0.0) continue;
+    for (int i = k + 1; i < n; ++i) y[i] = y[i] - a[size_t(k) * n + i] * yk;
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    y[k] = y[k] / a[size_t(k) * n + k];
+    const double xk = y[k];
+    if (xk == 0.0) continue;
+    for (int i = 0; i < k; ++i) y[i] = y[i] - a[size_t(k) * n + i] * xk;
+  }
+  return y;
+}
+
+static bool all_finite(const std::vector<double>& v) {
+  for (double x : v)
+    if (!std::isfinite(x)) return false;
+  return true;
+}
+
+// sparse_lu_debug.rs:148-232 (solve)
+static LinReport direct_solve(const Csr& J, const std::vector<double>& rhs) {
+  LinReport rep;
+  const int n = J.n;
+  rep.backend = 1;
+  rep.rhs_norm = vnorm(rhs);
+  const DenseLu f = dense_lu(J);
+  if (!f.ok) {
+    rep.x.assign(n, 0.0);
+    rep.final_residual_norm = rep.rhs_norm;
+    return rep;
+  }
+  const double tol = 1e-12 + 5e-3 * rmax(rep.rhs_norm, F64_EPS);
+  auto residual_of = [&](const std::vector<double>& x) {
+    std::vector<double> ax, r(n);
+    csr_matvec(J, x, ax);
+    for (int i = 0; i < n; ++i) r[i] = rhs[i] - ax[i];
+    return r;
+  };
+  std::vector<double> x = dense_lu_solve(f, rhs);
+  std::vector<double> r = residual_of(x);
+  double rn = vnorm(r);
+  int solves = rn > 0.0 ? 1 : 0;
+  for (int it = 0; it < 2; ++it) {
+    if (!std::isfinite(rn) || rn <= tol) break;
+    const std::vector<double> c = dense_lu_solve(f, r);
+    if (!all_finite(c)) break;
+    std::vector<double> cand(n);
+    for (int i = 0; i < n; ++i) cand[i] = x[i] + c[i];
+    std::vector<double> cr = residual_of(cand);
+    const double crn = vnorm(cr);
+    if (!std::isfinite(crn) || crn >= rn * 0.95) break;
+    x = cand;
+    r = cr;
+    rn = crn;
+    ++solves;
+  }
+  rep.x = x;
+  rep.converged = rn <= tol;
+  rep.iterations = solves;
+  rep.final_residual_norm = rn;
+  return rep;
+}
+
+// solve_linearized_system_with_routing (fim/linear/mod.rs:262-300), native target, FgmresCpr
+static LinReport solve_linearized(const Csr& J, const std::vector<double>& rhs, int n_cells) {
+  if (J.n <= kDirectSolveRows) {
+    LinReport d = direct_solve(J, rhs);
+    if (d.converged) return d;
+    LinReport it = solve_with_wells(J, rhs, n_cells);
+    it.used_fallback = true;
+    return it;
+  }
+  return solve_with_wells(J, rhs, n_cells);
 }
 
 // ============================================================================================

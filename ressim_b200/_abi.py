@@ -3,7 +3,9 @@ from __future__ import annotations
 
 import ctypes as C
 
-RF_ABI_VERSION = 1
+RF_ABI_VERSION = 2
+RF_BACKEND_FGMRES_CPR = 0
+RF_BACKEND_SPARSE_LU = 1
 
 RF_OK = 0
 RF_STEP_WARNING = 1
@@ -97,4 +99,5 @@ class RfLinearReport(C.Structure):
     _fields_ = [
         ("converged", C.c_int32), ("iterations", C.c_int32),
         ("rhs_norm", C.c_double), ("final_residual_norm", C.c_double),
+        ("used_fallback", C.c_int32), ("backend", C.c_int32),
     ]

@@ -65,4 +65,4 @@ EXPORTED_SYMBOLS = (
 )
 
 PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",
-          "bicgstab_kernel")
+          "bicgstab_kernel", "direct_lu")

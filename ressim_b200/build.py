@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libressim_fim.so")
-SOURCES = ["rf_assembly.cu", "rf_linear.cu", "rf_state.cu", "rf_api.cu", "rf_noalloc.cu"]
+SOURCES = ["rf_assembly.cu", "rf_linear.cu", "rf_direct.cu", "rf_state.cu", "rf_api.cu", "rf_noalloc.cu"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
     "-Xcompiler", "-fPIC", "-shared", "--fmad=false", "-Xptxas", "-O3", "-cudart", "static",

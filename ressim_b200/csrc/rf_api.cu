@@ -673,10 +673,6 @@ static int load(Ctx& c, const RfDeck* d) {
   c.ny = d->ny;
   c.nz = d->nz;
   c.n = c.nx * c.ny * c.nz;
-  if (3ll * c.n <= 512) {
-    c.err = "systems of 512 rows or fewer take the reference's direct-LU route, which the device path does not implement";
-    return RF_ERR_UNSUPPORTED;
-  }
   const int n = c.n;
   c.dx = d->dx;
   c.dy = d->dy;
@@ -964,6 +960,9 @@ static void free_ctx(Ctx& c) {
     b->free();
   c.d_bmask.free();
   c.d_ctrl.free();
+  for (auto* b : {&c.d_dir_a, &c.d_dir_lu, &c.d_dir_vec}) b->free();
+  c.d_dir_perm.free();
+  c.dir_rows = 0;
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
   for (cudaEvent_t e : c.ev_pool) cudaEventDestroy(e);
@@ -1134,7 +1133,19 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
     RF_CUDA(cudaMemcpyAsync(c.d_val.p, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, c.stream));
     RF_CUDA(cudaMemcpyAsync(c.d_rhs_red.p, rhs, sizeof(double) * 3 * c.n, cudaMemcpyHostToDevice, c.stream));
     RF_CUDA(cudaStreamSynchronize(c.stream));
-    rf::LinResult r = rf::linear_solve_reduced(c);
+    // systems of at most 512 rows: direct LU first, CPR-FGMRES when it does not converge
+    // (fim/linear/mod.rs:279-300)
+    rf::LinResult r;
+    bool direct_ok = false, fell_back = false;
+    if (rf::direct_rows(c, false) <= rf::kDirectSolveRows) {
+      r = rf::linear_solve_direct(c, false, nullptr);
+      direct_ok = r.converged;
+      fell_back = !direct_ok;
+    }
+    if (!direct_ok) {
+      r = rf::linear_solve_reduced(c);
+      r.used_fallback = fell_back;
+    }
     RF_CUDA(cudaMemcpyAsync(x, c.d_x.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream));
     RF_CUDA(cudaStreamSynchronize(c.stream));
     if (out) {
@@ -1142,6 +1153,8 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
       out->iterations = r.iterations;
       out->rhs_norm = r.rhs_norm;
       out->final_residual_norm = r.final_residual_norm;
+      out->used_fallback = r.used_fallback;
+      out->backend = r.backend;
     }
     return RF_OK;
   });
@@ -1180,7 +1193,7 @@ int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32
     }
     if (enable >= 0) c.profiling = enable > 0;
     if (reset) {
-      for (int k = 0; k < 8; ++k) {
+      for (int k = 0; k < rf::kPhCount; ++k) {
         c.phase_ms[k] = 0.0;
         c.phase_count[k] = 0;
       }

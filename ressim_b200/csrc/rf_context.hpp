@@ -123,6 +123,11 @@ struct Ctx {
   DBuf<double> d_dense;       // N*N dense pressure inverse when N <= 299
   DBuf<int> d_dense_perm;     // its row permutation
   int dense_ok = 0;
+  // direct route of small systems: dense matrix and factors (column-major), vectors, permutation
+  DBuf<double> d_dir_a, d_dir_lu, d_dir_vec;
+  DBuf<int> d_dir_perm;
+  int dir_rows = 0, dir_cs = 0;
+  size_t dir_smem = 0;
   DBuf<double> d_pvec;        // BiCGStab workspace: 10 x N
   DBuf<double> d_partials, d_scal;
   // pinned staging for the step path's small device-to-host readbacks (d2h / d2h_wait below):
@@ -157,8 +162,8 @@ struct Ctx {
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
-  double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  long long phase_count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double phase_ms[9] = {};        // per Phase (kPhCount entries)
+  long long phase_count[9] = {};
   long long* d_bicg_iters = nullptr;  // device counter of BiCGStab iterations
 };
 
@@ -197,8 +202,10 @@ enum Phase {
   kPhKrylov = 5,    // FGMRES SpMV, Gram-Schmidt, candidate and true residual
   kPhUpdate = 6,    // chop/update, wells, substep reductions
   kPhBicgKernel = 7,  // the BiCGStab kernel alone (inside kPhCoarse)
-  kPhCount = 8
+  kPhDirect = 8,      // direct LU route of small systems
+  kPhCount = 9
 };
+static_assert(sizeof(Ctx::phase_ms) / sizeof(double) == kPhCount, "one timing slot per phase");
 
 inline cudaEvent_t prof_event(Ctx& c) {
   if (c.ev_used == c.ev_pool.size()) {

@@ -23,6 +23,8 @@ struct CudaError : std::runtime_error {
   } while (0)
 
 constexpr int kBlock = 256;
+// Full systems of at most this many rows take the direct route (fim/linear/mod.rs:15).
+constexpr int kDirectSolveRows = 512;
 
 inline int blocks_for(long long n, int block = kBlock) {
   long long b = (n + block - 1) / block;

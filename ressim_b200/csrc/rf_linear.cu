@@ -1930,6 +1930,14 @@ LinResult linear_solve_reduced(Ctx& c) {
 }
 
 LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
+  // small systems go to the direct LU first; CPR-FGMRES runs when it does not converge
+  // (fim/linear/mod.rs:279-300)
+  bool fell_back = false;
+  if (direct_rows(c, true) <= kDirectSolveRows) {
+    LinResult d = linear_solve_direct(c, true, &h_dx_tail);
+    if (d.converged) return d;
+    fell_back = true;
+  }
   const int n = c.n;
   const long long n3 = 3ll * n;
   // rhs_red = -res (cell rows); Schur corrects the perforated rows and adds the fill
@@ -2035,6 +2043,7 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
   out.final_residual_norm = full_norm;
   out.converged = lin.converged && full_norm <= tol;
   out.finite = nonfinite == 0;
+  out.used_fallback = fell_back;
   return out;
 }
 

@@ -17,6 +17,8 @@ struct LinResult {
   int iterations = 0;
   double rhs_norm = 0, final_residual_norm = 0;
   bool finite = true;
+  int backend = 0;             // 0: CPR-FGMRES, 1: direct LU
+  bool used_fallback = false;  // the direct LU did not converge and CPR-FGMRES ran instead
 };
 
 // Well Schur elimination + CPR-FGMRES on the reduced system + recovery.  Reads d_res/d_res_tail
@@ -25,6 +27,17 @@ struct LinResult {
 LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail);
 // CPR-FGMRES on an already assembled tail-free system: rhs in d_rhs_red, solution in d_x.
 LinResult linear_solve_reduced(Ctx& c);
+
+// Direct route for systems of at most kDirectSolveRows rows (fim/linear/mod.rs:15, 262-300).
+// Rows of the system the route would factor: the full Newton system (with_wells) or the
+// tail-free cell system.
+int direct_rows(const Ctx& c, bool with_wells);
+// Dense LU with partial pivoting on one thread-block cluster, then one solve and at most two
+// refinement solves (sparse_lu_debug.rs:148-232).  with_wells: the full system from the assembled
+// Jacobian, rhs = -residual, tail solution into *h_dx_tail; otherwise the tail-free system in
+// d_val / d_rhs_red.  The cell solution goes to d_x.  Not converged when a pivot is zero or the
+// residual stays above 1e-12 + 5e-3 |b|.
+LinResult linear_solve_direct(Ctx& c, bool with_wells, std::vector<double>* h_dx_tail);
 
 // Build-once helpers
 void build_levels(Ctx& c);

@@ -28,7 +28,7 @@ def test_abi_struct_sizes_are_stable():
     # explicit layout check: the C side is compiled with the same header
     assert C.sizeof(_abi.RfWell) == 8 * 4 + 8 * 8
     assert C.sizeof(_abi.RfTimePointRates) == 12 * 8
-    assert C.sizeof(_abi.RfLinearReport) == 8 + 16
+    assert C.sizeof(_abi.RfLinearReport) == 8 + 16 + 8
 
 
 def test_setter_validation_matches_reference_messages():
