@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define RF_ABI_VERSION 2
+#define RF_ABI_VERSION 3
 
 /* status codes */
 #define RF_OK 0
@@ -89,9 +89,26 @@ typedef struct RfDeck {
   double target_injector_surface_rate_m3_day; /* NaN: none */
   double target_producer_surface_rate_m3_day; /* NaN: none */
   double well_bhp_min, well_bhp_max;
-  /* three-phase black-oil mode: reserved, must be 0 in this ABI version */
+  /* three-phase black-oil mode (setThreePhaseModeEnabled, frontend.rs:1088-1241) */
   int32_t three_phase_mode;
-  int32_t injected_fluid; /* 0 water, 1 gas */
+  int32_t injected_fluid; /* 0 water, 1 gas (the reference's default); water in two-phase mode */
+  /* PVT table (setPvtTable, pvt.rs:36-104): n_pvt_rows rows of six doubles in input order,
+   * p [bar], Rs [Sm3/Sm3], Bo, mu_o [cP], Bg, mu_g [cP]; the table's undersaturated oil
+   * compressibility is pvt_c_o (the fluid c_o when the table was set) */
+  int32_t n_pvt_rows;
+  const double* pvt_rows;
+  double pvt_c_o;
+  /* three-phase Corey SCAL (setThreePhaseRelPermProps, relperm.rs:199-228); has_scal_3p = 0
+   * keeps the two-phase curves and an immobile gas phase */
+  int32_t has_scal_3p;
+  double s_wc_3p, s_or_3p, n_w_3p, n_o_3p, k_rw_max_3p, k_ro_max_3p;
+  double s_gc, s_gr, s_org, n_g, k_rg_max;
+  /* gas-oil capillary pressure (setGasOilCapillaryParams, capillary.rs:100-172) */
+  int32_t has_pc_og;
+  double pc_og_entry, pc_og_lambda;
+  /* gas properties (setGasFluidProperties) and redissolution (setGasRedissolutionEnabled) */
+  double mu_g, c_g, rho_g;
+  int32_t gas_redissolution_enabled;
 } RfDeck;
 
 /* Per-report-step outcome (FimStepStats subset, src/lib/ressim/src/reporting.rs:191-243). */
@@ -122,6 +139,12 @@ typedef struct RfTimePointRates {
   double avg_water_saturation;
   double producer_bhp_limited_fraction;
   double injector_bhp_limited_fraction;
+  /* three-phase mode (zero otherwise): surface gas produced per day (free plus dissolved), the
+   * mean gas saturation, the cumulative gas material-balance error [Sm3] and the producing GOR */
+  double total_production_gas;
+  double avg_gas_saturation;
+  double material_balance_error_gas_m3;
+  double producing_gor;
 } RfTimePointRates;
 
 /* Linear-solve report (FimLinearSolveReport, src/lib/ressim/src/fim/linear/mod.rs:213-230).

@@ -64,6 +64,9 @@ def lib():
         L.orc_head_offsets.argtypes = [C.c_void_p, _dp, C.c_int32]
         L.orc_assemble_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp, _ip, _ip, _dp, _ip, _ip, _dp]
         L.orc_topology.argtypes = [C.c_void_p, _ip, _ip]
+        L.orc_assemble_state_regimes.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip,
+                                                 _dp, _ip, _ip, _dp]
+        L.orc_blackoil_probe.argtypes = [_dp, C.c_int32, C.c_double, C.c_int32, _dp, _dp]
         _lib = L
     return _lib
 
@@ -90,7 +93,9 @@ class OracleSimulator:
         n = deck.n_cells
         p = np.ascontiguousarray(deck.pressure, dtype=np.float64)
         sw = np.ascontiguousarray(deck.sat_water, dtype=np.float64)
-        lib().orc_set_state(self._h, ptr(p), ptr(sw), None, None, 0.0)
+        sg = np.ascontiguousarray(deck.sat_gas, dtype=np.float64)
+        rs = np.ascontiguousarray(deck.rs, dtype=np.float64)
+        lib().orc_set_state(self._h, ptr(p), ptr(sw), ptr(sg), ptr(rs), 0.0)
         self.n = n
 
     def close(self):
@@ -169,11 +174,41 @@ class OracleSimulator:
         lib().orc_assemble_state(*args, C.byref(nu), C.byref(nnz), ptr(res), iptr(ptr_), iptr(col), ptr(val))
         return res, ptr_, col, val
 
+    def assemble_state_regimes(self, dt, prev, cur, prev_regime, cur_regime, bhp, q):
+        """assemble_state with explicit cell regimes (0 saturated, 1 undersaturated)."""
+        prev = np.ascontiguousarray(prev, dtype=np.float64).ravel()
+        cur = np.ascontiguousarray(cur, dtype=np.float64).ravel()
+        pr = np.ascontiguousarray(prev_regime, dtype=np.int32)
+        cr = np.ascontiguousarray(cur_regime, dtype=np.int32)
+        bhp = np.ascontiguousarray(bhp, dtype=np.float64)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        nu, nnz = C.c_int32(), C.c_int32()
+        args = (self._h, dt, ptr(prev), ptr(cur), iptr(pr), iptr(cr), ptr(bhp) if bhp.size else None,
+                ptr(q) if q.size else None)
+        lib().orc_assemble_state_regimes(*args, C.byref(nu), C.byref(nnz), None, None, None, None)
+        res = np.zeros(nu.value)
+        ptr_ = np.zeros(nu.value + 1, dtype=np.int32)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        val = np.zeros(nnz.value)
+        lib().orc_assemble_state_regimes(*args, C.byref(nu), C.byref(nnz), ptr(res), iptr(ptr_), iptr(col), ptr(val))
+        return res, ptr_, col, val
+
     def initial_well_state(self, n_wells, n_perfs):
         b = np.zeros(max(n_wells, 1))
         q = np.zeros(max(n_perfs, 1))
         lib().orc_initial_well_state(self._h, ptr(b), ptr(q))
         return b[:n_wells], q[:n_perfs]
+
+
+def blackoil_probe(rows, c_o, mode, inputs, n_out=16):
+    """orc_blackoil_probe: black-oil known-answer evaluations on a PVT table (see orc_driver.inc)."""
+    r = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(-1, 6))
+    x = np.ascontiguousarray(np.asarray(inputs, dtype=np.float64))
+    out = np.zeros(n_out)
+    rc = lib().orc_blackoil_probe(ptr(r), len(r), float(c_o), int(mode), ptr(x), ptr(out))
+    if rc != 0:
+        raise ValueError(f"probe mode {mode} rejected")
+    return out
 
 
 def linear_solve_csr(ptr_, col, val, rhs, n_cells):

@@ -1,6 +1,6 @@
-// ORACLE — test infrastructure only (see orc_core.hpp).  Two-phase oil-water physics of the
-// reference FIM path: PVT, Corey relperm (tabulated), capillary pressure, cell properties,
-// accumulation, face flux and the AD well model.
+// ORACLE — test infrastructure only (see orc_core.hpp).  Physics of the reference FIM path:
+// PVT, relative permeability, capillary pressure, cell properties (two-phase oil-water and the
+// three-phase black-oil regimes), accumulation, face flux and the AD well model.
 #pragma once
 
 #include <map>
@@ -8,6 +8,7 @@
 #include <tuple>
 
 #include "../include/ressim_fim.h"
+#include "orc_blackoil.hpp"
 #include "orc_core.hpp"
 
 namespace orc {
@@ -57,7 +58,18 @@ struct Sim {
   std::vector<double> dz, porosity, kx, ky, kz;
   double mu_o = 1, mu_w = 0.5, c_o = 1e-5, c_w = 3e-6, rho_o = 800, rho_w = 1000;
   double b_o = 1, b_w = 1, p_wref = 300, c_r = 0, p_rref = 300, depth_ref = 0;
-  double rho_g = 10.0;  // default gas density; the gas phase carries no flow in two-phase mode
+  double rho_g = 10.0;  // surface gas density [kg/m3] (frontend.rs:117)
+  // three-phase black-oil (frontend.rs:1011-1241); absent parts keep the reference's defaults
+  bool three_phase = false;
+  bool has_pvt = false;
+  PvtTable pvt;
+  bool has_scal3 = false;
+  Scal3 scal3{};
+  bool has_pc_og = false;
+  double pcog_entry = 0.0, pcog_lambda = 2.0;
+  double mu_g = 0.02, c_g = 1e-4;
+  int injected_fluid = 1;  // 0 water, 1 gas (InjectedFluid::Gas is the reference default)
+  bool gas_redissolution = true;
   bool gravity = false;
   double s_wc = 0.1, s_or = 0.1, n_w = 2, n_o = 2, krw_max = 1, kro_max = 1;
   int table_points = 21;
@@ -71,7 +83,7 @@ struct Sim {
   std::vector<double> pressure, sat_water, sat_oil, sat_gas, rs;
   double time_days = 0;
   std::vector<RfTimePointRates> rate_history;
-  double cum_inj = 0, cum_prod = 0, cum_mb = 0, cum_mb_oil = 0;
+  double cum_inj = 0, cum_prod = 0, cum_mb = 0, cum_mb_oil = 0, cum_mb_gas = 0;
   std::string last_warning;
   Topo topo;
 
@@ -117,10 +129,58 @@ inline S base_oil_fvf_g(const Sim& s, const S& p) {
   return max_floor(sc<S>(s.b_o) * s_exp(p * (-s.c_o)), 1e-9);
 }
 inline double base_oil_fvf(const Sim& s, double p) { return rmax(s.b_o * std::exp(-s.c_o * p), 1e-9); }
+// ---- simulator-level black-oil accessors (pvt.rs:628-1009) ----
+// get_b_g (pvt.rs:835-841)
+inline double get_b_g(const Sim& s, double p) { return s.has_pvt ? pvt_interpolate(s.pvt, p).bg : 1.0; }
+// get_mu_g (pvt.rs:665-671)
+inline double get_mu_g(const Sim& s, double p) { return s.has_pvt ? pvt_interpolate(s.pvt, p).mu_g : s.mu_g; }
+// get_b_o_for_rs (pvt.rs:792-803)
+inline double get_b_o_for_rs(const Sim& s, double p, double rs) {
+  if (!s.has_pvt) return base_oil_fvf(s, p);
+  if (!s.three_phase) return pvt_interpolate(s.pvt, p).bo;
+  double bo, mu;
+  pvt_interpolate_oil(s.pvt, p, rs, bo, mu);
+  return bo;
+}
+// get_mu_o_for_rs (pvt.rs:649-659)
+inline double get_mu_o_for_rs(const Sim& s, double p, double rs) {
+  if (!s.has_pvt) return s.mu_o;
+  if (!s.three_phase) return pvt_interpolate(s.pvt, p).mu_o;
+  double bo, mu;
+  pvt_interpolate_oil(s.pvt, p, rs, bo, mu);
+  return mu;
+}
+// get_b_o_cell / get_mu_o_cell (pvt.rs:636-647, 769-779): the simulator's Rs of the cell
+inline double get_b_o_cell(const Sim& s, int id, double p) { return get_b_o_for_rs(s, p, s.rs[id]); }
+inline double get_mu_o_cell(const Sim& s, int id, double p) { return get_mu_o_for_rs(s, p, s.rs[id]); }
+// get_mu_o_for_rs_generic / get_mu_g_generic (pvt.rs:674-693)
 template <class S>
-inline S oil_density_g(const Sim& s, const S& p) {
+inline S mu_o_for_rs_g(const Sim& s, const S& p, const S& rs) {
+  if (!s.has_pvt) return sc<S>(s.mu_o);
+  if (!s.three_phase) return pvt_saturated_g(s.pvt, p).mu_o;
+  S bo, mu;
+  pvt_oil_g(s.pvt, p, rs, bo, mu);
+  return mu;
+}
+template <class S>
+inline S mu_g_g(const Sim& s, const S& p) {
+  return s.has_pvt ? pvt_saturated_g(s.pvt, p).mu_g : sc<S>(s.mu_g);
+}
+// oil_density_generic / gas_density_generic (pvt.rs:988-1009)
+template <class S>
+inline S oil_density_g(const Sim& s, const S& p, const S& rs) {
+  if (s.has_pvt) {
+    S bo, mu;
+    pvt_oil_g(s.pvt, p, rs, bo, mu);
+    return (sc<S>(s.rho_o) + rs * s.rho_g) / max_floor(bo, 1e-9);
+  }
   S bo = max_floor(sc<S>(s.b_o) * s_exp(p * (-s.c_o)), 1e-9);
   return sc<S>(s.rho_o) / bo;
+}
+template <class S>
+inline S gas_density_g(const Sim& s, const S& p) {
+  if (s.has_pvt) return sc<S>(s.rho_g) / max_floor(pvt_saturated_g(s.pvt, p).bg, 1e-9);
+  return sc<S>(s.rho_g);
 }
 
 // ---- relperm (relperm.rs:491-629) ----
@@ -188,43 +248,201 @@ inline S capillary_pressure_g(const Sim& s, const S& sw) {
   return min_ceil(max_floor(pc, 0.0), pc_max);
 }
 
-// ---- mobility (mobility.rs:196-249 generic; 114-149 f64) ----
+// ---- mobility (mobility.rs:114-149 f64; 196-249 generic) ----
 template <class S>
 struct Mob {
   S w, o, g;
 };
 template <class S>
-inline Mob<S> phase_mobilities_g(const Sim& s, const S& sw) {
+inline Mob<S> phase_mobilities_g(const Sim& s, const S& sw, const S& sg, const S& p, const S& rs) {
+  const S mu_w = sc<S>(s.mu_w);
+  Mob<S> m;
+  if (s.three_phase) {
+    if (!s.has_scal3) {
+      S krw, kro;
+      corey_analytic_g(s, sw, krw, kro);
+      m.w = krw / mu_w;
+      m.o = kro / mu_o_for_rs_g(s, p, rs);
+      m.g = sc<S>(0.0);
+      return m;
+    }
+    m.w = k_rw3_g(s.scal3, sw) / mu_w;
+    m.o = k_ro_stone2_g(s.scal3, sw, sg) / mu_o_for_rs_g(s, p, rs);
+    m.g = k_rg3_g(s.scal3, sg) / mu_g_g(s, p);
+    return m;
+  }
   S krw, kro;
   two_phase_relperm_g(s, sw, krw, kro);
-  Mob<S> m;
-  m.w = krw / sc<S>(s.mu_w);
-  m.o = kro / sc<S>(s.mu_o);
+  m.w = krw / mu_w;
+  m.o = kro / mu_o_for_rs_g(s, p, rs);
   m.g = sc<S>(0.0);
   return m;
 }
-inline Mob<double> phase_mobilities_f64(const Sim& s, double sw) {
+inline Mob<double> phase_mobilities_f64(const Sim& s, double sw, double sg, double p, double rs) {
+  if (s.three_phase) {
+    if (!s.has_scal3) return Mob<double>{k_rw(s, sw) / s.mu_w, k_ro(s, sw) / get_mu_o_for_rs(s, p, rs), 0.0};
+    return Mob<double>{k_rw3(s.scal3, sw) / s.mu_w, k_ro_stone2(s.scal3, sw, sg) / get_mu_o_for_rs(s, p, rs),
+                       k_rg3(s.scal3, sg) / get_mu_g(s, p)};
+  }
   double krw, kro;
   two_phase_relperm_g(s, sw, krw, kro);
-  return Mob<double>{krw / s.mu_w, kro / s.mu_o, 0.0};
+  return Mob<double>{krw / s.mu_w, kro / get_mu_o_for_rs(s, p, rs), 0.0};
 }
 
-// ---- cell properties (properties.rs:37-73, two-phase branch) ----
+// ---- the gas flash (step.rs:65-200, fim/flash_ad.rs:25-207, fim/flash.rs:13-160) ----
+// solve_rs_for_dissolved_gas: 64 bisection steps on dissolved(rs) = So PV rs / Bo(p, rs)
+inline double solve_rs_plain(const Sim& s, double p, double sw, double sg, double pv, double dissolved,
+                             double rs_upper) {
+  if (!s.has_pvt) return 0.0;
+  const double target = rmax(dissolved, 0.0);
+  if (target <= 0.0 || rs_upper <= 0.0) return 0.0;
+  const double so = rmax(1.0 - sw - sg, 0.0);
+  if (so <= 1e-12 || pv <= 0.0) return 0.0;
+  double lo = 0.0, hi = rmax(rs_upper, 0.0);
+  for (int i = 0; i < 64; ++i) {
+    const double mid = 0.5 * (lo + hi);
+    double bo, mu;
+    pvt_interpolate_oil(s.pvt, p, mid, bo, mu);
+    const double d = (so * pv / rmax(bo, 1e-9)) * mid;
+    if (d < target)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// split_gas_inventory_after_transport (step.rs:106-200), gas redissolution enabled
+inline void split_gas_plain(const Sim& s, double p, double pv, double sw, double free_sc, double dissolved_sc,
+                            double& sg, double& so, double& rs) {
+  const double total_hc = rmax(1.0 - sw, 0.0);
+  const double bg = rmax(get_b_g(s, p), 1e-9);
+  const double free_t = rmax(free_sc, 0.0);
+  const double sg_t = rclamp((free_t * bg) / rmax(pv, 1e-9), 0.0, total_hc);
+  const double dissolved = rmax(dissolved_sc, 0.0);
+  const double rs_max = rmax(pvt_interpolate(s.pvt, p).rs, 0.0);
+  const double total_gas = free_t + dissolved;
+  double bo_sat_raw, mu;
+  pvt_interpolate_oil(s.pvt, p, rs_max, bo_sat_raw, mu);
+  const double bo_sat = rmax(bo_sat_raw, 1e-9), rs_sat = rs_max;
+  const double max_all = (total_hc * pv / bo_sat) * rs_sat;
+  if (total_gas <= max_all + 1e-9) {
+    rs = solve_rs_plain(s, p, sw, 0.0, pv, total_gas, rs_sat);
+    sg = 0.0;
+    so = total_hc;
+    return;
+  }
+  const double denom = (1.0 / bg) - (rs_sat / bo_sat);
+  const double sg_sat = std::fabs(denom) > 1e-12 ? ((total_gas / pv) - (total_hc * rs_sat / bo_sat)) / denom : sg_t;
+  sg = rclamp(sg_sat, 0.0, total_hc);
+  so = rmax(total_hc - sg, 0.0);
+  rs = rs_sat;
+}
+
+// dissolved_gas_value_generic (flash_ad.rs:29-43)
+template <class S>
+inline S dissolved_gas_g(const Sim& s, const S& p, const S& rs, const S& so, const S& pv) {
+  S bo = sc<S>(1.0), mu;
+  if (s.has_pvt) pvt_oil_g(s.pvt, p, rs, bo, mu);
+  return (so * pv / max_floor(bo, 1e-9)) * rs;
+}
+// solve_rs_for_dissolved_gas_generic (flash_ad.rs:46-100): the plain bisection's root, with its
+// derivative from one implicit-function Newton step
+template <class S>
+inline S solve_rs_g(const Sim& s, const S& p, const S& sw, const S& sg, const S& pv, const S& dissolved,
+                    double rs_upper) {
+  const double rs_star = solve_rs_plain(s, val(p), val(sw), val(sg), val(pv), val(dissolved), rs_upper);
+  S so = max_floor(sc<S>(1.0) - sw - sg, 0.0);
+  S target = max_floor(dissolved, 0.0);
+  const double dgdrs = dissolved_gas_g<Ad<1>>(s, ad_const<1>(val(p)), ad_var<1>(rs_star, 0),
+                                              ad_const<1>(val(so)), ad_const<1>(val(pv)))
+                           .d[0];
+  if (std::fabs(dgdrs) < 1e-14) return sc<S>(rs_star);
+  S g = dissolved_gas_g<S>(s, p, sc<S>(rs_star), so, pv) - target;
+  return sc<S>(rs_star) - g / dgdrs;
+}
+// split_gas_inventory_after_transport_generic (flash_ad.rs:104-207), redissolution enabled
+template <class S>
+inline void split_gas_g(const Sim& s, const S& p, const S& pv, const S& sw, const S& free_sc, const S& dissolved_sc,
+                        S& sg, S& so, S& rs) {
+  const PvtTable& t = s.pvt;
+  S total_hc = max_floor(sc<S>(1.0) - sw, 0.0);
+  S bg = max_floor(pvt_saturated_g(t, p).bg, 1e-9);
+  S free_t = max_floor(free_sc, 0.0);
+  S sg_t = min_of(max_floor((free_t * bg) / max_floor(pv, 1e-9), 0.0), total_hc);
+  S dissolved = max_floor(dissolved_sc, 0.0);
+  S rs_max = max_floor(pvt_saturated_g(t, p).rs, 0.0);
+  S total_gas = free_t + dissolved;
+  S bo_sat_raw, mu;
+  pvt_oil_g(t, p, rs_max, bo_sat_raw, mu);
+  S bo_sat = max_floor(bo_sat_raw, 1e-9);
+  S rs_sat = rs_max;
+  S max_all = (total_hc * pv / bo_sat) * rs_sat;
+  if (val(total_gas) <= val(max_all) + 1e-9) {
+    rs = solve_rs_g(s, p, sw, sc<S>(0.0), pv, total_gas, val(rs_sat));
+    sg = sc<S>(0.0);
+    so = total_hc;
+    return;
+  }
+  S denom = s_recip(bg) - (rs_sat / bo_sat);
+  S sg_sat = std::fabs(val(denom)) > 1e-12 ? ((total_gas / pv) - (total_hc * rs_sat / bo_sat)) / denom : sg_t;
+  sg = min_of(max_of(sg_sat, sc<S>(0.0)), total_hc);
+  so = max_floor(total_hc - sg, 0.0);
+  rs = rs_sat;
+}
+
+// classify_cell_regime (flash.rs:13-40): 0 saturated, 1 undersaturated
+inline int classify_cell_regime(const Sim& s, double p, double sg, double rs) {
+  if (!s.three_phase || !s.has_pvt) return 0;
+  if (sg > 1e-9) return 0;
+  const double rs_sat = pvt_interpolate(s.pvt, p).rs;
+  return rs < rs_sat - 1e-6 ? 1 : 0;
+}
+
+// ---- cell properties (properties.rs:37-133) ----
 template <class S>
 struct Props {
   S so, sg, rs, bo, bg;
 };
 template <class S>
-inline Props<S> cell_props_g(const Sim& s, const S& p, const S& sw, const S& hc) {
+inline Props<S> cell_props_g(const Sim& s, int regime, const S& p, const S& sw, const S& hc) {
   const S one = sc<S>(1.0);
   const S raw_total = one - sw;
-  const S total = max_floor(raw_total, 0.0);
   Props<S> pr;
-  pr.sg = min_of(max_floor(hc, 0.0), total);
-  pr.so = max_floor(one - sw - pr.sg, 0.0);
-  pr.bo = base_oil_fvf_g(s, p);
-  pr.rs = sc<S>(0.0);
-  pr.bg = sc<S>(1.0);
+  if (!s.three_phase || !s.has_pvt) {
+    const S total = max_floor(raw_total, 0.0);
+    pr.sg = min_of(max_floor(hc, 0.0), total);
+    pr.so = max_floor(one - sw - pr.sg, 0.0);
+    pr.bo = base_oil_fvf_g(s, p);
+    pr.rs = sc<S>(0.0);
+    pr.bg = sc<S>(1.0);
+    return pr;
+  }
+  const PvtTable& t = s.pvt;
+  S mu;
+  if (regime == 0) {
+    pr.sg = hc;
+    pr.rs = pvt_saturated_g(t, p).rs;
+    pr.so = raw_total - pr.sg;
+    pvt_oil_g(t, p, pr.rs, pr.bo, mu);
+    pr.bg = pvt_saturated_g(t, p).bg;
+    return pr;
+  }
+  S rs_cap = max_floor(pvt_saturated_g(t, p).rs, 0.0);
+  const S& rs_trial = hc;
+  if (val(rs_trial) <= val(rs_cap) + 1e-6) {
+    pr.sg = sc<S>(0.0);
+    pr.so = raw_total;
+    pr.rs = rs_trial;
+  } else {
+    S bo_t;
+    pvt_oil_g(t, p, rs_trial, bo_t, mu);
+    bo_t = max_floor(bo_t, 1e-9);
+    S dissolved = raw_total * rs_trial / bo_t;
+    split_gas_g(s, p, sc<S>(1.0), sw, sc<S>(0.0), dissolved, pr.sg, pr.so, pr.rs);
+  }
+  pvt_oil_g(t, p, pr.rs, pr.bo, mu);
+  pr.bg = pvt_saturated_g(t, p).bg;
   return pr;
 }
 
@@ -241,26 +459,27 @@ inline void component_inventory_g(const Sim& s, const S& pv, const S& p, const S
   out[2] = pv * pr.sg / max_floor(pr.bg, 1e-9) + out[1] * pr.rs;
 }
 
-// properties.rs:171-212
+// properties.rs:171-212: the previous inventory is evaluated with the previous regime
 template <class S>
-inline void cell_accumulation_g(const Sim& s, int cell, const S& p, const S& sw, const S& hc,
-                                double pp, double psw, double phc, S out[3]) {
-  Props<S> pr = cell_props_g(s, p, sw, hc);
+inline void cell_accumulation_g(const Sim& s, int cell, int regime, const S& p, const S& sw, const S& hc,
+                                double pp, double psw, double phc, int pregime, S out[3]) {
+  Props<S> pr = cell_props_g(s, regime, p, sw, hc);
   S pv = pore_volume_g(s, cell, p);
   S cur[3];
   component_inventory_g(s, pv, p, sw, pr, cur);
-  Props<double> ppr = cell_props_g<double>(s, pp, psw, phc);
+  Props<double> ppr = cell_props_g<double>(s, pregime, pp, psw, phc);
   double ppv = pore_volume_g<double>(s, cell, pp);
   double prev[3];
   component_inventory_g<double>(s, ppv, pp, psw, ppr, prev);
   for (int c = 0; c < 3; ++c) out[c] = cur[c] - prev[c];
 }
 
-// ---- face flux (flux.rs:42-118) ----
+// ---- face flux (flux.rs:42-191) ----
 template <class S>
 struct FaceIn {
   S p, sw, hc;
   double depth;
+  int regime;
 };
 template <class S>
 inline S gravity_head_g(const Sim& s, double di, double dj, const S& ri, const S& rj) {
@@ -268,23 +487,29 @@ inline S gravity_head_g(const Sim& s, double di, double dj, const S& ri, const S
   S avg = (ri + rj) * 0.5;
   return avg * (GRAVITY * (di - dj) * 1e-5);
 }
+// gas_oil_capillary_pressure_generic (flux.rs:137-142)
+template <class S>
+inline S gas_oil_pc_g(const Sim& s, const S& sg) {
+  if (s.has_pc_og && s.has_scal3) return pc_og_g(s.scal3, s.pcog_entry, s.pcog_lambda, sg);
+  return sc<S>(0.0);
+}
 template <class S>
 inline void face_flux_g(const Sim& s, double geom_t, const FaceIn<S>& i, const FaceIn<S>& j,
                         S flux[3]) {
-  Props<S> pi = cell_props_g(s, i.p, i.sw, i.hc);
-  Props<S> pj = cell_props_g(s, j.p, j.sw, j.hc);
+  Props<S> pi = cell_props_g(s, i.regime, i.p, i.sw, i.hc);
+  Props<S> pj = cell_props_g(s, j.regime, j.p, j.sw, j.hc);
   S rwi = water_density_g(s, i.p), rwj = water_density_g(s, j.p);
-  S roi = oil_density_g(s, i.p), roj = oil_density_g(s, j.p);
-  S rgi = sc<S>(s.rho_g), rgj = sc<S>(s.rho_g);
+  S roi = oil_density_g(s, i.p, pi.rs), roj = oil_density_g(s, j.p, pj.rs);
+  S rgi = gas_density_g(s, i.p), rgj = gas_density_g(s, j.p);
   S pcwi = capillary_pressure_g(s, i.sw), pcwj = capillary_pressure_g(s, j.sw);
-  S pcogi = sc<S>(0.0), pcogj = sc<S>(0.0);
+  S pcogi = gas_oil_pc_g(s, pi.sg), pcogj = gas_oil_pc_g(s, pj.sg);
   S gw = gravity_head_g(s, i.depth, j.depth, rwi, rwj);
   S go = gravity_head_g(s, i.depth, j.depth, roi, roj);
   S gg = gravity_head_g(s, i.depth, j.depth, rgi, rgj);
   S dphi_w = (i.p - j.p) - (pcwi - pcwj) - gw;
   S dphi_o = (i.p - j.p) - go;
   S dphi_g = (i.p - j.p) + (pcogi - pcogj) - gg;
-  Mob<S> mi = phase_mobilities_g(s, i.sw), mj = phase_mobilities_g(s, j.sw);
+  Mob<S> mi = phase_mobilities_g(s, i.sw, pi.sg, i.p, pi.rs), mj = phase_mobilities_g(s, j.sw, pj.sg, j.p, pj.rs);
   S mob_w, p_w, mob_o, bo_o, rs_o, mob_g, bg_g;
   if (val(dphi_w) >= 0.0) {
     mob_w = mi.w;
@@ -417,55 +642,96 @@ inline Control physical_well_control(const Sim& s, int w) {
   return c;
 }
 
-// derive_cell two-phase (state.rs:823-854, flash.rs:43-72)
+// resolve_cell_flash (flash.rs:43-160), gas redissolution enabled
+struct Flash {
+  int regime;
+  double so, sg, rs;
+};
+inline Flash resolve_cell_flash(const Sim& s, double p, double sw, double hc, int regime) {
+  const double raw_total = 1.0 - sw;
+  const double bounded_total = rmax(raw_total, 0.0);
+  if (!s.three_phase || !s.has_pvt) return Flash{regime, bounded_total, 0.0, 0.0};
+  if (regime == 0) {
+    const double sg = hc;
+    const double rs = pvt_interpolate(s.pvt, p).rs;
+    return Flash{regime, raw_total - sg, sg, rs};
+  }
+  const double rs_cap = rmax(pvt_interpolate(s.pvt, p).rs, 0.0);
+  const double rs_trial = hc;
+  if (rs_trial <= rs_cap + 1e-6) return Flash{regime, raw_total, 0.0, rs_trial};
+  const double bo_trial = rmax(get_b_o_for_rs(s, p, rs_trial), 1e-9);
+  const double dissolved = raw_total * rs_trial / bo_trial;
+  Flash f;
+  split_gas_plain(s, p, 1.0, sw, 0.0, dissolved, f.sg, f.so, f.rs);
+  f.regime = f.sg > 1e-12 ? 0 : 1;
+  return f;
+}
+
+// derive_cell (state.rs:823-854)
 struct Derived {
-  double so, sg, rs, bo;
+  double so, sg, rs, bo, bg;
 };
 inline Derived derive_cell(const Sim& s, const Cell& c) {
+  const Flash f = resolve_cell_flash(s, c.p, c.sw, c.hc, c.regime);
   Derived d;
-  d.so = rmax(1.0 - c.sw, 0.0);
-  d.sg = 0.0;
-  d.rs = 0.0;
-  d.bo = base_oil_fvf(s, c.p);
+  d.so = f.so;
+  d.sg = f.sg;
+  d.rs = f.rs;
+  if (s.has_pvt) {
+    double mu;
+    pvt_interpolate_oil(s.pvt, c.p, f.rs, d.bo, mu);
+    d.bg = pvt_interpolate(s.pvt, c.p).bg;
+  } else {
+    d.bo = base_oil_fvf(s, c.p);
+    d.bg = 1.0;
+  }
   return d;
 }
+
+// effective_injected_fluid (fim/wells.rs:618-624): 1 when the injectors inject gas
+inline int injected_fluid(const Sim& s) { return s.three_phase ? s.injected_fluid : 0; }
 
 // fim/wells.rs:1098-1129
 inline bool connection_rate_for_bhp(const Sim& s, const State& st, int perf, double bhp, double& q) {
   const Perf& pf = s.topo.perfs[perf];
-  const RfWell& w = s.wells[pf.entry];
   const Cell& c = st.cells[pf.cell];
-  Mob<double> m = phase_mobilities_f64(s, c.sw);
+  const Derived d = derive_cell(s, c);
+  Mob<double> m = phase_mobilities_f64(s, c.sw, d.sg, c.p, d.rs);
   if (!pf.has_wi) return false;
   const double mob = rmax(m.w + m.o + m.g, 0.0);
   const double raw = pf.wi * mob * (c.p - (bhp + s.head_offset[pf.entry]));
-  (void)w;
   if (!std::isfinite(raw)) return false;
   q = pf.injector ? rmin(raw, 0.0) : rmax(raw, 0.0);
   return true;
 }
 
-// producer_control_state (fim/wells.rs:834-859), two-phase
+// producer_control_state (fim/wells.rs:834-859)
 struct ProducerState {
-  double wf, of, gf, bo;
+  double wf, of, gf, bo, bg, rs;
 };
 inline ProducerState producer_control_state(const Sim& s, const Cell& c) {
-  Mob<double> m = phase_mobilities_f64(s, c.sw);
+  const Derived d = derive_cell(s, c);
+  Mob<double> m = phase_mobilities_f64(s, c.sw, d.sg, c.p, d.rs);
   const double lw = rmax(m.w, 0.0), lo = rmax(m.o, 0.0), lg = rmax(m.g, 0.0);
   const double lt = rmax(lw + lo + lg, F64_EPS);
   ProducerState p;
   p.wf = rclamp(lw / lt, 0.0, 1.0);
   p.of = rclamp(lo / lt, 0.0, 1.0);
   p.gf = rclamp(lg / lt, 0.0, 1.0);
-  p.bo = rmax(base_oil_fvf(s, c.p), 1e-9);
+  p.bo = rmax(d.bo, 1e-9);
+  p.bg = rmax(d.bg, 1e-9);
+  p.rs = rmax(d.rs, 0.0);
   return p;
 }
 
-// fim/wells.rs:1147-1170 (injected fluid is water in two-phase mode)
+// fim/wells.rs:1147-1170
 inline double perforation_surface_rate_sc_day(const Sim& s, const State& st, int perf, double q) {
   const Perf& pf = s.topo.perfs[perf];
   const Cell& c = st.cells[pf.cell];
-  if (pf.injector) return rmax(-q, 0.0) * water_inverse_fvf_g(s, c.p);
+  if (pf.injector) {
+    if (injected_fluid(s) == 1) return rmax(-q, 0.0) / rmax(derive_cell(s, c).bg, 1e-9);
+    return rmax(-q, 0.0) * water_inverse_fvf_g(s, c.p);
+  }
   ProducerState ps = producer_control_state(s, c);
   return rmax(q, 0.0) * ps.of / rmax(ps.bo, 1e-9);
 }
@@ -535,6 +801,7 @@ inline bool solve_bhp_from_target(const Sim& s, const State& st, int w, double& 
 template <class S>
 struct WellCell {
   S p, sw, hc;
+  int regime;
 };
 template <class S>
 struct Fractions {
@@ -544,7 +811,8 @@ struct Fractions {
 template <class S>
 inline Fractions<S> producer_fractions_g(const Sim& s, const WellCell<S>& c) {
   S lw = sc<S>(0.0), lo = sc<S>(0.0), lg = sc<S>(0.0);
-  Mob<S> m = phase_mobilities_g(s, c.sw);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  Mob<S> m = phase_mobilities_g(s, c.sw, pr.sg, c.p, pr.rs);
   lw = lw + max_floor(m.w, 0.0);
   lo = lo + max_floor(m.o, 0.0);
   lg = lg + max_floor(m.g, 0.0);
@@ -559,18 +827,25 @@ inline Fractions<S> producer_fractions_g(const Sim& s, const WellCell<S>& c) {
 template <class S>
 inline S connection_rate_g(const Sim& s, double wi, double head, bool injector, const WellCell<S>& c,
                            const S& bhp) {
-  Mob<S> m = phase_mobilities_g(s, c.sw);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  Mob<S> m = phase_mobilities_g(s, c.sw, pr.sg, c.p, pr.rs);
   S cm = max_floor(m.w + m.o + m.g, 0.0);
   S raw = (cm * (c.p - bhp - sc<S>(head))) * wi;
   if (injector) return val(raw) < 0.0 ? raw : sc<S>(0.0);
   return val(raw) > 0.0 ? raw : sc<S>(0.0);
 }
-// component_rate_coefficients_generic (wells_ad.rs:161-201), water injection
+// component_rate_coefficients_generic (wells_ad.rs:161-201)
 template <class S>
 inline void component_coefficients_g(const Sim& s, bool injector, const WellCell<S>& c,
                                      const Fractions<S>* f, S out[3]) {
-  Props<S> pr = cell_props_g(s, c.p, c.sw, c.hc);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
   if (injector) {
+    if (injected_fluid(s) == 1) {
+      out[0] = sc<S>(0.0);
+      out[1] = sc<S>(0.0);
+      out[2] = s_recip(max_floor(pr.bg, 1e-9));
+      return;
+    }
     out[0] = water_inverse_fvf_g(s, c.p);
     out[1] = sc<S>(0.0);
     out[2] = sc<S>(0.0);
@@ -586,8 +861,12 @@ inline void component_coefficients_g(const Sim& s, bool injector, const WellCell
 template <class S>
 inline S perforation_surface_rate_g(const Sim& s, bool injector, const WellCell<S>& c,
                                     const Fractions<S>* f, const S& q) {
-  Props<S> pr = cell_props_g(s, c.p, c.sw, c.hc);
-  if (injector) return max_floor(-q, 0.0) * water_inverse_fvf_g(s, c.p);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  if (injector) {
+    S clamped = max_floor(-q, 0.0);
+    if (injected_fluid(s) == 1) return clamped / max_floor(pr.bg, 1e-9);
+    return clamped * water_inverse_fvf_g(s, c.p);
+  }
   return max_floor(q, 0.0) * f->of / max_floor(pr.bo, 1e-9);
 }
 template <class S>

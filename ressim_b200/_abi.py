@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-RF_ABI_VERSION = 2
+RF_ABI_VERSION = 3
 RF_BACKEND_FGMRES_CPR = 0
 RF_BACKEND_SPARSE_LU = 1
 
@@ -68,6 +68,18 @@ class RfDeck(C.Structure):
         ("well_bhp_min", C.c_double), ("well_bhp_max", C.c_double),
         ("three_phase_mode", C.c_int32),
         ("injected_fluid", C.c_int32),
+        ("n_pvt_rows", C.c_int32),
+        ("pvt_rows", _dp),
+        ("pvt_c_o", C.c_double),
+        ("has_scal_3p", C.c_int32),
+        ("s_wc_3p", C.c_double), ("s_or_3p", C.c_double), ("n_w_3p", C.c_double), ("n_o_3p", C.c_double),
+        ("k_rw_max_3p", C.c_double), ("k_ro_max_3p", C.c_double),
+        ("s_gc", C.c_double), ("s_gr", C.c_double), ("s_org", C.c_double), ("n_g", C.c_double),
+        ("k_rg_max", C.c_double),
+        ("has_pc_og", C.c_int32),
+        ("pc_og_entry", C.c_double), ("pc_og_lambda", C.c_double),
+        ("mu_g", C.c_double), ("c_g", C.c_double), ("rho_g", C.c_double),
+        ("gas_redissolution_enabled", C.c_int32),
     ]
 
 
@@ -89,6 +101,7 @@ class RfTimePointRates(C.Structure):
         "total_production_liquid_reservoir", "total_injection", "total_injection_reservoir",
         "material_balance_error_m3", "material_balance_error_oil_m3", "avg_reservoir_pressure",
         "avg_water_saturation", "producer_bhp_limited_fraction", "injector_bhp_limited_fraction",
+        "total_production_gas", "avg_gas_saturation", "material_balance_error_gas_m3", "producing_gor",
     )]
 
     def as_dict(self) -> dict:

@@ -91,6 +91,18 @@ class Deck:
     well_bhp_min: float = -100.0
     well_bhp_max: float = 2000.0
     three_phase_mode: bool = False
+    # three-phase black-oil (frontend.rs:1011-1241)
+    injected_fluid: str = "gas"  # InjectedFluid::Gas is the reference's default
+    pvt_rows: list = None
+    pvt_c_o: float = 0.0
+    scal_3p: tuple = None
+    pc_og: tuple = None
+    mu_g: float = 0.02
+    c_g: float = 1e-4
+    rho_g: float = 10.0
+    gas_redissolution_enabled: bool = True
+    sat_gas: np.ndarray = None
+    rs: np.ndarray = None
 
     def __post_init__(self):
         n = self.nx * self.ny * self.nz
@@ -108,6 +120,10 @@ class Deck:
             self.pressure = np.full(n, 300.0)
         if self.sat_water is None:
             self.sat_water = np.full(n, 0.3)
+        if self.sat_gas is None:
+            self.sat_gas = np.zeros(n)
+        if self.rs is None:
+            self.rs = np.zeros(n)
 
     # ---- geometry / rock (frontend.rs:573-640, 1291-1324) ----
     @property
@@ -245,6 +261,64 @@ class Deck:
     def set_fim_corey_table_points(self, points):
         self.corey_table_points = int(points)
 
+    # ---- three-phase black-oil (frontend.rs:1011-1241) ----
+    def set_three_phase_mode_enabled(self, enabled):
+        self.three_phase_mode = bool(enabled)
+
+    def set_three_phase_rel_perm_props(self, s_wc, s_or, s_gc, s_gr, s_org, n_w, n_o, n_g, k_rw_max, k_ro_max,
+                                       k_rg_max):
+        if s_wc + s_or + s_gc + s_gr >= 1.0:
+            raise ValueError("Invalid saturation endpoints: S_wc + S_or + S_gc + S_gr must be < 1.0, got "
+                             f"{s_wc + s_or + s_gc + s_gr}")
+        if s_wc + s_org >= 1.0:
+            raise ValueError(f"Invalid saturation endpoints: S_wc + S_org must be < 1.0, got {s_wc + s_org}")
+        if n_w <= 0.0 or n_o <= 0.0 or n_g <= 0.0:
+            raise ValueError(f"Corey exponents must be positive, got n_w={n_w}, n_o={n_o}, n_g={n_g}")
+        self.scal_3p = tuple(float(v) for v in (s_wc, s_or, n_w, n_o, k_rw_max, k_ro_max, s_gc, s_gr, s_org, n_g,
+                                                 k_rg_max))
+
+    def set_gas_oil_capillary_params(self, p_entry, lam):
+        if p_entry < 0.0:
+            raise ValueError(f"Gas-oil capillary entry pressure must be non-negative, got {p_entry}")
+        if lam <= 0.0:
+            raise ValueError(f"Gas-oil capillary lambda must be positive, got {lam}")
+        self.pc_og = (float(p_entry), float(lam))
+
+    def set_gas_fluid_properties(self, mu_g, c_g, rho_g):
+        if mu_g <= 0.0:
+            raise ValueError(f"Gas viscosity must be positive, got {mu_g}")
+        if c_g < 0.0:
+            raise ValueError(f"Gas compressibility must be non-negative, got {c_g}")
+        if rho_g <= 0.0:
+            raise ValueError(f"Gas density must be positive, got {rho_g}")
+        self.mu_g, self.c_g, self.rho_g = float(mu_g), float(c_g), float(rho_g)
+
+    def set_gas_redissolution_enabled(self, enabled):
+        self.gas_redissolution_enabled = bool(enabled)
+
+    def set_injected_fluid(self, fluid):
+        f = fluid.lower()
+        if f not in ("water", "gas"):
+            raise ValueError(f"Unknown injected fluid '{f}'; expected 'water' or 'gas'")
+        self.injected_fluid = f
+
+    def set_pvt_table(self, rows):
+        """setPvtTable: the table takes the current oil compressibility, and every cell gets the
+        saturated Rs at its pressure."""
+        from .pvt import PvtTable
+
+        table = PvtTable(rows, self.c_o)
+        self.pvt_rows = [r.as_tuple() for r in table.rows]
+        self.pvt_c_o = table.c_o
+        self.rs = np.array([table.interpolate(float(p)).rs_m3m3 for p in self.pressure])
+
+    def set_initial_rs(self, rs):
+        self.rs = np.full(self.n_cells, float(rs))
+
+    def set_initial_gas_saturation(self, sat_gas):
+        sg = min(max(float(sat_gas), 0.0), 1.0)
+        self.sat_gas = np.minimum(sg, 1.0 - np.asarray(self.sat_water, dtype=np.float64))
+
     # ---- wells and controls (frontend.rs:125-345, 430-520) ----
     def add_well(self, i, j, k, bhp, well_radius, skin, injector, physical_well_id=None):
         if not (0 <= i < self.nx and 0 <= j < self.ny and 0 <= k < self.nz):
@@ -376,5 +450,18 @@ class Deck:
         d.target_injector_surface_rate_m3_day = _nan(self.target_injector_surface_rate_m3_day)
         d.target_producer_surface_rate_m3_day = _nan(self.target_producer_surface_rate_m3_day)
         d.three_phase_mode = int(self.three_phase_mode)
-        d.injected_fluid = 0
+        d.injected_fluid = 1 if self.injected_fluid == "gas" else 0
+        if self.pvt_rows:
+            d.n_pvt_rows = len(self.pvt_rows)
+            d.pvt_rows = arr(np.array(self.pvt_rows, dtype=np.float64), 6 * len(self.pvt_rows))
+            d.pvt_c_o = float(self.pvt_c_o)
+        if self.scal_3p is not None:
+            d.has_scal_3p = 1
+            (d.s_wc_3p, d.s_or_3p, d.n_w_3p, d.n_o_3p, d.k_rw_max_3p, d.k_ro_max_3p, d.s_gc, d.s_gr, d.s_org,
+             d.n_g, d.k_rg_max) = self.scal_3p
+        if self.pc_og is not None:
+            d.has_pc_og = 1
+            d.pc_og_entry, d.pc_og_lambda = self.pc_og
+        d.mu_g, d.c_g, d.rho_g = self.mu_g, self.c_g, self.rho_g
+        d.gas_redissolution_enabled = int(self.gas_redissolution_enabled)
         return d, keep

@@ -124,6 +124,53 @@ def ensemble_variant(index: int, seed: int = 1000, steps: int = 40, dt_days: flo
     return d
 
 
+def black_oil_3d(nx: int, ny: int, nz: int, seed: int = 7, dx: float = 20.0, dz: float = 2.0, sigma: float = 1.0,
+                 corr_cells: float = 5.0, kv_kh: float = 0.1, rate_per_perf: float = 20.0,
+                 producer_bhp: float = 150.0, pb_bar: float = 200.0, p_init: float = 250.0,
+                 gravity: bool = True, pc_og: bool = False, injected_fluid: str = "water") -> Deck:
+    """Three-phase black-oil inverted five-spot: the 3D deck's seeded field statistics (ln kh ~
+    N(ln 100 mD, sigma), kv = kv_kh kh, phi = clip(0.1 + 0.02 z, 0.05, 0.3)); a correlation PVT
+    table (API 35, gas gravity 0.75, 80 C, bubble point `pb_bar`, 20 rows to 300 bar, c_o 1e-4/bar);
+    Corey three-phase SCAL with Stone II (Swc = Sor = 0.1, Sgc = Sgr = 0.05, Sorg = 0.15, nw = no = 2,
+    ng = 1.5); initial pressure `p_init` with the saturated Rs and no free gas; gravity on; four
+    corner rate injectors of `injected_fluid` and a centre BHP producer at `producer_bhp`, every
+    layer perforated."""
+    from .pvt import black_oil_table
+
+    d = Deck(nx, ny, nz, 0.2)
+    d.set_cell_dimensions(dx, dx, dz)
+    kh, z = lognormal_field((nz, ny, nx), seed, math.log(100.0), sigma, corr_cells)
+    d.set_permeability_field(kh, kh, kv_kh * kh)
+    d.set_porosity_field(np.clip(0.1 + 0.02 * z, 0.05, 0.3))
+    d.set_rel_perm_props(0.1, 0.1, 2.0, 2.0, 1.0, 1.0)
+    d.set_fluid_properties(1.0, 0.5)
+    d.set_fluid_compressibilities(1e-4, 3e-6)
+    d.set_fluid_densities(800.0, 1000.0)
+    d.set_rock_properties(1e-6, 0.0, 1.1, 1.0)
+    d.set_capillary_params(0.0, 2.0)
+    d.set_gravity_enabled(gravity)
+    d.set_initial_pressure(p_init)
+    d.set_initial_saturation(0.1)
+    d.set_three_phase_mode_enabled(True)
+    d.set_three_phase_rel_perm_props(0.1, 0.1, 0.05, 0.05, 0.15, 2.0, 2.0, 1.5, 1.0, 1.0, 1.0)
+    d.set_gas_fluid_properties(0.02, 1e-4, 10.0)
+    if pc_og:
+        d.set_gas_oil_capillary_params(0.5, 2.0)
+    d.set_pvt_table(black_oil_table(35.0, 0.75, 80.0, pb_bar, 300.0, 20, 1e-4))
+    d.set_initial_gas_saturation(0.0)
+    d.set_injected_fluid(injected_fluid)
+    d.set_well_control_modes("rate", "pressure")
+    d.set_target_well_rates(rate_per_perf * nz, 0.0)
+    d.set_well_bhp_limits(50.0, 600.0)
+    corners = [(0, 0), (nx - 1, 0), (0, ny - 1), (nx - 1, ny - 1)]
+    for n, (i, j) in enumerate(corners):
+        for k in range(nz):
+            d.add_well_with_id(i, j, k, 400.0, 0.1, 0.0, True, f"INJ{n + 1}")
+    for k in range(nz):
+        d.add_well_with_id(nx // 2, ny // 2, k, producer_bhp, 0.1, 0.0, False, "PROD")
+    return d
+
+
 def mixed_precision_deck(seed: int = 7) -> Deck:
     """The 2M-cell waterflood (200 x 200 x 50) of the mixed-precision configuration."""
     return waterflood_3d(200, 200, 50, seed=seed)
@@ -131,7 +178,7 @@ def mixed_precision_deck(seed: int = 7) -> Deck:
 
 def deck_digest(d: Deck) -> str:
     h = hashlib.sha256()
-    for a in (d.dz, d.porosity, d.perm_x, d.perm_y, d.perm_z, d.pressure, d.sat_water):
+    for a in (d.dz, d.porosity, d.perm_x, d.perm_y, d.perm_z, d.pressure, d.sat_water, d.sat_gas, d.rs):
         h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
     for w in d.wells:
         h.update(repr((w.i, w.j, w.k, w.bhp, w.injector, w.physical_well_id)).encode())

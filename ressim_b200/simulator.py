@@ -59,7 +59,9 @@ class ReservoirSimulator(Deck):
         self._h, self._keep = h, (d, keep)
         p = np.ascontiguousarray(self.pressure, dtype=np.float64)
         sw = np.ascontiguousarray(self.sat_water, dtype=np.float64)
-        rc = L.rf_set_state(h, _ptr(p), _ptr(sw), None, None, float(self.time_days))
+        sg = np.ascontiguousarray(self.sat_gas, dtype=np.float64)
+        rs = np.ascontiguousarray(self.rs, dtype=np.float64)
+        rc = L.rf_set_state(h, _ptr(p), _ptr(sw), _ptr(sg), _ptr(rs), float(self.time_days))
         if rc != _abi.RF_OK:
             raise DeviceError(f"rf_set_state failed ({rc}): {_lib.last_error(h)}")
         return h

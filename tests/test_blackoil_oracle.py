@@ -1,0 +1,205 @@
+"""Three-phase black-oil pieces of the oracle against the reference's own known answers.
+
+Restated from the reference's unit tests: PVTO/PVDG interpolation and the Rs-knot derivative
+(src/lib/ressim/src/pvt.rs:1048-1265), regime classification and the derived cell state
+(fim/flash.rs:166-187, fim/state.rs:1105-1181).  Stone II is checked against its formula
+(relperm.rs:336-351) and its AD derivative against central differences; the assembled black-oil
+Jacobian against central differences of the residual in both regimes (fim/numjac.rs:13-40).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle_py import OracleSimulator, blackoil_probe
+from ressim_b200 import decks
+
+PVTO = [(50.0, 20.0, 1.10, 1.00, 0.02, 0.015), (350.0, 20.0, 1.0675, 1.030, 0.02, 0.015),
+        (150.0, 80.0, 1.25, 0.70, 0.008, 0.018), (350.0, 80.0, 1.2252, 0.714, 0.008, 0.018)]
+TWO_ROW = [(100.0, 10.0, 1.1, 1.2, 0.01, 0.02), (200.0, 20.0, 1.0, 1.1, 0.005, 0.02)]
+
+
+def oil_segment(r0, r1, t):
+    inv_bo = (1.0 / r0[2]) + t * (1.0 / r1[2] - 1.0 / r0[2])
+    inv_bo_mu = (1.0 / (r0[2] * r0[3])) + t * (1.0 / (r1[2] * r1[3]) - 1.0 / (r0[2] * r0[3]))
+    return 1.0 / inv_bo, inv_bo / inv_bo_mu
+
+
+def test_pvto_interpolates_inverse_bo_and_inverse_bo_mu_in_pressure_and_rs():
+    low = oil_segment(PVTO[0], PVTO[1], 1.0 / 3.0)
+    high = oil_segment(PVTO[2], PVTO[3], 0.5)
+    t = 0.5
+    inv_bo = 1.0 / low[0] + t * (1.0 / high[0] - 1.0 / low[0])
+    inv_bo_mu = 1.0 / (low[0] * low[1]) + t * (1.0 / (high[0] * high[1]) - 1.0 / (low[0] * low[1]))
+    expected = (1.0 / inv_bo, inv_bo / inv_bo_mu)
+    out = blackoil_probe(PVTO, 1e-4, 1, [200.0, 50.0])
+    assert abs(out[0] - expected[0]) < 1e-14 and abs(out[1] - expected[1]) < 1e-14
+    assert abs(out[2] - out[0]) < 1e-14 and abs(out[3] - out[1]) < 1e-14
+
+
+def test_pvto_rs_knot_uses_left_extreme_guided_derivative():
+    rows = PVTO + [(250.0, 140.0, 1.40, 0.50, 0.005, 0.022), (350.0, 140.0, 1.3861, 0.505, 0.005, 0.022)]
+    h = 1e-4
+    at = blackoil_probe(rows, 1e-4, 1, [200.0, 80.0])
+    left = blackoil_probe(rows, 1e-4, 1, [200.0, 80.0 - h])
+    assert abs(at[5] - (at[0] - left[0]) / h) < 1e-8
+    assert abs(at[7] - (at[1] - left[1]) / h) < 1e-8
+
+
+def test_pvdg_segment_interpolates_inverse_bg_and_inverse_bg_mu():
+    rows = [(150.0, 10.0, 1.0, 1.0, 0.008, 0.018), (250.0, 20.0, 1.0, 1.0, 0.005, 0.022)]
+    row = blackoil_probe(rows, 1e-5, 0, [200.0])
+    inv_bg = 0.5 * (1.0 / 0.008 + 1.0 / 0.005)
+    inv_bg_mu = 0.5 * (1.0 / (0.008 * 0.018) + 1.0 / (0.005 * 0.022))
+    assert abs(row[4] - 1.0 / inv_bg) < 1e-15
+    assert abs(row[5] - inv_bg / inv_bg_mu) < 1e-15
+    gen = blackoil_probe(rows, 1e-5, 2, [200.0])
+    assert abs(gen[2] - row[4]) < 1e-15 and abs(gen[4] - row[5]) < 1e-15
+
+
+def test_table_bg_derivative_uses_the_active_segment():
+    rows = [(100.0, 10.0, 1.2, 1.0, 0.01, 0.02), (200.0, 20.0, 1.1, 1.0, 0.0065, 0.02),
+            (300.0, 30.0, 1.0, 1.0, 0.005, 0.02)]
+
+    def expected(p, lp, lbg, hp, hbg):
+        slope = (1.0 / hbg - 1.0 / lbg) / (hp - lp)
+        inv_bg = 1.0 / lbg + (p - lp) * slope
+        return -slope / (inv_bg * inv_bg)
+
+    assert abs(blackoil_probe(rows, 1e-5, 2, [200.0])[7] - expected(200.0, 100.0, 0.01, 200.0, 0.0065)) < 1e-15
+    assert abs(blackoil_probe(rows, 1e-5, 2, [250.0])[7] - expected(250.0, 200.0, 0.0065, 300.0, 0.005)) < 1e-15
+    assert abs(blackoil_probe(rows, 1e-5, 2, [300.0])[7] + 0.005 / 300.0) < 1e-15
+
+
+def test_saturated_curve_extrapolation_and_bubble_point():
+    rows = [(100.0, 10.0, 1.1, 1.2, 0.01, 0.02), (200.0, 20.0, 1.0, 1.1, 0.005, 0.02)]
+    above = blackoil_probe(rows, 1e-4, 0, [260.0])
+    assert above[1] == 20.0
+    assert abs(above[2] - 1.0 * np.exp(-1e-4 * 60.0)) < 1e-15
+    assert abs(above[4] - 0.005 * 200.0 / 260.0) < 1e-15
+    below = blackoil_probe(rows, 1e-4, 0, [50.0])
+    assert tuple(below[:6]) == rows[0]
+    assert blackoil_probe(rows, 1e-4, 3, [15.0])[0] == 150.0
+    assert blackoil_probe(rows, 1e-4, 3, [5.0])[0] == 100.0
+    assert blackoil_probe(rows, 1e-4, 3, [25.0])[0] == 200.0
+
+
+def test_classifies_undersaturated_cell_and_uses_rs_as_primary():
+    # classifies_undersaturated_cell_without_free_gas (flash.rs:166-187) and
+    # from_simulator_uses_rs_for_undersaturated_cells (state.rs:1105-1137)
+    out = blackoil_probe(TWO_ROW, 1e-5, 4, [150.0, 0.25, 0.0, 12.0])
+    assert out[0] == 1  # undersaturated
+    assert out[1] == 1 and out[2] == 0.75 and out[3] == 0.0 and out[4] == 12.0
+
+
+def test_derive_cell_recovers_saturations_and_props():
+    # derive_cell_recovers_saturations_and_props (state.rs:1140-1181)
+    out = blackoil_probe(TWO_ROW, 1e-5, 4, [150.0, 0.2, 0.1, 0.0])
+    assert out[0] == 0
+    so, sg, bo, bg = out[2], out[3], out[5], out[6]
+    assert abs(sg - 0.1) < 1e-12 and abs(so - 0.7) < 1e-12
+    assert bo > 0.0 and bg > 0.0
+
+
+def test_undersaturated_cell_above_saturated_rs_flashes_gas():
+    """An undersaturated trial Rs above the saturated value at p: the flash keeps the cell's gas
+    inventory and moves the excess to free gas, switching to the saturated regime
+    (flash.rs:117-157, step.rs:106-200)."""
+    p, sw, rs_trial = 150.0, 0.2, 19.0
+    sat = blackoil_probe(TWO_ROW, 1e-5, 0, [p])
+    assert abs(sat[1] - 15.0) < 1e-12
+    bo_trial = blackoil_probe(TWO_ROW, 1e-5, 1, [p, rs_trial])[0]
+    gas_in = (1.0 - sw) * rs_trial / bo_trial
+    regime, so, sg, rs = blackoil_probe(TWO_ROW, 1e-5, 6, [p, sw, rs_trial, 1])[:4]
+    assert regime == 0 and sg > 0.0 and abs(rs - 15.0) < 1e-12 and abs(so + sg - (1 - sw)) < 1e-12
+    bo = blackoil_probe(TWO_ROW, 1e-5, 1, [p, rs])[0]
+    gas_out = sg / sat[4] + so * rs / bo
+    assert abs(gas_out - gas_in) < 1e-12 * gas_in
+    # below the cap the trial Rs is kept and no gas appears
+    regime, so, sg, rs = blackoil_probe(TWO_ROW, 1e-5, 6, [p, sw, 12.0, 1])[:4]
+    assert regime == 1 and sg == 0.0 and rs == 12.0 and so == 1 - sw
+
+
+def test_stone2_value_and_derivatives():
+    scal = [0.1, 0.1, 2.0, 2.0, 1.0, 0.9, 0.05, 0.05, 0.15, 1.5, 0.8]
+    sw, sg = 0.35, 0.2
+    out = blackoil_probe([], 0.0, 5, [sw, sg] + scal)
+    s_wc, s_or, n_w, n_o, krw_max, kro_max, s_gc, s_gr, s_org, n_g, krg_max = scal
+    krw = krw_max * ((sw - s_wc) / (1 - s_wc - s_or)) ** n_w
+    krg = krg_max * ((sg - s_gc) / (1 - s_wc - s_gc - s_gr)) ** n_g
+    kro_w = kro_max * ((1 - sw - s_or) / (1 - s_wc - s_or)) ** n_o
+    kro_g = kro_max * ((1 - s_wc - sg - s_org) / (1 - s_wc - s_org)) ** n_o
+    kro = kro_max * ((kro_w / kro_max + krw) * (kro_g / kro_max + krg) - krw - krg)
+    assert abs(out[0] - krw) < 1e-14 and abs(out[2] - krg) < 1e-14
+    assert abs(out[1] - min(max(kro, 0.0), kro_max)) < 1e-14
+    assert abs(out[3] - out[0]) < 1e-14 and abs(out[4] - out[1]) < 1e-13 and abs(out[5] - out[2]) < 1e-14
+    h = 1e-6
+    fw = (blackoil_probe([], 0.0, 5, [sw + h, sg] + scal)[1] - blackoil_probe([], 0.0, 5, [sw - h, sg] + scal)[1])
+    fg = (blackoil_probe([], 0.0, 5, [sw, sg + h] + scal)[1] - blackoil_probe([], 0.0, 5, [sw, sg - h] + scal)[1])
+    assert abs(out[6] - fw / (2 * h)) < 1e-7 and abs(out[7] - fg / (2 * h)) < 1e-7
+
+
+def _fd_check_blackoil(deck, dt, cur, prev, regimes, seed=0):
+    sim = OracleSimulator(deck)
+    nw, npf = sim.topology()
+    rng = np.random.default_rng(seed)
+    bhp = np.array([w.bhp for w in deck.wells][:nw], dtype=float)
+    q = rng.uniform(5, 20, npf)
+    for k, w in enumerate(deck.wells):
+        q[k] = -q[k] if w.injector else q[k]
+    n = deck.n_cells
+    res, ptr_, col, val = sim.assemble_state_regimes(dt, prev, cur, regimes, regimes, bhp, q)
+    J = np.zeros((len(res), len(res)))
+    for r in range(len(res)):
+        J[r, col[ptr_[r]:ptr_[r + 1]]] = val[ptr_[r]:ptr_[r + 1]]
+    x = np.concatenate([cur.ravel(), bhp, q])
+    worst = 0.0
+    for j in range(len(x)):
+        h = 1e-6 * (1 + abs(x[j]))
+        xp, xm = x.copy(), x.copy()
+        xp[j] += h
+        xm[j] -= h
+
+        def resid(v):
+            return sim.assemble_state_regimes(dt, prev, v[:3 * n].reshape(n, 3), regimes, regimes,
+                                              v[3 * n:3 * n + nw], v[3 * n + nw:])[0]
+        fd = (resid(xp) - resid(xm)) / (2 * h)
+        scale = np.maximum(np.abs(J[:, j]), np.max(np.abs(J[:, j])) * 1e-6 + 1e-8)
+        worst = max(worst, float(np.max(np.abs(fd - J[:, j]) / scale)))
+    return worst
+
+
+@pytest.mark.parametrize("pc_og, fluid", [(False, "water"), (True, "gas")])
+def test_blackoil_jacobian_matches_finite_differences(pc_og, fluid):
+    """Saturated cells with free gas and undersaturated cells below and above the saturated Rs
+    (the split path), gravity, Pc_og and both injected fluids."""
+    d = decks.black_oil_3d(3, 3, 2, seed=2, dz=4.0, pc_og=pc_og, injected_fluid=fluid, rate_per_perf=5.0)
+    n = d.n_cells
+    rng = np.random.default_rng(1)
+    p = rng.uniform(150.0, 190.0, n)
+    sw = rng.uniform(0.15, 0.4, n)
+    regimes = np.array([0, 1] * (n // 2) + [0] * (n % 2), dtype=np.int32)
+    hc = np.where(regimes == 0, rng.uniform(0.05, 0.15, n), 0.0)
+    from ressim_b200.pvt import PvtTable
+    table = PvtTable(d.pvt_rows, d.pvt_c_o)
+    for i in range(n):
+        if regimes[i] == 1:
+            rs_sat = table.interpolate(p[i]).rs_m3m3
+            hc[i] = rs_sat * (0.8 if i % 4 == 1 else 1.05)  # below the cap, or flashing free gas
+    cur = np.stack([p, sw, hc], axis=1)
+    prev = cur.copy()
+    prev[:, 0] += 3.0
+    assert _fd_check_blackoil(d, 0.5, cur, prev, regimes) < 1e-4
+
+
+def test_blackoil_run_conserves_mass():
+    d = decks.black_oil_3d(6, 6, 2, seed=4, rate_per_perf=10.0)
+    sim = OracleSimulator(d)
+    for _ in range(4):
+        rc, rep = sim.step(5.0)
+        assert rc == 0
+    st = sim.state()
+    assert np.max(st["sat_gas"]) > 0.01  # gas came out of solution near the producer
+    h = sim.rate_history()[-1]
+    pore_volume = float(np.sum(d.porosity) * 20.0 * 20.0 * 2.0)
+    assert h["material_balance_error_m3"] < 1e-4 * pore_volume
+    assert h["material_balance_error_oil_m3"] < 1e-4 * pore_volume
+    assert h["producing_gor"] > 0.0 and h["total_production_gas"] > 0.0

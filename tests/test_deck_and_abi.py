@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_struct_sizes_are_stable():
     # explicit layout check: the C side is compiled with the same header
     assert C.sizeof(_abi.RfWell) == 8 * 4 + 8 * 8
-    assert C.sizeof(_abi.RfTimePointRates) == 12 * 8
+    assert C.sizeof(_abi.RfTimePointRates) == 16 * 8
     assert C.sizeof(_abi.RfLinearReport) == 8 + 16 + 8
 
 
