@@ -13,6 +13,7 @@
 // All per-cell work (assembly, norms, linear solve, update, reductions) runs on the device; the
 // host only reads scalars and the perforated cells' state.
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -23,6 +24,8 @@
 #include <thread>
 #include <tuple>
 
+#include "rf_blackoil.cuh"
+#include "rf_fluid.hpp"
 #include "rf_ops.hpp"
 #include "rf_state.hpp"
 
@@ -66,15 +69,64 @@ static WellControlH well_control(const Ctx& c, int w) {
   return k;
 }
 
-// perforated-cell state, 3 doubles per perforation (p, sw, hc)
+// perforated-cell state, 3 doubles per perforation (p, sw, hc), and the regimes (three-phase)
 struct PerfCells {
   std::vector<double> v;
+  std::vector<int> reg;
   double p(int k) const { return v[3 * k]; }
   double sw(int k) const { return v[3 * k + 1]; }
   double hc(int k) const { return v[3 * k + 2]; }
+  int regime(int k) const { return reg.empty() ? 0 : reg[k]; }
 };
 
+static void gather_perf(Ctx& c, const double* p, const double* sw, const double* hc, PerfCells& pc) {
+  if (!c.fluid.three_phase) {
+    gather_perf_cells(c, p, sw, hc, pc.v);
+    pc.reg.clear();
+    return;
+  }
+  std::vector<double> t;
+  gather_perf_cells3(c, p, sw, hc, c.d_reg.p, t);
+  const int P = c.topo.n_perfs;
+  pc.v.resize(3 * size_t(P));
+  pc.reg.resize(P);
+  for (int k = 0; k < P; ++k) {
+    for (int e = 0; e < 3; ++e) pc.v[3 * k + e] = t[4 * k + e];
+    pc.reg[k] = int(t[4 * k + 3]);
+  }
+}
+
+// producer_control_state (fim/wells.rs:834-859), three-phase
+struct ProducerState3 {
+  double wf, of, gf, bo, bg, rs;
+};
+static ProducerState3 producer_state3(const Fluid& f, double p, double sw, const Derived3& d) {
+  const Mob3<double> m = mobilities3_f64(f, sw, d.sg, p, d.rs);
+  const double lw = fmax(m.w, 0.0), lo = fmax(m.o, 0.0), lg = fmax(m.g, 0.0);
+  const double lt = fmax(lw + lo + lg, kF64Eps);
+  ProducerState3 s;
+  s.wf = clamp01(lw / lt, 0.0, 1.0);
+  s.of = clamp01(lo / lt, 0.0, 1.0);
+  s.gf = clamp01(lg / lt, 0.0, 1.0);
+  s.bo = fmax(d.bo, 1e-9);
+  s.bg = fmax(d.bg, 1e-9);
+  s.rs = fmax(d.rs, 0.0);
+  return s;
+}
+
 static bool connection_rate_for_bhp(const Ctx& c, const PerfCells& pc, int k, double bhp, double& q) {
+  if (c.fluid.three_phase) {
+    // fim/wells.rs:1098-1129 with the cell's flashed Sg and Rs
+    const Fluid& f = c.hfluid;
+    const Derived3 d = derive_cell3(f, pc.p(k), pc.sw(k), pc.hc(k), pc.regime(k));
+    const Mob3<double> m = mobilities3_f64(f, pc.sw(k), d.sg, pc.p(k), d.rs);
+    if (!c.topo.perf_has_wi[k]) return false;
+    const double mob = fmax(m.w + m.o + m.g, 0.0);
+    const double raw = c.topo.perf_wi[k] * mob * (pc.p(k) - (bhp + c.head_offset[c.topo.perf_entry[k]]));
+    if (!std::isfinite(raw)) return false;
+    q = c.topo.perf_inj[k] ? fmin(raw, 0.0) : fmax(raw, 0.0);
+    return true;
+  }
   Mob<double> m = mobilities<double>(c.fluid, pc.sw(k));
   if (!c.topo.perf_has_wi[k]) return false;
   const double mob = fmax(m.w + m.o + 0.0, 0.0);
@@ -85,6 +137,17 @@ static bool connection_rate_for_bhp(const Ctx& c, const PerfCells& pc, int k, do
 }
 
 static double surface_rate_sc(const Ctx& c, const PerfCells& pc, int k, double q) {
+  if (c.fluid.three_phase) {
+    // perforation_surface_rate_sc_day (fim/wells.rs:1147-1170)
+    const Fluid& f = c.hfluid;
+    const Derived3 d = derive_cell3(f, pc.p(k), pc.sw(k), pc.hc(k), pc.regime(k));
+    if (c.topo.perf_inj[k]) {
+      if (f.inject_gas) return fmax(-q, 0.0) / fmax(d.bg, 1e-9);
+      return fmax(-q, 0.0) * inv_bw(f, pc.p(k));
+    }
+    const ProducerState3 ps = producer_state3(f, pc.p(k), pc.sw(k), d);
+    return fmax(q, 0.0) * ps.of / fmax(ps.bo, 1e-9);
+  }
   if (c.topo.perf_inj[k]) return fmax(-q, 0.0) * inv_bw(c.fluid, pc.p(k));
   Mob<double> m = mobilities<double>(c.fluid, pc.sw(k));
   const double lw = fmax(m.w, 0.0), lo = fmax(m.o, 0.0), lg = 0.0;
@@ -340,9 +403,12 @@ static NewtonReport run_newton(Ctx& c, WellState& ws, double dt) {
     for (int p = 0; p < P; ++p) cand.q[p] = ws.q[p] + 1.0 * (dx_tail[W + p] * relax);
     double pmax;
     bool finite;
-    apply_cell_update(c, relax, pmax, finite);
+    if (c.fluid.three_phase)
+      apply_cell_update3(c, relax, pmax, finite);
+    else
+      apply_cell_update(c, relax, pmax, finite);
     enforce_control_bounds(c, pmax, cand.bhp);
-    gather_perf_cells(c, c.d_cp.p, c.d_csw.p, c.d_chc.p, pc.v);
+    gather_perf(c, c.d_cp.p, c.d_csw.p, c.d_chc.p, pc);
     relax_wells(c, pc, cand.bhp, cand.q);
     enforce_control_bounds(c, pmax, cand.bhp);
     for (double v : cand.bhp) finite = finite && std::isfinite(v);
@@ -393,7 +459,7 @@ static WellState initial_well_state(Ctx& c) {
   ws.q.assign(P, 0.0);
   for (int w = 0; w < W; ++w) ws.bhp[w] = well_control(c, w).bhp_target;
   PerfCells pc;
-  gather_perf_cells(c, c.d_pp.p, c.d_psw.p, c.d_phc.p, pc.v);
+  gather_perf(c, c.d_pp.p, c.d_psw.p, c.d_phc.p, pc);
   for (int w = 0; w < W; ++w) {
     double b;
     if (solve_bhp_from_target(c, pc, w, b)) ws.bhp[w] = b;
@@ -473,6 +539,84 @@ static void record_step(Ctx& c, const WellState& ws, double dt, double water_cha
   c.rate_history.push_back(r);
 }
 
+// record_fim_step_report, three-phase (reporting.rs:553-734, fim/wells.rs:1634-1667): injector
+// surface rates of water or gas, producer component rates from the flashed cell state, the gas
+// ledger and the producing GOR.  sums: state_sums3 over the written-back state.
+static void record_step3(Ctx& c, const WellState& ws, double dt, double water_change, double oil_removed,
+                         double gas_change, const double sums[kStateQ3]) {
+  const Fluid& f = c.hfluid;
+  PerfCells pc;
+  gather_perf(c, c.d_p.p, c.d_sw.p, c.d_hc.p, pc);
+  double prod_oil = 0, prod_liq = 0, prod_liq_res = 0, inj = 0, inj_res = 0, winj_res = 0, pwat_res = 0, winj_sc = 0,
+         pwat_sc = 0, prod_gas = 0, ginj_sc = 0;
+  int prc = 0, irc = 0, pbl = 0, ibl = 0;
+  for (int w = 0; w < c.topo.n_wells; ++w) {
+    const WellControlH k = well_control(c, w);
+    if (k.enabled && k.rate_controlled) {
+      const double b = ws.bhp[w];
+      const bool lim = k.injector ? b >= k.bhp_limit - 1e-6 : b <= k.bhp_limit + 1e-6;
+      if (k.injector) {
+        irc++;
+        ibl += lim;
+      } else {
+        prc++;
+        pbl += lim;
+      }
+    }
+  }
+  for (int p = 0; p < c.topo.n_perfs; ++p) {
+    const double q = ws.q[p];
+    const Derived3 d = derive_cell3(f, pc.p(p), pc.sw(p), pc.hc(p), pc.regime(p));
+    if (c.topo.perf_inj[p]) {
+      inj_res += fmax(-q, 0.0);
+      if (f.inject_gas) {
+        const double c2 = q / fmax(d.bg, 1e-9);
+        inj += fmax(-c2, 0.0);
+        ginj_sc += fmax(-c2, 0.0);
+        continue;
+      }
+      const double c0 = q * inv_bw(f, pc.p(p));
+      inj += fmax(-c0, 0.0);
+      winj_res += fmax(-q, 0.0);
+      winj_sc += fmax(-c0, 0.0);
+      continue;
+    }
+    const ProducerState3 ps = producer_state3(f, pc.p(p), pc.sw(p), d);
+    const double c0 = q * ps.wf * inv_bw(f, pc.p(p));
+    const double c1 = q * ps.of / fmax(ps.bo, 1e-9);
+    const double c2 = q * ps.gf / fmax(ps.bg, 1e-9) + c1 * ps.rs;
+    prod_gas += fmax(c2, 0.0);
+    prod_liq_res += fmax(q, 0.0);
+    pwat_res += fmax(q, 0.0) * ps.wf;
+    pwat_sc += fmax(c0, 0.0);
+    prod_oil += fmax(c1, 0.0);
+    prod_liq += fmax(c0, 0.0) + fmax(c1, 0.0);
+  }
+  c.cum_inj += winj_res * dt;
+  c.cum_prod += pwat_res * dt;
+  c.cum_mb += (winj_sc - pwat_sc) * dt - water_change;
+  c.cum_mb_oil += prod_oil * dt - oil_removed;
+  c.cum_mb_gas += (ginj_sc - prod_gas) * dt - gas_change;
+  RfTimePointRates r{};
+  r.time = c.time_days + dt;
+  r.total_production_oil = prod_oil;
+  r.total_production_liquid = prod_liq;
+  r.total_production_liquid_reservoir = prod_liq_res;
+  r.total_injection = inj;
+  r.total_injection_reservoir = inj_res;
+  r.material_balance_error_m3 = fabs(c.cum_mb);
+  r.material_balance_error_oil_m3 = fabs(c.cum_mb_oil);
+  r.avg_reservoir_pressure = sums[6] > 0.0 ? sums[5] / sums[6] : 0.0;
+  r.avg_water_saturation = c.n > 0 ? sums[7] / c.n : 0.0;
+  r.producer_bhp_limited_fraction = prc > 0 ? double(pbl) / prc : 0.0;
+  r.injector_bhp_limited_fraction = irc > 0 ? double(ibl) / irc : 0.0;
+  r.total_production_gas = prod_gas;
+  r.avg_gas_saturation = c.n > 0 ? sums[8] / c.n : 0.0;
+  r.material_balance_error_gas_m3 = fabs(c.cum_mb_gas);
+  r.producing_gor = prod_oil > 1e-9 ? prod_gas / prod_oil : 0.0;
+  c.rate_history.push_back(r);
+}
+
 // refresh_well_head_offsets (well_control.rs:192-276), on the state entering a report step: each
 // completion's head carries its physical well's datum BHP along the wellbore, density * g *
 // (depth(k) - datum) * 1e-5 bar.  Datum: the group's first explicit datum_depth_m, else its
@@ -485,8 +629,23 @@ static void refresh_head_offsets(Ctx& c) {
   c.head_offset.assign(c.wells.size(), 0.0);
   if (c.fluid.gravity && t.n_perfs > 0) {
     PerfCells pc;
-    gather_perf_cells(c, c.d_p.p, c.d_sw.p, c.d_hc.p, pc.v);
-    const Fluid& f = c.fluid;
+    std::vector<double> sg_rs;  // three-phase: the simulator's (Sg, Rs, -, -) per perforation
+    if (c.fluid.three_phase) {
+      std::vector<double> a;
+      gather_perf_cells3(c, c.d_p.p, c.d_sw.p, c.d_sg.p, nullptr, a);
+      gather_perf_cells3(c, c.d_rs.p, c.d_rs.p, c.d_rs.p, nullptr, sg_rs);
+      pc.v.resize(3 * size_t(t.n_perfs));
+      for (int k = 0; k < t.n_perfs; ++k) {
+        pc.v[3 * k] = a[4 * k];
+        pc.v[3 * k + 1] = a[4 * k + 1];
+        pc.v[3 * k + 2] = 0.0;
+        sg_rs[4 * k + 1] = sg_rs[4 * k];  // Rs
+        sg_rs[4 * k] = a[4 * k + 2];      // Sg
+      }
+    } else {
+      gather_perf_cells(c, c.d_p.p, c.d_sw.p, c.d_hc.p, pc.v);
+    }
+    const Fluid& f = c.fluid.three_phase ? c.hfluid : c.fluid;
     for (int w = 0; w < t.n_wells; ++w) {
       double datum = NAN, density = NAN;
       for (int q = t.well_ptr[w]; q < t.well_ptr[w + 1]; ++q) {
@@ -515,7 +674,27 @@ static void refresh_head_offsets(Ctx& c) {
           const double p = pc.p(k), sw = pc.sw(k);
           const double rho_w = inv_bw(f, p) * f.rho_w;
           double rho;
-          if (t.perf_inj[k]) {
+          if (f.three_phase) {
+            // producer_control_phase_fractions_for_pressures (well_control.rs:373-398)
+            const double sg = sg_rs[4 * k], rs = sg_rs[4 * k + 1];
+            if (t.perf_inj[k]) {
+              rho = f.inject_gas ? gas_density3<double>(f, p) : rho_w;
+            } else {
+              double lw, lo, lg = 0.0;
+              if (f.has_scal3) {
+                lw = fmax(k_rw3(f, sw) / f.mu_w, 0.0);
+                lo = fmax(k_ro_stone2(f, sw, sg) / mu_o_for_rs(f, p, rs), 0.0);
+                lg = fmax(k_rg3(f, sg) / get_mu_g(f, p), 0.0);
+              } else {
+                lw = fmax(corey_krw(f, sw) / f.mu_w, 0.0);
+                lo = fmax(corey_kro(f, sw) / mu_o_for_rs(f, p, rs), 0.0);
+              }
+              const double lt = fmax(lw + lo + lg, kF64Eps);
+              const double fw = std::clamp(lw / lt, 0.0, 1.0), fo = std::clamp(lo / lt, 0.0, 1.0),
+                           fg = std::clamp(lg / lt, 0.0, 1.0);
+              rho = fw * rho_w + fo * oil_density3<double>(f, p, fmax(rs, 0.0)) + fg * gas_density3<double>(f, p);
+            }
+          } else if (t.perf_inj[k]) {
             rho = rho_w;
           } else {
             const double lw = fmax(corey_krw(f, sw) / f.mu_w, 0.0), lo = fmax(corey_kro(f, sw) / f.mu_o, 0.0);
@@ -570,7 +749,10 @@ static int step(Ctx& c, double target, RfStepReport* out) {
     // (two-phase: zero) gas primary
     RF_CUDA(cudaMemcpyAsync(c.d_pp.p, c.d_p.p, nb, cudaMemcpyDeviceToDevice, c.stream));
     RF_CUDA(cudaMemcpyAsync(c.d_psw.p, c.d_sw.p, nb, cudaMemcpyDeviceToDevice, c.stream));
-    RF_CUDA(cudaMemsetAsync(c.d_phc.p, 0, nb, c.stream));
+    if (c.fluid.three_phase)
+      from_simulator3(c);  // regimes and hc = Sg (saturated) or Rs (undersaturated)
+    else
+      RF_CUDA(cudaMemsetAsync(c.d_phc.p, 0, nb, c.stream));
     const WellState ws0 = initial_well_state(c);
     for (;;) {
       WellState ws = ws0;
@@ -578,6 +760,27 @@ static int step(Ctx& c, double target, RfStepReport* out) {
       rep.newton_iterations += nr.newton_iterations;
       rep.linear_iterations += nr.linear_iterations;
       rep.linear_solves += nr.linear_solves;
+      if (nr.converged && c.fluid.three_phase) {
+        // relative change, and the inventories of the simulator state before the write-back
+        double sb[kStateQ3], sa[kStateQ3];
+        state_sums3(c, c.d_pp.p, c.d_psw.p, c.d_phc.p, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_pp.p, c.d_psw.p, sb);
+        const double rc = sb[1] > 0.0 ? sb[0] / sb[1] : 0.0;
+        errs[0] = errs[1];
+        errs[1] = errs[2];
+        errs[2] = rc;
+        growth = growth_factor(trial, nr.newton_iterations, errs, retry);
+        derive3(c);  // write back So, Sg, Rs
+        for (int p = 0; p < c.topo.n_perfs; ++p) c.wells[c.topo.perf_entry[p]].bhp = ws.bhp[c.topo.perf_well[p]];
+        state_sums3(c, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_p.p, c.d_sw.p, sa);
+        record_step3(c, ws, trial, sa[2] - sb[2], sb[3] - sa[3], sa[4] - sb[4], sa);
+        c.time_days += trial;
+        stepped += trial;
+        last_dt = trial;
+        substeps++;
+        rep.substeps++;
+        rep.last_dt_days = trial;
+        break;
+      }
       if (nr.converged) {
         double sums_prev[7], sums_new[7];
         state_sums(c, c.d_pp.p, c.d_psw.p, c.d_phc.p, c.d_p.p, c.d_sw.p, c.d_hc.p, sums_new);
@@ -666,7 +869,16 @@ static int load(Ctx& c, const RfDeck* d) {
     return RF_ERR_INVALID;
   }
   if (d->three_phase_mode) {
-    c.err = "three-phase mode is not implemented by the device path in this ABI version";
+    if (d->n_pvt_rows < 1 || !d->pvt_rows) {
+      c.err = "three-phase mode without a PVT table is not supported";
+      return RF_ERR_UNSUPPORTED;
+    }
+    if (!d->gas_redissolution_enabled) {
+      c.err = "three-phase mode with gas redissolution disabled (DRSDT0) is not supported";
+      return RF_ERR_UNSUPPORTED;
+    }
+  } else if (d->n_pvt_rows > 0 && d->pvt_rows) {
+    c.err = "a PVT table in two-phase mode is not implemented by the device path";
     return RF_ERR_UNSUPPORTED;
   }
   c.nx = d->nx;
@@ -681,34 +893,8 @@ static int load(Ctx& c, const RfDeck* d) {
   c.kx.assign(d->perm_x, d->perm_x + n);
   c.ky.assign(d->perm_y, d->perm_y + n);
   c.kz.assign(d->perm_z, d->perm_z + n);
-  Fluid& f = c.fluid;
-  f.mu_o = d->mu_o;
-  f.mu_w = d->mu_w;
-  f.c_o = d->c_o;
-  f.c_w = d->c_w;
-  f.rho_o = d->rho_o;
-  f.rho_w = d->rho_w;
-  f.rho_g = 10.0;
-  f.b_o = d->b_o;
-  f.b_w = d->b_w;
-  f.p_wref = d->water_pvt_reference_pressure_bar;
-  f.c_r = d->rock_compressibility;
-  f.p_rref = d->rock_reference_pressure_bar;
-  f.gravity = d->gravity_enabled;
-  f.s_wc = d->s_wc;
-  f.s_or = d->s_or;
-  f.n_w = d->n_w;
-  f.n_o = d->n_o;
-  f.krw_max = d->k_rw_max;
-  f.kro_max = d->k_ro_max;
-  f.table_points = d->corey_table_points;
-  if (f.table_points > kMaxKnots) {
-    c.err = "corey_table_points above 64 is not supported";
-    return RF_ERR_UNSUPPORTED;
-  }
-  f.pc_entry = d->pc_entry;
-  f.pc_lambda = d->pc_lambda;
-  fill_knots(f);
+  if (fluid_from_deck(d, c.fluid, c.h_pvt, c.err) != RF_OK) return RF_ERR_UNSUPPORTED;
+  c.hfluid = c.fluid;
   c.wells.assign(d->wells, d->wells + d->n_wells);
   c.inj_rate_ctl = d->injector_rate_controlled;
   c.prod_rate_ctl = d->producer_rate_controlled;
@@ -897,6 +1083,16 @@ static void setup_device(Ctx& c) {
   upload(c.d_depth, c.depth_layer);
   for (auto* b : {&c.d_p, &c.d_sw, &c.d_hc, &c.d_pp, &c.d_psw, &c.d_phc, &c.d_cp, &c.d_csw, &c.d_chc}) b->alloc(n);
   RF_CUDA(cudaMemset(c.d_hc.p, 0, sizeof(double) * n));
+  if (c.fluid.three_phase) {
+    c.d_reg.alloc(n);
+    for (auto* b : {&c.d_so, &c.d_sg, &c.d_rs}) b->alloc(n);
+    RF_CUDA(cudaMemset(c.d_reg.p, 0, sizeof(int) * n));
+    RF_CUDA(cudaMemset(c.d_sg.p, 0, sizeof(double) * n));
+    RF_CUDA(cudaMemset(c.d_rs.p, 0, sizeof(double) * n));
+    upload(c.d_pvt, c.h_pvt);
+    c.fluid.pvt = c.d_pvt.p;
+    c.hfluid.pvt = c.h_pvt.data();
+  }
   build_pattern(c);
   upload(c.d_row_ptr, c.h_row_ptr);
   upload(c.d_col, c.h_col);
@@ -944,8 +1140,9 @@ static void free_ctx(Ctx& c) {
                   &c.d_jww_ctrl_bhp, &c.d_tinv, &c.d_rhs_red, &c.d_rhs_full, &c.d_dx_tail, &c.d_jrr_perf, &c.d_V,
                   &c.d_Z, &c.d_w, &c.d_x, &c.d_tmp, &c.d_tmp2, &c.d_cand, &c.d_cpr_w, &c.d_pval, &c.d_plu,
                   &c.d_pdiag, &c.d_lu, &c.d_dinv, &c.d_cres, &c.d_full, &c.d_dense, &c.d_pvec, &c.d_partials,
-                  &c.d_scal})
+                  &c.d_scal, &c.d_so, &c.d_sg, &c.d_rs, &c.d_pvt})
     b->free();
+  c.d_reg.free();
   for (auto* b : {&c.d_row_ptr, &c.d_col, &c.d_diag, &c.d_stencil, &c.d_fill_off, &c.d_fill_pos, &c.d_perf_cell,
                   &c.d_perf_well, &c.d_perf_inj, &c.d_perf_has_wi, &c.d_well_ptr, &c.d_well_perfs, &c.d_tinv_off,
                   &c.d_perf_row_off, &c.d_flag_dense, &c.d_dense_perm})
@@ -1050,6 +1247,23 @@ int32_t rf_set_state(RfCtx* ctx, const double* p, const double* sw, const double
   if (!ctx || !p || !sw) return RF_ERR_INVALID;
   return guarded(ctx, [&]() -> int32_t {
     rf::Ctx& c = ctx->c;
+    if (c.fluid.three_phase) {
+      // loadState (frontend.rs:931-1008): So = max(1 - Sw - Sg, 0)
+      const size_t bytes = sizeof(double) * c.n;
+      std::vector<double> hsg(c.n, 0.0), hrs(c.n, 0.0), hso(c.n);
+      if (sg) hsg.assign(sg, sg + c.n);
+      if (rs) hrs.assign(rs, rs + c.n);
+      for (int i = 0; i < c.n; ++i) hso[i] = fmax(1.0 - sw[i] - hsg[i], 0.0);
+      RF_CUDA(cudaMemcpyAsync(c.d_p.p, p, bytes, cudaMemcpyHostToDevice, c.stream));
+      RF_CUDA(cudaMemcpyAsync(c.d_sw.p, sw, bytes, cudaMemcpyHostToDevice, c.stream));
+      RF_CUDA(cudaMemcpyAsync(c.d_sg.p, hsg.data(), bytes, cudaMemcpyHostToDevice, c.stream));
+      RF_CUDA(cudaMemcpyAsync(c.d_rs.p, hrs.data(), bytes, cudaMemcpyHostToDevice, c.stream));
+      RF_CUDA(cudaMemcpyAsync(c.d_so.p, hso.data(), bytes, cudaMemcpyHostToDevice, c.stream));
+      RF_CUDA(cudaMemsetAsync(c.d_hc.p, 0, bytes, c.stream));
+      RF_CUDA(cudaStreamSynchronize(c.stream));
+      c.time_days = t;
+      return RF_OK;
+    }
     for (int i = 0; i < c.n; ++i)
       if (sg && sg[i] != 0.0) {
         c.err = "a nonzero gas saturation needs the three-phase path";
@@ -1072,6 +1286,16 @@ int32_t rf_get_state(const RfCtx* cctx, double* p, double* sw, double* so, doubl
   RfCtx* ctx = const_cast<RfCtx*>(cctx);
   return guarded(ctx, [&]() -> int32_t {
     rf::Ctx& c = ctx->c;
+    if (c.fluid.three_phase) {
+      const size_t bytes = sizeof(double) * c.n;
+      const double* src[5] = {c.d_p.p, c.d_sw.p, c.d_so.p, c.d_sg.p, c.d_rs.p};
+      double* dst[5] = {p, sw, so, sg, rs};
+      for (int a = 0; a < 5; ++a)
+        if (dst[a]) RF_CUDA(cudaMemcpyAsync(dst[a], src[a], bytes, cudaMemcpyDeviceToHost, c.stream));
+      RF_CUDA(cudaStreamSynchronize(c.stream));
+      if (t) *t = c.time_days;
+      return RF_OK;
+    }
     std::vector<double> hp(c.n), hsw(c.n);
     RF_CUDA(cudaMemcpyAsync(hp.data(), c.d_p.p, sizeof(double) * c.n, cudaMemcpyDeviceToHost, c.stream));
     RF_CUDA(cudaMemcpyAsync(hsw.data(), c.d_sw.p, sizeof(double) * c.n, cudaMemcpyDeviceToHost, c.stream));

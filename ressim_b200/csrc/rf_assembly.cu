@@ -329,6 +329,10 @@ __global__ void k_sum_final(int nblocks, const double* __restrict__ partials, do
 
 // ---- host launchers ----
 void launch_assembly(Ctx& c, double dt) {
+  if (c.fluid.three_phase) {
+    launch_assembly3(c, dt);
+    return;
+  }
   const int n = c.n;
   k_cells<<<blocks_for(n, 128), 128, 0, c.stream>>>(c.fluid, c.nx, c.ny, c.nz, dt, c.d_pv.p, c.d_tx.p, c.d_ty.p,
                                                      c.d_tz.p, c.d_depth.p, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_pp.p,
@@ -356,7 +360,12 @@ void launch_norms(Ctx& c, double dt, double* h_out /* kNormQ + 1 */) {
   const int n = c.n;
   int nb = blocks_for(n);
   if (nb > 4 * c.num_sms) nb = 4 * c.num_sms;
-  k_norms_cells<<<nb, kBlock, 0, c.stream>>>(c.fluid, n, dt, c.d_pv.p, c.d_p.p, c.d_res.p, c.d_partials.p);
+  if (c.fluid.three_phase) {
+    launch_norm_partials3(c, dt, nb);
+    c.launches--;  // counted below with the other three launches
+  } else {
+    k_norms_cells<<<nb, kBlock, 0, c.stream>>>(c.fluid, n, dt, c.d_pv.p, c.d_p.p, c.d_res.p, c.d_partials.p);
+  }
   k_norms_final<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, c.d_scal.p);
   k_cnv_violation<<<nb, kBlock, 0, c.stream>>>(n, c.d_pv.p, c.d_res.p, c.d_scal.p, c.d_partials.p);
   k_sum_final<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, c.d_scal.p + kNormQ);

@@ -14,15 +14,6 @@
 
 namespace rf {
 
-// Stencil slot order of a block row: z-, y-, x-, diagonal, x+, y+, z+.  This is also the
-// ascending column order, and the order in which the reference's assembly loop adds face terms
-// into a cell's rows (faces owned by lower-index neighbours first).
-enum { kZm = 0, kYm = 1, kXm = 2, kDiag = 3, kXp = 4, kYp = 5, kZp = 6 };
-
-struct WellControlH {
-  int enabled, rate_controlled, uses_surface_target, has_target, injector;
-  double target_rate, bhp_limit, bhp_target;
-};
 
 struct Topology {
   int n_wells = 0, n_perfs = 0;
@@ -67,7 +58,9 @@ struct Ctx {
   int nx = 0, ny = 0, nz = 0, n = 0;
   double dx = 0, dy = 0;
   std::vector<double> dz, depth_layer, porosity, kx, ky, kz, pv;
-  Fluid fluid{};
+  Fluid fluid{};   // kernels' copy (PVT table pointer in device memory)
+  Fluid hfluid{};  // host controller's copy (PVT table pointer in host memory)
+  std::vector<double> h_pvt;  // flat PVT table (three-phase mode)
   std::vector<RfWell> wells;
   std::vector<double> head_offset;
   int inj_rate_ctl = 0, prod_rate_ctl = 0, inj_enabled = 1;
@@ -78,7 +71,7 @@ struct Ctx {
   std::vector<double> h_p, h_sw, h_so, h_sg, h_rs;
   double time_days = 0;
   std::vector<RfTimePointRates> rate_history;
-  double cum_inj = 0, cum_prod = 0, cum_mb = 0, cum_mb_oil = 0;
+  double cum_inj = 0, cum_prod = 0, cum_mb = 0, cum_mb_oil = 0, cum_mb_gas = 0;
   std::string last_warning;
 
   // block pattern (reduced reservoir system): stencil + well fill
@@ -94,6 +87,9 @@ struct Ctx {
   DBuf<double> d_pv, d_tx, d_ty, d_tz, d_depth;
   DBuf<double> d_p, d_sw, d_hc, d_pp, d_psw, d_phc, d_cp, d_csw, d_chc;
   DBuf<double> d_res, d_val;
+  // three-phase mode: regimes (frozen per Newton attempt), the simulator's So, Sg, Rs, PVT table
+  DBuf<int> d_reg;
+  DBuf<double> d_so, d_sg, d_rs, d_pvt;
   // wells on the device
   DBuf<int> d_perf_cell, d_perf_well, d_perf_inj, d_perf_has_wi, d_well_ptr, d_well_perfs;
   DBuf<double> d_perf_wi, d_perf_head;

@@ -11,6 +11,9 @@ void launch_assembly(Ctx& c, double dt);
 // h_out receives kNormQuantities + 1 doubles (family maxima, FVF sums, CNV maxima, residual
 // sums, pore-volume sum, violating pore volume).
 void launch_norms(Ctx& c, double dt, double* h_out);
+// Three-phase assembly and the first pass of the norms (rf_blackoil.cu).
+void launch_assembly3(Ctx& c, double dt);
+void launch_norm_partials3(Ctx& c, double dt, int nb);
 
 struct LinResult {
   bool converged = false;

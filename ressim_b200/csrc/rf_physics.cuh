@@ -18,8 +18,11 @@
 
 #ifdef __CUDACC__
 #define RF_HD __host__ __device__ __forceinline__
+// large bodies that several call sites share (kept out of line on the device to bound code size)
+#define RF_HD_CALL __host__ __device__ __noinline__ inline
 #else
 #define RF_HD inline
+#define RF_HD_CALL inline
 #endif
 
 namespace rf {
@@ -191,6 +194,17 @@ RF_HD Dual<N> smin(const Dual<N>& a, const Dual<N>& b) {
   return a.v <= b.v ? a : b;
 }
 
+// Stencil slot order of a block row: z-, y-, x-, diagonal, x+, y+, z+.  This is also the
+// ascending column order, and the order in which the reference's assembly loop adds face terms
+// into a cell's rows (faces owned by lower-index neighbours first).
+enum { kZm = 0, kYm = 1, kXm = 2, kDiag = 3, kXp = 4, kYp = 5, kZp = 6 };
+
+// Control of one physical well as the assembly kernels read it (fim/wells.rs:691-798).
+struct WellControlH {
+  int enabled, rate_controlled, uses_surface_target, has_target, injector;
+  double target_rate, bhp_limit, bhp_target;
+};
+
 // ---------------------------------------------------------------------------------------------
 // Fluid / rock / SCAL parameters (plain data, passed by value to kernels)
 // ---------------------------------------------------------------------------------------------
@@ -203,6 +217,17 @@ struct Fluid {
   double pc_entry, pc_lambda;
   double knot_lo, knot_hi, knot_step;
   double knot_x[kMaxKnots], knot_krw[kMaxKnots], knot_kro[kMaxKnots];
+  // three-phase black-oil mode (rf_blackoil.cuh); zero in two-phase mode
+  int three_phase, has_scal3, has_pc_og, inject_gas;
+  double mu_g;
+  double s3_wc, s3_or, s3_nw, s3_no, s3_krw, s3_kro, s3_gc, s3_gr, s3_org, s3_ng, s3_krg;
+  double pcog_entry, pcog_lambda;
+  // PVT table, flat: n_sat saturated rows of (p, rs, bo, mu_o, bg, mu_g); at pvt_hdr one
+  // (rs, first row, row count) triple per undersaturated-oil branch; at pvt_rows the branch rows.
+  // Device memory in the kernels' copy of this struct, host memory in the host's copy.
+  const double* pvt;
+  int pvt_n_sat, pvt_n_br, pvt_hdr, pvt_rows;
+  double pvt_c_o;
 };
 
 // analytic Corey values (relperm.rs:491-520), used to sample the table knots on the host

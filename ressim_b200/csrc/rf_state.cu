@@ -134,6 +134,16 @@ void apply_cell_update(Ctx& c, double relax, double& pmax, bool& finite) {
   finite = h[1] == 0.0;
 }
 
+void max2_final(Ctx& c, int nb, double& pmax, bool& finite) {
+  k_max2_final<<<1, 32, 0, c.stream>>>(nb, c.d_partials.p, c.d_scal.p + 200);
+  c.launches++;
+  double h[2];
+  d2h(c, h, c.d_scal.p + 200, sizeof(h));
+  d2h_wait(c);
+  pmax = h[0];
+  finite = h[1] == 0.0;
+}
+
 void state_sums(Ctx& c, const double* ap, const double* asw, const double* ahc, const double* bp, const double* bsw,
                 const double* bhc, double out[7]) {
   const int nb = red_blocks(c);
