@@ -5,12 +5,13 @@ assembly, well Schur elimination, CPR-FGMRES and the update, including any subst
 on a seeded synthetic waterflood deck, run through the C ABI (`rf_step`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ensemble|72k|2m|1d] [--variants V] [--precision fp64|mixed]
+                    [--workload ensemble|72k|72k-bo|2m|1d] [--variants V] [--precision fp64|mixed]
                     [--dt DAYS] [--no-cpu-baseline]
 
 The default workload is the sensitivity ensemble: 256 two-phase waterflood variants of uneven
 size (3,300 to 64,512 cells, 4.9M cells in all) per GPU, all advanced together one report step at
-a time (rf_batch_step).  `--workload 72k` is the single 60x60x20 deck of the plain FP64 form.
+a time (rf_batch_step).  `--workload 72k-bo` is the single 60x60x20 three-phase black-oil deck of
+the plain FP64 form; `--workload 72k` is the same grid and wells with two-phase oil-water physics.
 
 Legs of the `--impl ours` run:
   value     device time of K report steps with the state resident in HBM, L2 flushed (256 MB
@@ -60,6 +61,11 @@ WORKLOADS = {
             "waterflood_3d 60x60x20 (72,000 cells), two-phase oil-water, log-normal kh (ln-mean ln 100 mD, "
             "sigma 1, 5-cell correlation), kv/kh 0.1, inverted five-spot (4 rate injectors, 1 BHP producer), "
             "no gravity, dt 10 d report steps, FP64"),
+    "72k-bo": (60, 60, 20, 10.0,
+               "black_oil_3d 60x60x20 (72,000 cells), three-phase black-oil (PVT table with bubble point 200 bar, "
+               "Stone II, regime switching, gas flash), log-normal kh (ln-mean ln 100 mD, sigma 1, 5-cell correlation), "
+               "kv/kh 0.1, phi from ln k, gravity on, p_init 250 bar, inverted five-spot (4 water rate injectors, "
+               "1 BHP producer at 150 bar), dt 10 d report steps, FP64"),
     "2m": (200, 200, 50, 10.0,
            "waterflood_3d 200x200x50 (2,000,000 cells), same statistics and wells, dt 10 d report steps, FP64"),
     "1d": (200, 1, 1, 10.0, "waterflood_1d 200x1x1, rate injector cell 0, BHP producer cell 199, dt 10 d, FP64"),
@@ -95,6 +101,8 @@ def make_deck(workload):
         return decks.ensemble_variant(0), dt, desc
     if workload == "1d":
         deck, _, _ = decks.waterflood_1d()
+    elif workload == "72k-bo":
+        deck = decks.black_oil_3d(nx, ny, nz, seed=7)
     else:
         deck = decks.waterflood_3d(nx, ny, nz, seed=7)
     return deck, dt, desc
@@ -242,7 +250,7 @@ def cpu_leg(workload, dt, warmup, steps, budget_s):
         el += time.perf_counter() - t0
         newton += rep.newton_iterations
         st = sim.state()
-        states.append((st["pressure"], st["sat_water"]))
+        states.append((st["pressure"], st["sat_water"], st["sat_gas"]))
         k += 1
         if el >= budget_s:
             break
@@ -561,7 +569,7 @@ def main():
         reps.append(r)
         dev_ms += r["device_ms"]
         st = sim.state()  # outside the device-timed region (rf_step's own events)
-        gpu_states.append((st["pressure"], st["sat_water"]))
+        gpu_states.append((st["pressure"], st["sat_water"], st["sat_gas"]))
         newton += r["newton_iterations"]
         lin += r["linear_iterations"]
         substeps += r["substeps"]
@@ -583,13 +591,18 @@ def main():
     sim2.set_linear_precision(args.precision)
     for _ in range(args.warmup):
         sim2.step(dt)
-    p_host = torch.empty(n, dtype=torch.float64).pin_memory()
-    sw_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    # per-cell state the step reads and writes: p, sw (two-phase); p, sw, sg, rs (three-phase)
+    three = bool(deck.three_phase_mode)
+    keys = ("pressure", "sat_water", "sat_gas", "rs") if three else ("pressure", "sat_water")
     st = sim2.state()
-    p_host.numpy()[:] = st["pressure"]
-    sw_host.numpy()[:] = st["sat_water"]
-    pp = C.cast(p_host.data_ptr(), C.POINTER(C.c_double))
-    sp = C.cast(sw_host.data_ptr(), C.POINTER(C.c_double))
+    bufs = []
+    for key in keys:
+        b = torch.empty(n, dtype=torch.float64).pin_memory()
+        b.numpy()[:] = st[key]
+        bufs.append(b)
+    ptrs = [C.cast(b.data_ptr(), C.POINTER(C.c_double)) for b in bufs]
+    pp, sp = ptrs[0], ptrs[1]
+    gp, rp = (ptrs[2], ptrs[3]) if three else (None, None)
     tt = C.c_double()
     rep = _abi.RfStepReport()
     l2_flush()
@@ -599,14 +612,14 @@ def main():
     e2e_s = 0.0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        rc = L.rf_set_state(h, pp, sp, None, None, C.c_double(sim2.time_days))
+        rc = L.rf_set_state(h, pp, sp, gp, rp, C.c_double(sim2.time_days))
         if rc != 0:
             raise RuntimeError(f"rf_set_state failed: {_lib.last_error(h)}")
         rc = L.rf_step(h, C.c_double(dt), C.byref(rep))
         if rc < 0:
             raise RuntimeError(f"rf_step failed: {_lib.last_error(h)}")
         sim2.time_days = rep.time_days
-        rc = L.rf_get_state(h, pp, sp, None, None, None, C.byref(tt))
+        rc = L.rf_get_state(h, pp, sp, None, gp, rp, C.byref(tt))
         if rc != 0:
             raise RuntimeError(f"rf_get_state failed: {_lib.last_error(h)}")
         e2e_s += time.perf_counter() - t0
@@ -641,7 +654,8 @@ def main():
             ep = max(float(np.max(np.abs(g[0] - c[0]) / np.maximum(np.abs(c[0]), 1.0)))
                      for g, c in zip(gpu_states, cpu_states))
             es = max(float(np.max(np.abs(g[1] - c[1]))) for g, c in zip(gpu_states, cpu_states))
-            field_err = {"pressure_rel": ep, "sat_water_abs": es,
+            eg = max(float(np.max(np.abs(g[2] - c[2]))) for g, c in zip(gpu_states, cpu_states))
+            field_err = {"pressure_rel": ep, "sat_water_abs": es, "sat_gas_abs": eg,
                          "report_steps": [args.warmup + i for i in range(min(len(gpu_states), len(cpu_states)))],
                          "against": "FP64 oracle (C++ restatement of the reference), same deck and steps"}
             cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
@@ -662,8 +676,8 @@ def main():
             "config": {"workload": desc, "cells": n, "dt_days": dt, "parallelism": f"replicas{world}",
                        "l2": "flushed (256 MB write) between timed report steps",
                        "newton_iterations": newton, "linear_iterations": lin, "substeps": substeps},
-            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * n,
-                    "d2h_bytes_per_step": 2 * 8 * n},
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(keys) * 8 * n,
+                    "d2h_bytes_per_step": len(keys) * 8 * n},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
             "phase_ms": phases, "precision": args.precision, "field_error_vs_oracle": field_err,
         }
