@@ -225,6 +225,35 @@ int64_t rf_kernel_launches(const RfCtx* ctx);
  * enable > 0 switches the profiler on, 0 off, < 0 leaves it as is; reset != 0 zeroes the totals. */
 int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n);
 
+/* Controller options; no counterpart in the reference (whose controller picks substeps by its
+ * PID rule and accepts by its CNV/MB tiers).  one_substep_per_report_step != 0 takes every report
+ * step as exactly one substep of the full dt, without retries (a Newton failure ends the step with
+ * a warning); cnv_tol > 0 replaces the CNV tiers with this one tolerance (and mb_tol > 0 the MB
+ * ones), without the pore-volume relaxation.  Both make the converged states smooth functions of
+ * the inputs, which finite-difference checks of the adjoint need.  Defaults: 0, 0, 0. */
+int32_t rf_set_controller_options(RfCtx* ctx, int32_t one_substep_per_report_step, double cnv_tol, double mb_tol);
+
+/* ---- Discrete adjoint (no counterpart in the reference, which has no adjoint).
+ * rf_adjoint_record(ctx, 1) clears the tape and starts recording: every later rf_step checkpoints
+ * the simulator state at its start (p, Sw; So, Sg, Rs in three-phase mode; device copies) and
+ * keeps the dt of each accepted substep.  rf_adjoint_record(ctx, 0) stops recording.
+ * rf_backward runs the backward pass over the recorded report steps: each report step is replayed
+ * from its checkpoint (same substeps, same converged states), then the transposed Newton systems
+ * are solved in reverse time (well Schur complement transposed, CPR-FGMRES with iterative
+ * refinement to 1e-11 relative).  It returns the objective value, its gradient with respect to
+ * the log of each cell's permeability multiplier (kx, ky, kz scaled together; n_cells values) and
+ * with respect to each physical well's active control (its target rate when rate controlled, its
+ * BHP target otherwise; physical wells in order of first appearance, rf_well_count of them).  The
+ * substep sizes are held fixed.  The simulator state is left as it was. */
+#define RF_OBJECTIVE_CUMULATIVE_OIL 0 /* surface oil produced by the producers' connections [Sm3] */
+typedef struct RfObjective {
+  int32_t kind;
+} RfObjective;
+int32_t rf_adjoint_record(RfCtx* ctx, int32_t enable);
+int32_t rf_backward(RfCtx* ctx, const RfObjective* objective, double* value, double* dJ_dlnk, double* dJ_dcontrols,
+                    int32_t n_controls);
+int32_t rf_well_count(const RfCtx* ctx);
+
 /* ---- Dense pressure solve that allocates nothing.  No counterpart in the reference, where the
  * dense inverse of a pressure block of at most 299 rows runs inside the preconditioner
  * (gmres_block_jacobi.rs:903-917); this exposes that solve alone for callers that may not call

@@ -114,3 +114,10 @@ class RfLinearReport(C.Structure):
         ("rhs_norm", C.c_double), ("final_residual_norm", C.c_double),
         ("used_fallback", C.c_int32), ("backend", C.c_int32),
     ]
+
+
+RF_OBJECTIVE_CUMULATIVE_OIL = 0
+
+
+class RfObjective(C.Structure):
+    _fields_ = [("kind", C.c_int32)]

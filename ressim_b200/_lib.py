@@ -47,6 +47,10 @@ def load():
     L.rf_batch_step.argtypes = [C.c_void_p, C.c_double, C.POINTER(_abi.RfStepReport)]
     L.rf_dense_solve_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
                                          C.c_size_t]
+    L.rf_set_controller_options.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double]
+    L.rf_adjoint_record.argtypes = [C.c_void_p, C.c_int32]
+    L.rf_backward.argtypes = [C.c_void_p, C.POINTER(_abi.RfObjective), _dp, _dp, _dp, C.c_int32]
+    L.rf_well_count.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -61,7 +65,8 @@ EXPORTED_SYMBOLS = (
     "rf_create", "rf_destroy", "rf_last_error", "rf_set_state", "rf_get_state", "rf_get_well_bhp",
     "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_kernel_launches",
     "rf_profile", "rf_set_linear_precision", "rf_set_cluster_size", "rf_batch_create", "rf_batch_destroy", "rf_batch_size",
-    "rf_batch_context", "rf_batch_step", "rf_dense_solve_noalloc",
+    "rf_batch_context", "rf_batch_step", "rf_dense_solve_noalloc", "rf_set_controller_options", "rf_adjoint_record",
+    "rf_backward", "rf_well_count",
 )
 
 PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",

@@ -282,7 +282,7 @@ static bool family_osc(double f0, double f1, double f2) {
 struct CnvMb {
   bool accept;
 };
-static bool cnv_mb_accept(const double* st, int n, bool final_it) {
+static bool cnv_mb_accept(const double* st, int n, bool final_it, double cnv_tol = 0.0, double mb_tol = 0.0) {
   // st: [0..2] family maxima, [3..5] FVF sums, [6..8] max |r|/pv, [9..11] residual sums,
   // [12] pore-volume sum, [13] violating pore volume
   const double nn = double(n > 0 ? n : 1);
@@ -292,8 +292,13 @@ static bool cnv_mb_accept(const double* st, int n, bool final_it) {
     cnv[k] = bavg[k] * st[6 + k];
     mb[k] = fabs(bavg[k] * st[9 + k]) / fmax(st[12], 1e-9);
   }
-  const bool pv_relax = st[13] < 0.03 * st[12];
-  const double mbt = final_it ? 1e-6 : 1e-7, cnvt = final_it ? 1.0 : 1e-2;
+  bool pv_relax = st[13] < 0.03 * st[12];
+  double mbt = final_it ? 1e-6 : 1e-7, cnvt = final_it ? 1.0 : 1e-2;
+  if (cnv_tol > 0.0) {  // controller option: fixed tolerances, no relaxed tiers
+    cnvt = cnv_tol;
+    mbt = mb_tol > 0.0 ? mb_tol : mbt;
+    pv_relax = false;
+  }
   bool ok = true;
   for (int k = 0; k < 3; ++k) ok = ok && (cnv[k] <= cnvt || (pv_relax && cnv[k] <= 1.0)) && mb[k] <= mbt;
   return ok;
@@ -371,7 +376,7 @@ static NewtonReport run_newton(Ctx& c, WellState& ws, double dt) {
     n2 = n1;
     n1 = fam;
     const bool final_it = it + 1 == max_it;
-    if (it >= 2 && cnv_mb_accept(st, c.n, final_it)) {
+    if (it >= 2 && cnv_mb_accept(st, c.n, final_it, c.ctl_cnv, c.ctl_mb)) {
       rep.converged = true;
       rep.newton_iterations = it + 1;
       return rep;
@@ -425,7 +430,7 @@ static NewtonReport run_newton(Ctx& c, WellState& ws, double dt) {
   launch_assembly(c, dt);
   launch_norms(c, dt, st);
   rep.newton_iterations = max_it;
-  rep.converged = cnv_mb_accept(st, c.n, true);
+  rep.converged = cnv_mb_accept(st, c.n, true, c.ctl_cnv, c.ctl_mb);
   return rep;
 }
 
@@ -728,6 +733,7 @@ static void refresh_head_offsets(Ctx& c) {
 static int step(Ctx& c, double target, RfStepReport* out) {
   RfStepReport rep{};
   RF_CUDA(cudaEventRecord(c.ev0, c.stream));
+  adjoint_on_step_begin(c);
   refresh_head_offsets(c);
   double stepped = 0.0;
   int substeps = 0, warning = 0;
@@ -743,7 +749,7 @@ static int step(Ctx& c, double target, RfStepReport* out) {
       proposed = c.time_days <= 1e-12 ? fmin(remaining, remaining <= 1.0 + 1e-12 ? 0.25 : 1.0) : remaining;
     else
       proposed = fmin(remaining, last_dt * growth);
-    double trial = fmin(proposed, remaining);
+    double trial = c.ctl_one_substep ? remaining : fmin(proposed, remaining);
     int retry = 0;
     // previous_state = FimState::from_simulator: the accepted state with the written-back
     // (two-phase: zero) gas primary
@@ -773,6 +779,7 @@ static int step(Ctx& c, double target, RfStepReport* out) {
         for (int p = 0; p < c.topo.n_perfs; ++p) c.wells[c.topo.perf_entry[p]].bhp = ws.bhp[c.topo.perf_well[p]];
         state_sums3(c, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_p.p, c.d_sw.p, sa);
         record_step3(c, ws, trial, sa[2] - sb[2], sb[3] - sa[3], sa[4] - sb[4], sa);
+        adjoint_on_substep_accepted(c, trial);
         c.time_days += trial;
         stepped += trial;
         last_dt = trial;
@@ -796,12 +803,18 @@ static int step(Ctx& c, double target, RfStepReport* out) {
         double sums_after[7];
         state_sums(c, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_p.p, c.d_sw.p, c.d_hc.p, sums_after);
         record_step(c, ws, trial, sums_after[2] - sums_prev[2], sums_prev[3] - sums_after[3], sums_after);
+        adjoint_on_substep_accepted(c, trial);
         c.time_days += trial;
         stepped += trial;
         last_dt = trial;
         substeps++;
         rep.substeps++;
         rep.last_dt_days = trial;
+        break;
+      }
+      if (c.ctl_one_substep) {  // controller option: no retries
+        warning = 2;
+        c.last_warning = "FIM Newton step did not converge in the one substep of the report step";
         break;
       }
       const double next = trial * 0.33;
@@ -1134,6 +1147,7 @@ static void setup_device(Ctx& c) {
 }
 
 static void free_ctx(Ctx& c) {
+  adjoint_free(c);
   for (auto* b : {&c.d_pv, &c.d_tx, &c.d_ty, &c.d_tz, &c.d_depth, &c.d_p, &c.d_sw, &c.d_hc, &c.d_pp, &c.d_psw, &c.d_phc,
                   &c.d_cp, &c.d_csw, &c.d_chc, &c.d_res, &c.d_val, &c.d_perf_wi, &c.d_perf_head, &c.d_bhp, &c.d_q,
                   &c.d_res_tail, &c.d_jrw, &c.d_jwr_perf, &c.d_jwr_ctrl, &c.d_jww_perf_bhp, &c.d_jww_ctrl_q,
@@ -1172,6 +1186,8 @@ static void free_ctx(Ctx& c) {
   c.h_pin = nullptr;
   if (c.stream) cudaStreamDestroy(c.stream);
 }
+
+#include "rf_adjoint.inc"
 
 }  // namespace rf
 
@@ -1322,6 +1338,31 @@ int32_t rf_step(RfCtx* ctx, double target_dt_days, RfStepReport* out) {
   if (!ctx || !(target_dt_days > 0.0) || !std::isfinite(target_dt_days)) return RF_ERR_INVALID;
   return guarded(ctx, [&]() -> int32_t { return rf::step(ctx->c, target_dt_days, out); });
 }
+
+int32_t rf_set_controller_options(RfCtx* ctx, int32_t one_substep_per_report_step, double cnv_tol, double mb_tol) {
+  if (!ctx || !(cnv_tol >= 0.0) || !(mb_tol >= 0.0)) return RF_ERR_INVALID;
+  ctx->c.ctl_one_substep = one_substep_per_report_step != 0;
+  ctx->c.ctl_cnv = cnv_tol;
+  ctx->c.ctl_mb = mb_tol;
+  return RF_OK;
+}
+
+int32_t rf_adjoint_record(RfCtx* ctx, int32_t enable) {
+  if (!ctx) return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t { return rf::adjoint_record(ctx->c, enable); });
+}
+
+int32_t rf_backward(RfCtx* ctx, const RfObjective* objective, double* value, double* dJ_dlnk, double* dJ_dcontrols,
+                    int32_t n_controls) {
+  if (!ctx || !objective) return RF_ERR_INVALID;
+  if (objective->kind != RF_OBJECTIVE_CUMULATIVE_OIL) {
+    ctx->c.err = "unknown objective kind";
+    return RF_ERR_INVALID;
+  }
+  return guarded(ctx, [&]() -> int32_t { return rf::backward(ctx->c, value, dJ_dlnk, dJ_dcontrols, n_controls); });
+}
+
+int32_t rf_well_count(const RfCtx* ctx) { return ctx ? ctx->c.topo.n_wells : 0; }
 
 int32_t rf_rate_history_len(const RfCtx* ctx) { return ctx ? int32_t(ctx->c.rate_history.size()) : 0; }
 

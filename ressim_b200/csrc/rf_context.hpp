@@ -135,6 +135,12 @@ struct Ctx {
     size_t off, bytes;
   };
   std::vector<PinCopy> pin_pending;
+  // controller options (rf_set_controller_options): one substep per report step, and CNV / MB
+  // tolerances replacing the reference's tiers when > 0
+  int ctl_one_substep = 0;
+  double ctl_cnv = 0.0, ctl_mb = 0.0;
+  // discrete adjoint tape (rf_adjoint.cu); null until recording starts
+  struct AdjointTape* tape = nullptr;
   int cluster_size = 0;  // CTAs in the one cluster that runs the level-scheduled kernels
   // slice ownership schedule of the distributed-shared-memory BiCGStab (built for cluster_size)
   int own_slice = 0;

@@ -1929,17 +1929,8 @@ LinResult linear_solve_reduced(Ctx& c) {
   return out;
 }
 
-LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
-  // small systems go to the direct LU first; CPR-FGMRES runs when it does not converge
-  // (fim/linear/mod.rs:279-300)
-  bool fell_back = false;
-  if (direct_rows(c, true) <= kDirectSolveRows) {
-    LinResult d = linear_solve_direct(c, true, &h_dx_tail);
-    if (d.converged) return d;
-    fell_back = true;
-  }
-  const int n = c.n;
-  const long long n3 = 3ll * n;
+void schur_eliminate(Ctx& c) {
+  const long long n3 = 3ll * c.n;
   // rhs_red = -res (cell rows); Schur corrects the perforated rows and adds the fill
   k_neg<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_res.p, c.d_rhs_red.p);
   c.launches++;
@@ -1974,6 +1965,57 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
     k_schur<<<W, kBlock, smem, c.stream>>>(s);
     c.launches++;
   }
+}
+
+LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol, int max_passes) {
+  // iterative refinement over the path's own inner solve (direct LU for small systems, else
+  // CPR-FGMRES at its 5e-3 relative tolerance): x += solve(b - A x) until |b - A x| <= rtol |b|
+  const long long n3 = 3ll * c.n;
+  LinResult out;
+  dot_dev(c, n3, b, nullptr, c.d_scal.p + 26, true);
+  double bn = 0.0;
+  d2h(c, &bn, c.d_scal.p + 26, sizeof(double));
+  d2h_wait(c);
+  out.rhs_norm = bn;
+  RF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n3, c.stream));
+  const bool direct = direct_rows(c, false) <= kDirectSolveRows;
+  for (int pass = 0; pass <= max_passes; ++pass) {
+    spmv_res(c, x, b, c.d_rhs_red.p);
+    dot_dev(c, n3, c.d_rhs_red.p, nullptr, c.d_scal.p + 27, true);
+    double rn = 0.0;
+    d2h(c, &rn, c.d_scal.p + 27, sizeof(double));
+    d2h_wait(c);
+    out.final_residual_norm = rn;
+    out.finite = std::isfinite(rn);
+    if (!out.finite) return out;
+    if (rn <= rtol * bn || bn == 0.0) {
+      out.converged = true;
+      return out;
+    }
+    if (pass == max_passes) break;
+    LinResult inner;
+    if (direct) inner = linear_solve_direct(c, false, nullptr);
+    if (!direct || !inner.converged) inner = linear_solve_reduced(c);
+    out.iterations += inner.iterations;
+    k_add_inplace<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_x.p, x);
+    c.launches++;
+  }
+  return out;
+}
+
+LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
+  // small systems go to the direct LU first; CPR-FGMRES runs when it does not converge
+  // (fim/linear/mod.rs:279-300)
+  bool fell_back = false;
+  if (direct_rows(c, true) <= kDirectSolveRows) {
+    LinResult d = linear_solve_direct(c, true, &h_dx_tail);
+    if (d.converged) return d;
+    fell_back = true;
+  }
+  const int n = c.n;
+  const long long n3 = 3ll * n;
+  schur_eliminate(c);
+  const int W = c.topo.n_wells;
   LinResult lin = linear_solve_reduced(c);
   h_dx_tail.assign(size_t(W) + c.topo.n_perfs, 0.0);
   // full-system residual: reduced residual for unperforated rows, direct rows elsewhere

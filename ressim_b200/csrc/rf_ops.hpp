@@ -1,6 +1,8 @@
 // rf_ops.hpp — host launchers of the device kernels (assembly, norms, linear solve).
 #pragma once
 
+#include <vector>
+
 #include "rf_context.hpp"
 
 namespace rf {
@@ -28,8 +30,25 @@ struct LinResult {
 // (rhs = -residual) and the assembled Jacobian; writes the reduced solution into d_x and the
 // tail solution into h_dx_tail (n_wells + n_perfs).
 LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail);
+// Well Schur elimination of the assembled system: d_val becomes the reduced matrix
+// S = A - B D^-1 C (fill added into the well cliques), d_tinv the per-well dense D^-1 and d_rhs_red
+// the reduced right-hand side of rhs = -residual.
+void schur_eliminate(Ctx& c);
 // CPR-FGMRES on an already assembled tail-free system: rhs in d_rhs_red, solution in d_x.
 LinResult linear_solve_reduced(Ctx& c);
+
+// Accurate solve of the tail-free system in d_val: x = A^-1 b to |b - A x| <= rtol |b| by
+// iterative refinement over the inner solve (at most max_passes inner solves).  b and x are
+// device vectors of 3N (not d_rhs_red / d_x, which the inner solves use).
+LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol, int max_passes);
+
+// Discrete adjoint kernels (rf_adjoint.cu)
+void adj_transpose(Ctx& c, const int* d_tpos);
+void adj_accum(Ctx& c, const double* lam_next, double* out);
+void adj_grad(Ctx& c, double dt, const double* kx, const double* ky, const double* kz, const double* dz,
+              const double* lam, double* grad);
+void adj_add_at(Ctx& c, const std::vector<int>& idx, const std::vector<double>& v, double* out, int* d_idx);
+void adj_gather_at(Ctx& c, const std::vector<int>& idx, const double* v, std::vector<double>& out, int* d_idx);
 
 // Direct route for systems of at most kDirectSolveRows rows (fim/linear/mod.rs:15, 262-300).
 // Rows of the system the route would factor: the full Newton system (with_wells) or the
@@ -41,6 +60,11 @@ int direct_rows(const Ctx& c, bool with_wells);
 // d_val / d_rhs_red.  The cell solution goes to d_x.  Not converged when a pivot is zero or the
 // residual stays above 1e-12 + 5e-3 |b|.
 LinResult linear_solve_direct(Ctx& c, bool with_wells, std::vector<double>* h_dx_tail);
+
+// Discrete adjoint tape hooks of the outer controller (rf_adjoint.cu); no-ops unless recording.
+void adjoint_on_step_begin(Ctx& c);
+void adjoint_on_substep_accepted(Ctx& c, double dt);
+void adjoint_free(Ctx& c);
 
 // Build-once helpers
 void build_levels(Ctx& c);

@@ -165,6 +165,38 @@ class ReservoirSimulator(Deck):
             raise DeviceError(f"rf_set_cluster_size failed ({rc}): {_lib.last_error(self._context())}")
         return rc
 
+    def set_controller_options(self, one_substep_per_report_step: bool = False, cnv_tol: float = 0.0,
+                               mb_tol: float = 0.0) -> None:
+        """Controller options of the device path (no counterpart in the reference): take every
+        report step as one substep without retries, and/or converge Newton to fixed CNV / MB
+        tolerances instead of the reference's tiers.  Defaults restore the reference controller."""
+        rc = _lib.load().rf_set_controller_options(self._context(), int(bool(one_substep_per_report_step)),
+                                                   float(cnv_tol), float(mb_tol))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_set_controller_options failed ({rc}): {_lib.last_error(self._context())}")
+
+    def adjoint_record(self, enable: bool = True) -> None:
+        """Start (clearing the tape) or stop recording report-step checkpoints for `backward`."""
+        rc = _lib.load().rf_adjoint_record(self._context(), int(bool(enable)))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_adjoint_record failed ({rc}): {_lib.last_error(self._context())}")
+
+    def backward(self):
+        """Discrete adjoint over the recorded report steps (no counterpart in the reference).
+        Returns (cumulative surface oil produced [Sm3], d/d ln(permeability multiplier) per cell,
+        d/d(active control) per physical well)."""
+        h = self._context()
+        L = _lib.load()
+        nw = int(L.rf_well_count(h))
+        g = np.zeros(self.n_cells)
+        gc = np.zeros(max(nw, 1))
+        val = C.c_double()
+        obj = _abi.RfObjective(_abi.RF_OBJECTIVE_CUMULATIVE_OIL)
+        rc = L.rf_backward(h, C.byref(obj), C.byref(val), _ptr(g), _ptr(gc), nw)
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_backward failed ({rc}): {_lib.last_error(h)}")
+        return val.value, g, gc[:nw]
+
     def kernel_launches(self) -> int:
         return int(_lib.load().rf_kernel_launches(self._context()))
 
