@@ -5,7 +5,7 @@ assembly, well Schur elimination, CPR-FGMRES and the update, including any subst
 on a seeded synthetic waterflood deck, run through the C ABI (`rf_step`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ensemble|72k|72k-bo|2m|1d] [--variants V] [--precision fp64|mixed]
+                    [--workload ensemble|72k|72k-bo|adjoint|2m|1d] [--variants V] [--precision fp64|mixed]
                     [--dt DAYS] [--no-cpu-baseline]
 
 The default workload is the sensitivity ensemble: 256 two-phase waterflood variants of uneven
@@ -66,6 +66,12 @@ WORKLOADS = {
                "Stone II, regime switching, gas flash), log-normal kh (ln-mean ln 100 mD, sigma 1, 5-cell correlation), "
                "kv/kh 0.1, phi from ln k, gravity on, p_init 250 bar, inverted five-spot (4 water rate injectors, "
                "1 BHP producer at 150 bar), dt 10 d report steps, FP64"),
+    "adjoint": (60, 60, 20, 2.0,
+                "discrete adjoint on black_oil_3d 60x60x20 (72,000 cells, the three-phase deck of --workload 72k-bo): "
+                "forward report steps recorded with per-report-step checkpoints, then the backward pass (substeps "
+                "replayed from the checkpoints, transposed well-Schur / CPR-FGMRES solves in reverse time); objective "
+                "cumulative surface oil, gradient in 72,000 per-cell ln k and 5 well controls; one substep per report "
+                "step, Newton to CNV 1e-9 / MB 1e-11, dt 2 d, FP64"),
     "2m": (200, 200, 50, 10.0,
            "waterflood_3d 200x200x50 (2,000,000 cells), same statistics and wells, dt 10 d report steps, FP64"),
     "1d": (200, 1, 1, 10.0, "waterflood_1d 200x1x1, rate injector cell 0, BHP producer cell 199, dt 10 d, FP64"),
@@ -101,7 +107,7 @@ def make_deck(workload):
         return decks.ensemble_variant(0), dt, desc
     if workload == "1d":
         deck, _, _ = decks.waterflood_1d()
-    elif workload == "72k-bo":
+    elif workload in ("72k-bo", "adjoint"):
         deck = decks.black_oil_3d(nx, ny, nz, seed=7)
     else:
         deck = decks.waterflood_3d(nx, ny, nz, seed=7)
@@ -497,6 +503,146 @@ def run_ensemble(args, rank, world):
     return 0
 
 
+ADJ_CNV, ADJ_MB = 1e-9, 1e-11
+
+
+def adjoint_objective(deck, dt, steps):
+    """Cumulative surface oil of a forward run (controller options as the adjoint leg's)."""
+    from ressim_b200 import ReservoirSimulator
+
+    sim = ReservoirSimulator.from_deck(deck)
+    sim.set_controller_options(True, ADJ_CNV, ADJ_MB)
+    for _ in range(steps):
+        r = sim.step(dt)
+        if r["warning"]:
+            raise RuntimeError(f"forward warning {r['warning']}")
+    t0, J = 0.0, 0.0
+    for h in sim.get_rate_history():
+        J += (h["time"] - t0) * h["total_production_oil"]
+        t0 = h["time"]
+    sim.close()
+    return J
+
+
+def run_adjoint(args, rank, world):
+    """`--workload adjoint`: a warm-up of W recorded report steps and a backward pass on a separate
+    simulator; then, from the initial state, K recorded forward report steps and the backward pass
+    over them, timed together with CUDA events (value) and by the host clock through the public
+    API with the state uploaded from host memory and the gradient read back (e2e).  One rank per GPU runs a replica (the backward pass does not shard).  A directional
+    derivative along a seeded random direction is checked against central differences (step 1e-4
+    in ln k) of two more forward runs."""
+    import copy
+
+    import numpy as np
+    import torch
+
+    from ressim_b200 import ReservoirSimulator
+
+    torch.cuda.set_device(0)
+    dev_index = (os.environ.get("CUDA_VISIBLE_DEVICES", "") or "0").split(",")[0].strip() or "0"
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", 0))
+        pg = dist
+    deck, dt_default, desc = make_deck("adjoint")
+    dt = args.dt if args.dt is not None else dt_default
+    n, K, W = deck.n_cells, args.steps, args.warmup
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # warm-up: W recorded report steps and a backward pass on a separate simulator (untimed)
+    warm = ReservoirSimulator.from_deck(deck)
+    warm.set_controller_options(True, ADJ_CNV, ADJ_MB)
+    warm.adjoint_record(True)
+    for _ in range(W):
+        warm.step(dt)
+    if W:
+        warm.backward()
+    warm.close()
+    sim = ReservoirSimulator.from_deck(deck)
+    sim.set_controller_options(True, ADJ_CNV, ADJ_MB)
+    st0 = sim.state()
+    t_state = sim.time_days
+    flush.zero_()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(dev_index)
+    clocks.start()
+    launches0 = sim.kernel_launches()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    t0 = time.perf_counter()
+    # the public API from host buffers: upload the state, record K steps, backward, read back
+    from ressim_b200 import _abi, _lib
+    import ctypes as C
+
+    L = _lib.load()
+    h = sim._context()
+    bufs = [np.ascontiguousarray(st0[k]) for k in ("pressure", "sat_water", "sat_gas", "rs")]
+    ptrs = [b.ctypes.data_as(C.POINTER(C.c_double)) for b in bufs]
+    ev[0].record()
+    if L.rf_set_state(h, *ptrs, C.c_double(t_state)) != 0:
+        raise RuntimeError(_lib.last_error(h))
+    sim.adjoint_record(True)
+    newton = 0
+    for _ in range(K):
+        r = sim.step(dt)
+        newton += r["newton_iterations"]
+        if r["warning"]:
+            raise RuntimeError(f"forward warning {r['warning']}")
+    sim.adjoint_record(False)
+    ev[1].record()
+    J, grad, gctl = sim.backward()
+    ev[2].record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = sim.kernel_launches() - launches0
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    dev_ms = max_over_ranks(fwd_ms + bwd_ms, pg, "cuda")
+    wall = max_over_ranks(wall, pg, "cuda")
+    value = world * n * K / (dev_ms / 1e3)
+    check = None
+    if rank == 0:
+        rng = np.random.default_rng(2024)
+        v = rng.standard_normal(n)
+        hstep = 1e-4
+
+        def shifted(sign):
+            d = copy.deepcopy(deck)
+            m = np.exp(sign * hstep * v)
+            d.perm_x, d.perm_y, d.perm_z = (np.asarray(a) * m for a in (d.perm_x, d.perm_y, d.perm_z))
+            return adjoint_objective(d, dt, K)
+
+        j_fwd = adjoint_objective(deck, dt, K)
+        fd = (shifted(1.0) - shifted(-1.0)) / (2 * hstep)
+        dd = float(grad @ v)
+        check = {"direction": "seeded standard normal over all cells", "step_ln_k": hstep, "adjoint": dd, "fd": fd,
+                 "rel_err": abs(dd - fd) / max(abs(fd), 1e-300), "objective": J,
+                 "objective_forward_run": j_fwd}
+    if rank == 0:
+        line = {
+            "metric": "FIM cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": dev_ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded deck generator)",
+            "config": {"workload": desc, "cells": n, "dt_days": dt, "parallelism": f"replicas{world}",
+                       "newton_iterations": newton, "parameters": n + len(gctl)},
+            "e2e": {"value": world * n * K / wall, "unit": "cell-steps/s", "h2d_bytes_per_step": 4 * 8 * n // K,
+                    "d2h_bytes_per_step": 8 * (n + len(gctl)) // K},
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / max(fwd_ms, 1e-9),
+            "gradient_check": check, "clocks": clk, "gpu_launches": int(launches), "roofline": None,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -504,6 +650,8 @@ def main():
     rank, world, local = dist_setup(args)
     if args.workload == "ensemble":
         return run_ensemble(args, rank, world)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world)
     cpu_job = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "2m":
         import multiprocessing as mp
