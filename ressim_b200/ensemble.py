@@ -32,7 +32,9 @@ class Ensemble:
         for i, d in enumerate(self.decks):
             p = np.ascontiguousarray(d.pressure, dtype=np.float64)
             sw = np.ascontiguousarray(d.sat_water, dtype=np.float64)
-            rc = L.rf_set_state(self._ctx[i], _ptr(p), _ptr(sw), None, None, 0.0)
+            sg = np.ascontiguousarray(d.sat_gas, dtype=np.float64)
+            rs = np.ascontiguousarray(d.rs, dtype=np.float64)
+            rc = L.rf_set_state(self._ctx[i], _ptr(p), _ptr(sw), _ptr(sg), _ptr(rs), 0.0)
             if rc != _abi.RF_OK:
                 raise DeviceError(f"rf_set_state failed for variant {i}: {_lib.last_error(self._ctx[i])}")
             rc = L.rf_set_linear_precision(self._ctx[i], codes[precision])
@@ -57,12 +59,12 @@ class Ensemble:
 
     def state(self, i: int) -> dict:
         n = self.decks[i].n_cells
-        p, sw, so = np.zeros(n), np.zeros(n), np.zeros(n)
+        p, sw, so, sg, rs = (np.zeros(n) for _ in range(5))
         t = C.c_double()
-        rc = _lib.load().rf_get_state(self._ctx[i], _ptr(p), _ptr(sw), _ptr(so), None, None, C.byref(t))
+        rc = _lib.load().rf_get_state(self._ctx[i], _ptr(p), _ptr(sw), _ptr(so), _ptr(sg), _ptr(rs), C.byref(t))
         if rc != _abi.RF_OK:
             raise DeviceError(f"rf_get_state failed for variant {i}: {_lib.last_error(self._ctx[i])}")
-        return {"pressure": p, "sat_water": sw, "sat_oil": so, "time": t.value}
+        return {"pressure": p, "sat_water": sw, "sat_oil": so, "sat_gas": sg, "rs": rs, "time": t.value}
 
     def kernel_launches(self) -> int:
         L = _lib.load()
