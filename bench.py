@@ -94,6 +94,10 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="linear-solver precision of the device path (mixed: FP32 ILU and pressure stage)")
     ap.add_argument("--variants", type=int, default=256, help="ensemble variants per GPU (--workload ensemble)")
+    ap.add_argument("--cluster-table", default=None,
+                    help="ensemble: JSON table of tuned cluster sizes (ressim_b200.autotune) applied per variant")
+    ap.add_argument("--tune-variants", type=int, default=0,
+                    help="ensemble: first tune this many variants spread over the size range into --cluster-table")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="wall budget of the CPU baseline sample")
     return ap.parse_args()
@@ -364,6 +368,8 @@ def run_ensemble(args, rank, world):
 
     import torch
 
+    import numpy as np
+
     from ressim_b200 import Ensemble, _abi, _lib, decks
 
     if not torch.cuda.is_available():
@@ -385,7 +391,25 @@ def run_ensemble(args, rank, world):
     nv = args.variants
     ds = [decks.ensemble_variant(rank * nv + i) for i in range(nv)]
     cells = sum(d.n_cells for d in ds)
+    tuned = None
+    if args.cluster_table and args.tune_variants > 0 and rank == 0:
+        from ressim_b200 import autotune
+
+        order = sorted(range(nv), key=lambda i: ds[i].n_cells)
+        pick = sorted({order[int(round(q * (nv - 1)))] for q in np.linspace(0.0, 1.0, args.tune_variants)})
+        autotune.tune([ds[i] for i in pick], dt, args.precision, path=args.cluster_table)
+    if pg:
+        pg.barrier()
     ens = Ensemble(ds, precision=args.precision)
+    if args.cluster_table and os.path.exists(args.cluster_table):
+        from ressim_b200 import autotune
+
+        table = autotune.load(args.cluster_table)
+        sizes = autotune.apply(ens, table, args.precision,
+                               autotune.plan(table, ds, args.precision, host_threads=32,
+                                             sms=torch.cuda.get_device_properties(0).multi_processor_count))
+        tuned = {"table": os.path.basename(args.cluster_table),
+                 "sizes": {str(k): sizes.count(k) for k in sorted(set(sizes))}}
     L = _lib.load()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -489,7 +513,8 @@ def run_ensemble(args, rank, world):
                        "dt_days": dt, "parallelism": f"variants sharded over {world} GPU(s)",
                        "l2": "flushed (256 MB write) between timed report steps; state alone exceeds L2",
                        "newton_iterations": newton,
-                       "e2e_steps": "the K report steps after the timed ones"},
+                       "e2e_steps": "the K report steps after the timed ones",
+                       "cluster_sizes": tuned or "automatic (smallest that fits the shared-memory form)"},
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * cells,
                     "d2h_bytes_per_step": 2 * 8 * cells},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
@@ -593,9 +618,11 @@ def run_adjoint(args, rank, world):
         if r["warning"]:
             raise RuntimeError(f"forward warning {r['warning']}")
     sim.adjoint_record(False)
+    fwd_prof = sim.profile(enable=True, reset=True)
     ev[1].record()
     J, grad, gctl = sim.backward()
     ev[2].record()
+    bwd_prof = sim.profile(enable=False, reset=True)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     clk = clocks.stop()
@@ -632,6 +659,7 @@ def run_adjoint(args, rank, world):
             "e2e": {"value": world * n * K / wall, "unit": "cell-steps/s", "h2d_bytes_per_step": 4 * 8 * n // K,
                     "d2h_bytes_per_step": 8 * (n + len(gctl)) // K},
             "forward_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / max(fwd_ms, 1e-9),
+            "backward_phase_ms": {k: round(v, 1) for k, v in bwd_prof.items()},
             "gradient_check": check, "clocks": clk, "gpu_launches": int(launches), "roofline": None,
             "cpu_baseline": None,
         }

@@ -1814,7 +1814,7 @@ static inline void givens(double a, double b, double& cs, double& sn) {
   }
 }
 
-LinResult linear_solve_reduced(Ctx& c) {
+LinResult linear_solve_reduced(Ctx& c, bool rebuild) {
   LinResult out;
   const long long n3 = 3ll * c.n;
   const int R = Ctx::kRestart;
@@ -1822,7 +1822,7 @@ LinResult linear_solve_reduced(Ctx& c) {
   double* Z = c.d_Z.p;
   double* b = c.d_rhs_red.p;
   double* hbuf = c.d_scal.p + 32;  // H column (R+2)
-  cpr_build(c);
+  if (rebuild) cpr_build(c);
   dot_dev(c, n3, b, nullptr, c.d_scal.p + 21, true);
   double rhs_norm = 0.0;
   d2h(c, &rhs_norm, c.d_scal.p + 21, sizeof(double));
@@ -1995,7 +1995,8 @@ LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol
     if (pass == max_passes) break;
     LinResult inner;
     if (direct) inner = linear_solve_direct(c, false, nullptr);
-    if (!direct || !inner.converged) inner = linear_solve_reduced(c);
+    // the matrix is the same in every pass: the CPR factors of the first pass are reused
+    if (!direct || !inner.converged) inner = linear_solve_reduced(c, pass == 0 || direct);
     out.iterations += inner.iterations;
     k_add_inplace<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_x.p, x);
     c.launches++;

@@ -35,7 +35,8 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail);
 // the reduced right-hand side of rhs = -residual.
 void schur_eliminate(Ctx& c);
 // CPR-FGMRES on an already assembled tail-free system: rhs in d_rhs_red, solution in d_x.
-LinResult linear_solve_reduced(Ctx& c);
+// rebuild = false reuses the CPR factors of the previous call on the same matrix.
+LinResult linear_solve_reduced(Ctx& c, bool rebuild = true);
 
 // Accurate solve of the tail-free system in d_val: x = A^-1 b to |b - A x| <= rtol |b| by
 // iterative refinement over the inner solve (at most max_passes inner solves).  b and x are
