@@ -1176,6 +1176,8 @@ static void free_ctx(Ctx& c) {
   c.dir_rows = 0;
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
+  if (c.levels.d_long_rows) cudaFree(c.levels.d_long_rows);
+  if (c.levels.d_long_ptr) cudaFree(c.levels.d_long_ptr);
   for (cudaEvent_t e : c.ev_pool) cudaEventDestroy(e);
   c.ev_pool.clear();
   if (c.d_bicg_iters) cudaFree(c.d_bicg_iters);

@@ -30,7 +30,12 @@ struct Levels {
   std::vector<int> h_rows;
   int* d_rows = nullptr;
   int* d_ptr = nullptr;
+  // rows with more than kLongRowBlocks blocks (perforated rows with the well fill), per level;
+  // the factorisation gives each of them a warp
+  int* d_long_rows = nullptr;
+  int* d_long_ptr = nullptr;
 };
+constexpr int kLongRowBlocks = 9;
 
 template <class T>
 struct DBuf {
@@ -138,6 +143,9 @@ struct Ctx {
   // controller options (rf_set_controller_options): one substep per report step, and CNV / MB
   // tolerances replacing the reference's tiers when > 0
   int ctl_one_substep = 0;
+  // 1 while the adjoint solves a transposed system in d_val: the CPR build and apply use the
+  // transpose of the forward coarse correction (rf_linear.cu, k_cpr_weights_t)
+  int cpr_transposed = 0;
   double ctl_cnv = 0.0, ctl_mb = 0.0;
   // discrete adjoint tape (rf_adjoint.cu); null until recording starts
   struct AdjointTape* tape = nullptr;

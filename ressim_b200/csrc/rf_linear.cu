@@ -448,6 +448,48 @@ __global__ void k_cpr_weights(int nb, const int* __restrict__ rp, const int* __r
   }
 }
 
+// Transposed-system CPR (the adjoint's solves on S^T): the transpose of the forward two-stage
+// operator's coarse correction, P A_p^-1 R -> R^T A_p^-T P^T, with the forward weights.  The
+// weights of S (row 0 of S_ii^-1) are column 0 of (S^T)_ii^-1; the coarse matrix is
+// A_p^T[i, j] = sum_l S^T[(i,0),(j,l)] w_j[l]; restriction takes the pressure component and
+// prolongation spreads the correction with the weights.  The block-ILU0 smoother factors S^T.
+__global__ void k_cpr_weights_t(int nb, const int* __restrict__ rp, const int* __restrict__ diag,
+                                const double* __restrict__ val, double* __restrict__ w,
+                                unsigned char* __restrict__ mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  double inv[9];
+  mat3_inverse_or_diag(val + size_t(diag[i]) * 9, inv);
+  double r0 = inv[0], r1 = inv[3], r2 = inv[6];
+  const double mx = fmax(fmax(fmax(0.0, fabs(r0)), fabs(r1)), fabs(r2));
+  if (mx > kEps) {
+    r0 /= mx;
+    r1 /= mx;
+    r2 /= mx;
+  }
+  w[3 * i] = r0;
+  w[3 * i + 1] = r1;
+  w[3 * i + 2] = r2;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const double* a = val + size_t(k) * 9;
+    bool present = (k == diag[i]);
+    for (int e = 0; e < 9; ++e) present = present || fabs(a[e]) > kEps;
+    mask[k] = present ? 1 : 0;
+  }
+}
+__global__ void k_pressure_matrix_t(int nb, const int* __restrict__ rp, const int* __restrict__ col,
+                                    const double* __restrict__ val, const double* __restrict__ w,
+                                    double* __restrict__ pval) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const double* a = val + size_t(k) * 9;
+    const int j = col[k];
+    const double s = a[0] * w[3 * j] + a[1] * w[3 * j + 1] + a[2] * w[3 * j + 2];
+    pval[k] = fabs(s) > 1e-14 ? s : 0.0;
+  }
+}
+
 // A_p[i, j] = ((0 + w0 A[(i,0),(j,0)]) + w1 A[(i,1),(j,0)]) + w2 A[(i,2),(j,0)]; |A_p| <= 1e-14 -> 0
 __global__ void k_pressure_matrix(int nb, const int* __restrict__ rp, const double* __restrict__ val,
                                   const double* __restrict__ w, double* __restrict__ pval) {
@@ -552,6 +594,118 @@ __device__ void block_ilu_row(int i, const int* rp, const int* col, const int* d
   mat3_inverse_or_diag(lu + size_t(dp) * 9, dinv + size_t(i) * 9);
 }
 
+// Both ILU0 rows of a long row (a perforated cell's row with its well's fill) by one warp.  Its
+// work grows with the square of its length, so one thread per row made these rows the longest
+// step of their levels.  Every element gets the same operations in the same order as in
+// block_ilu_row / pressure_ilu_row:
+//  - block: for each present lower block kp in turn (all lanes form L_ik from the row's current
+//    block, the same value in every lane), the lanes share the U-row of col[kp]; each U entry
+//    updates at most one block of row i, so one kp's updates are independent;
+//  - pressure, lower part: for each kp in turn the lanes look up the terms plu[lp] U(col[lp], c)
+//    of all earlier lp in parallel and lane 0 sums them in lp order (rows of at most 32 lower
+//    entries; longer ones are done by lane 0 alone); the diagonal likewise; upper entries: one
+//    lane per entry, each summing over lp in order.
+__device__ void ilu_rows_warp(int i, const int* rp, const int* col, const int* diag, const double* val,
+                              const unsigned char* mask, double* lu, double* dinv, const double* pval, double* plu,
+                              double* pdiag) {
+  const int lane = threadIdx.x & 31;
+  const int b0 = rp[i], dp = diag[i], b1 = rp[i + 1];
+  for (int k = b0 + lane; k < b1; k += 32)
+    for (int e = 0; e < 9; ++e) lu[size_t(k) * 9 + e] = mask[k] ? val[size_t(k) * 9 + e] : 0.0;
+  __syncwarp();
+  for (int kp = b0; kp < dp; ++kp) {
+    if (!mask[kp]) continue;
+    const int kr = col[kp];
+    double lik[9];
+    mat3_mul(lu + size_t(kp) * 9, dinv + size_t(kr) * 9, lik);
+    __syncwarp();
+    for (int up = diag[kr] + 1 + lane; up < rp[kr + 1]; up += 32) {
+      if (!mask[up]) continue;
+      const int j = col[up];
+      int lo = kp + 1, hi = b1 - 1, t = -1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int cm = col[mid];
+        if (cm == j) {
+          t = mid;
+          break;
+        }
+        if (cm < j)
+          lo = mid + 1;
+        else
+          hi = mid - 1;
+      }
+      if (t < 0 || !mask[t]) continue;
+      double prod[9];
+      mat3_mul(lik, lu + size_t(up) * 9, prod);
+      double* tb = lu + size_t(t) * 9;
+      for (int e = 0; e < 9; ++e) tb[e] -= prod[e];
+    }
+    __syncwarp();
+    if (lane == 0)
+      for (int e = 0; e < 9; ++e) lu[size_t(kp) * 9 + e] = lik[e];
+    __syncwarp();
+  }
+  if (lane == 0) mat3_inverse_or_diag(lu + size_t(dp) * 9, dinv + size_t(i) * 9);
+  // pressure ILU0
+  if (dp - b0 > 32) {
+    if (lane == 0) pressure_ilu_row(i, rp, col, diag, pval, plu, pdiag);
+    __syncwarp();
+    return;
+  }
+  for (int kp = b0; kp < dp; ++kp) {
+    if (pval[kp] == 0.0) {
+      if (lane == 0) plu[kp] = 0.0;
+      __syncwarp();
+      continue;
+    }
+    const int c = col[kp];
+    const int lp = b0 + lane;
+    double term = 0.0;
+    if (lp < kp && pval[lp] != 0.0) term = plu[lp] * upper_entry(rp, col, diag, plu, col[lp], c);
+    double sum = pval[kp];
+    for (int q = b0; q < kp; ++q) {
+      const double tq = __shfl_sync(0xffffffffu, term, q - b0);
+      if (pval[q] != 0.0) sum -= tq;
+    }
+    if (lane == 0) {
+      const double d = pdiag[c];
+      plu[kp] = fabs(d) > kEps ? sum / d : 0.0;
+    }
+    __syncwarp();
+  }
+  {
+    const double de = pval[dp];
+    const int lp = b0 + lane;
+    double term = 0.0;
+    if (lp < dp && pval[lp] != 0.0) term = plu[lp] * upper_entry(rp, col, diag, plu, col[lp], i);
+    double ud = de;
+    for (int q = b0; q < dp; ++q) {
+      const double tq = __shfl_sync(0xffffffffu, term, q - b0);
+      if (pval[q] != 0.0) ud -= tq;
+    }
+    if (lane == 0) {
+      if (fabs(ud) <= kEps) ud = fabs(de) > kEps ? de : 1.0;
+      pdiag[i] = ud;
+      plu[dp] = 0.0;
+    }
+  }
+  for (int up = dp + 1 + lane; up < b1; up += 32) {
+    if (pval[up] == 0.0) {
+      plu[up] = 0.0;
+      continue;
+    }
+    const int c = col[up];
+    double s = pval[up];
+    for (int lp = b0; lp < dp; ++lp) {
+      if (pval[lp] == 0.0) continue;
+      s -= plu[lp] * upper_entry(rp, col, diag, plu, col[lp], c);
+    }
+    plu[up] = s;
+  }
+  __syncwarp();
+}
+
 // Level-scheduled triangular work: rows of level l depend only on rows of lower levels, so each
 // level is one parallel pass followed by a barrier.  The row arithmetic is the reference's, in the
 // reference's order, so factors and solves equal the natural-order sequential ones.
@@ -574,6 +728,8 @@ struct LevelSched {
   const int* rp;
   const int* col;
   const int* diag;
+  const int* long_rows;  // rows of more than kLongRowBlocks blocks, per level (factorisation only)
+  const int* long_ptr;
 };
 
 __device__ __forceinline__ void cluster_barrier() {
@@ -605,12 +761,17 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(LevelSched L, con
   __shared__ int s_ptr[kSmemLevels];
   const int* lp = stage_levels(L, s_ptr);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int warp = tid >> 5, nwarps = nth >> 5;
   for (int l = 0; l < L.n_levels; ++l) {
     for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) {
       const int r = L.lvl_rows[q];
+      if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
       block_ilu_row(r, L.rp, L.col, L.diag, val, mask, lu, dinv);
       pressure_ilu_row(r, L.rp, L.col, L.diag, pval, plu, pdiag);
     }
+    __syncwarp();
+    for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps)
+      ilu_rows_warp(L.long_rows[q], L.rp, L.col, L.diag, val, mask, lu, dinv, pval, plu, pdiag);
     cluster_barrier();
   }
 }
@@ -1448,6 +1609,19 @@ __global__ void k_prolong(int nb, const double* __restrict__ corr, double* __res
   out[3 * i + 1] = 0.0;
   out[3 * i + 2] = 0.0;
 }
+__global__ void k_restrict_t(int nb, const double* __restrict__ v, double* __restrict__ pr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nb) pr[i] = v[3 * i];
+}
+__global__ void k_prolong_t(int nb, const double* __restrict__ w, const double* __restrict__ corr,
+                            double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const double c = corr[i];
+  out[3 * i] = w[3 * i] * c;
+  out[3 * i + 1] = w[3 * i + 1] * c;
+  out[3 * i + 2] = w[3 * i + 2] * c;
+}
 __global__ void k_dense_matvec(int n, const double* __restrict__ a, const double* __restrict__ x, double* __restrict__ y) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
@@ -1593,6 +1767,8 @@ static LevelSched level_sched(Ctx& c) {
   L.n_levels = c.levels.n_levels;
   L.lvl_rows = c.levels.d_rows;
   L.lvl_ptr = c.levels.d_ptr;
+  L.long_rows = c.levels.d_long_rows;
+  L.long_ptr = c.levels.d_long_ptr;
   L.rp = c.d_row_ptr.p;
   L.col = c.d_col.p;
   L.diag = c.d_diag.p;
@@ -1621,9 +1797,16 @@ static void cluster_launch(Ctx& c, const void* fn, int block, void** args) {
 static void cpr_build(Ctx& c) {
   PhaseScope ps(c, kPhCprBuild);
   const int n = c.n;
-  k_cpr_weights<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_diag.p, c.d_val.p, c.d_cpr_w.p,
-                                                         c.d_bmask.p);
-  k_pressure_matrix<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_val.p, c.d_cpr_w.p, c.d_pval.p);
+  if (c.cpr_transposed) {
+    k_cpr_weights_t<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_diag.p, c.d_val.p, c.d_cpr_w.p,
+                                                             c.d_bmask.p);
+    k_pressure_matrix_t<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_col.p, c.d_val.p, c.d_cpr_w.p,
+                                                                 c.d_pval.p);
+  } else {
+    k_cpr_weights<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_diag.p, c.d_val.p, c.d_cpr_w.p,
+                                                           c.d_bmask.p);
+    k_pressure_matrix<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_val.p, c.d_cpr_w.p, c.d_pval.p);
+  }
   c.launches += 2;
   LevelSched L = level_sched(c);
   const double* val = c.d_val.p;
@@ -1763,7 +1946,10 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
   double* corr = c.d_pvec.p + size_t(11) * n;
   {
   PhaseScope ps(c, kPhCoarse);
-  k_restrict<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_cpr_w.p, v, prhs);
+  if (c.cpr_transposed)
+    k_restrict_t<<<blocks_for(n), kBlock, 0, c.stream>>>(n, v, prhs);
+  else
+    k_restrict<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_cpr_w.p, v, prhs);
   c.launches++;
   if (c.dense_ok) {
     k_dense_matvec<<<blocks_for(n, 64), 64, 0, c.stream>>>(n, c.d_dense.p, prhs, corr);
@@ -1775,7 +1961,10 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
     else
       launch_bicgstab<double>(c, c.d_pval.p, c.d_plu.p, c.d_pdiag.p, prhs, corr, c.d_pvec.p);
   }
-  k_prolong<<<blocks_for(n), kBlock, 0, c.stream>>>(n, corr, z);
+  if (c.cpr_transposed)
+    k_prolong_t<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_cpr_w.p, corr, z);
+  else
+    k_prolong<<<blocks_for(n), kBlock, 0, c.stream>>>(n, corr, z);
   c.launches++;
   }
   PhaseScope ps(c, kPhSmoother);
@@ -2113,6 +2302,19 @@ void build_levels(Ctx& c) {
   RF_CUDA(cudaMemcpy(c.levels.d_rows, rows.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   RF_CUDA(cudaMemcpy(c.levels.d_ptr, c.levels.h_ptr.data(), sizeof(int) * (c.levels.n_levels + 1),
                      cudaMemcpyHostToDevice));
+  std::vector<int> lptr(c.levels.n_levels + 1, 0), lrows;
+  for (int l = 0; l < c.levels.n_levels; ++l) {
+    for (int q = c.levels.h_ptr[l]; q < c.levels.h_ptr[l + 1]; ++q) {
+      const int r = rows[q];
+      if (c.h_row_ptr[r + 1] - c.h_row_ptr[r] > kLongRowBlocks) lrows.push_back(r);
+    }
+    lptr[l + 1] = int(lrows.size());
+  }
+  lrows.push_back(0);
+  RF_CUDA(cudaMalloc(&c.levels.d_long_rows, sizeof(int) * lrows.size()));
+  RF_CUDA(cudaMalloc(&c.levels.d_long_ptr, sizeof(int) * lptr.size()));
+  RF_CUDA(cudaMemcpy(c.levels.d_long_rows, lrows.data(), sizeof(int) * lrows.size(), cudaMemcpyHostToDevice));
+  RF_CUDA(cudaMemcpy(c.levels.d_long_ptr, lptr.data(), sizeof(int) * lptr.size(), cudaMemcpyHostToDevice));
 }
 
 // Automatic cluster size: the smallest power of two (<= 16) whose slices fit the FP64
