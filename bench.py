@@ -333,6 +333,10 @@ def run_reference(args):
         return 0
     if args.workload == "ensemble":
         return run_reference_ensemble(args)
+    if args.workload == "adjoint":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint (no backward pass to time)"}),
+              flush=True)
+        return 0
     _, dt_default, desc = make_deck(args.workload)
     dt = args.dt if args.dt is not None else dt_default
     v, k, el, newton, _ = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
