@@ -108,7 +108,7 @@ static void add_well_residual_terms(const Sim& s, const State& st, double dt, st
   for (int perf = 0; perf < int(s.topo.perfs.size()); ++perf) {
     const Perf& pf = s.topo.perfs[perf];
     const Cell& c = st.cells[pf.cell];
-    WellCell<double> wc{c.p, c.sw, c.hc, c.regime};
+    WellCell<double> wc{c.p, c.sw, c.hc, c.regime, c.base_rs};
     const double bhp = st.bhp[pf.well];
     const double q = st.q[perf];
     PerfInput<double> pi{wc, !pf.injector, {}, q};
@@ -144,14 +144,14 @@ static void add_well_jacobian_terms(const Sim& s, const State& st, double dt, st
   for (int perf = 0; perf < int(s.topo.perfs.size()); ++perf) {
     const Perf& pf = s.topo.perfs[perf];
     const Cell& c = st.cells[pf.cell];
-    WellCell<double> wc{c.p, c.sw, c.hc, c.regime};
+    WellCell<double> wc{c.p, c.sw, c.hc, c.regime, c.base_rs};
     const double bhp = st.bhp[pf.well];
     const double q = st.q[perf];
     PerfInput<double> pi{wc, !pf.injector, {}, q};
     if (!pf.injector) pi.frac = producer_fractions_g<double>(s, wc);
     inputs[pf.well].push_back(pi);
     const int prow = st.q_off(perf), qcol = st.q_off(perf), bcol = st.bhp_off(pf.well);
-    WellCell<Ad<4>> ca{ad_var<4>(c.p, 0), ad_var<4>(c.sw, 1), ad_var<4>(c.hc, 2), c.regime};
+    WellCell<Ad<4>> ca{ad_var<4>(c.p, 0), ad_var<4>(c.sw, 1), ad_var<4>(c.hc, 2), c.regime, c.base_rs};
     if (pf.has_wi) {
       Ad<4> conn = connection_rate_g<Ad<4>>(s, pf.wi, s.head_offset[pf.entry], pf.injector, ca,
                                             ad_var<4>(bhp, 3));
@@ -195,7 +195,7 @@ static void add_well_jacobian_terms(const Sim& s, const State& st, double dt, st
     for (int perf : s.topo.wells[w].perfs) {
       const Perf& pf = s.topo.perfs[perf];
       const Cell& cc = st.cells[pf.cell];
-      WellCell<Ad<4>> ca{ad_var<4>(cc.p, 0), ad_var<4>(cc.sw, 1), ad_var<4>(cc.hc, 2), cc.regime};
+      WellCell<Ad<4>> ca{ad_var<4>(cc.p, 0), ad_var<4>(cc.sw, 1), ad_var<4>(cc.hc, 2), cc.regime, cc.base_rs};
       Ad<4> qa = ad_var<4>(st.q[perf], 3);
       Ad<4> rate;
       if (c.uses_surface_target) {
@@ -222,14 +222,16 @@ static Assembly assemble(const Sim& s, const State& prev, const State& st, doubl
     const Cell& x = st.cells[c];
     const Cell& px = prev.cells[c];
     double acc[3];
-    cell_accumulation_g<double>(s, c, x.regime, x.p, x.sw, x.hc, px.p, px.sw, px.hc, px.regime, acc);
+    cell_accumulation_g<double>(s, c, x.regime, x.p, x.sw, x.hc, px.p, px.sw, px.hc, px.regime, acc, x.base_rs);
     for (int e = 0; e < 3; ++e) r[3 * c + e] += acc[e];
   }
   auto face_res = [&](int i, int j, char dim, int ki, int kj) {
     const double gt = DARCY_METRIC_FACTOR * geometric_transmissibility(s, i, j, dim);
     if (gt <= 0.0) return;
-    FaceIn<double> fi{st.cells[i].p, st.cells[i].sw, st.cells[i].hc, s.depth_at_k(ki), st.cells[i].regime};
-    FaceIn<double> fj{st.cells[j].p, st.cells[j].sw, st.cells[j].hc, s.depth_at_k(kj), st.cells[j].regime};
+    FaceIn<double> fi{st.cells[i].p, st.cells[i].sw, st.cells[i].hc, s.depth_at_k(ki), st.cells[i].regime,
+                      st.cells[i].base_rs};
+    FaceIn<double> fj{st.cells[j].p, st.cells[j].sw, st.cells[j].hc, s.depth_at_k(kj), st.cells[j].regime,
+                      st.cells[j].base_rs};
     double f[3];
     face_flux_g<double>(s, gt, fi, fj, f);
     for (int e = 0; e < 3; ++e) {
@@ -255,7 +257,7 @@ static Assembly assemble(const Sim& s, const State& prev, const State& st, doubl
     const Cell& px = prev.cells[c];
     Ad<3> acc[3];
     cell_accumulation_g<Ad<3>>(s, c, x.regime, ad_var<3>(x.p, 0), ad_var<3>(x.sw, 1), ad_var<3>(x.hc, 2), px.p,
-                               px.sw, px.hc, px.regime, acc);
+                               px.sw, px.hc, px.regime, acc, x.base_rs);
     double b[3][3];
     for (int e = 0; e < 3; ++e)
       for (int v = 0; v < 3; ++v) b[e][v] = acc[e].d[v];
@@ -265,9 +267,9 @@ static Assembly assemble(const Sim& s, const State& prev, const State& st, doubl
     const double gt = DARCY_METRIC_FACTOR * geometric_transmissibility(s, i, j, dim);
     if (gt <= 0.0) return;
     FaceIn<Ad<6>> fi{ad_var<6>(st.cells[i].p, 0), ad_var<6>(st.cells[i].sw, 1), ad_var<6>(st.cells[i].hc, 2),
-                     s.depth_at_k(ki), st.cells[i].regime};
+                     s.depth_at_k(ki), st.cells[i].regime, st.cells[i].base_rs};
     FaceIn<Ad<6>> fj{ad_var<6>(st.cells[j].p, 3), ad_var<6>(st.cells[j].sw, 4), ad_var<6>(st.cells[j].hc, 5),
-                     s.depth_at_k(kj), st.cells[j].regime};
+                     s.depth_at_k(kj), st.cells[j].regime, st.cells[j].base_rs};
     Ad<6> f[3];
     face_flux_g<Ad<6>>(s, gt, fi, fj, f);
     double bii[3][3], bij[3][3], bji[3][3], bjj[3][3];

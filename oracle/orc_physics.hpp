@@ -41,6 +41,9 @@ struct Control {
 struct Cell {
   double p, sw, hc;
   int regime;  // 0 saturated, 1 undersaturated
+  // gas redissolution off (DRSDT0): the simulator's Rs of the cell at the substep start, which
+  // caps Rs in the flash, the regime test and the properties; NaN when redissolution is on
+  double base_rs = NAN;
 };
 struct State {
   std::vector<Cell> cells;
@@ -312,21 +315,43 @@ inline double solve_rs_plain(const Sim& s, double p, double sw, double sg, doubl
   return 0.5 * (lo + hi);
 }
 
-// split_gas_inventory_after_transport (step.rs:106-200), gas redissolution enabled
+// split_gas_inventory_after_transport (step.rs:106-200); base_rs: the DRSDT0 cap (NaN: none)
 inline void split_gas_plain(const Sim& s, double p, double pv, double sw, double free_sc, double dissolved_sc,
-                            double& sg, double& so, double& rs) {
+                            double base_rs, double& sg, double& so, double& rs) {
   const double total_hc = rmax(1.0 - sw, 0.0);
   const double bg = rmax(get_b_g(s, p), 1e-9);
   const double free_t = rmax(free_sc, 0.0);
   const double sg_t = rclamp((free_t * bg) / rmax(pv, 1e-9), 0.0, total_hc);
+  const double so_t = rmax(total_hc - sg_t, 0.0);
   const double dissolved = rmax(dissolved_sc, 0.0);
   const double rs_max = rmax(pvt_interpolate(s.pvt, p).rs, 0.0);
+  const bool redis = s.gas_redissolution;
+  const double cap = redis ? rs_max : (std::isnan(base_rs) ? rs_max : rmin(rmax(base_rs, 0.0), rs_max));
+  double bo_cap, mu;
+  pvt_interpolate_oil(s.pvt, p, cap, bo_cap, mu);
+  bo_cap = rmax(bo_cap, 1e-9);
+  if (!redis) {
+    const double max_t = (so_t * pv / bo_cap) * cap;
+    if (dissolved <= max_t + 1e-9) {
+      rs = solve_rs_plain(s, p, sw, sg_t, pv, dissolved, cap);
+      sg = sg_t;
+      so = so_t;
+      return;
+    }
+  }
   const double total_gas = free_t + dissolved;
-  double bo_sat_raw, mu;
-  pvt_interpolate_oil(s.pvt, p, rs_max, bo_sat_raw, mu);
-  const double bo_sat = rmax(bo_sat_raw, 1e-9), rs_sat = rs_max;
+  double rs_sat, bo_sat;
+  if (redis) {
+    double bo_sat_raw;
+    pvt_interpolate_oil(s.pvt, p, rs_max, bo_sat_raw, mu);
+    rs_sat = rs_max;
+    bo_sat = rmax(bo_sat_raw, 1e-9);
+  } else {
+    rs_sat = cap;
+    bo_sat = bo_cap;
+  }
   const double max_all = (total_hc * pv / bo_sat) * rs_sat;
-  if (total_gas <= max_all + 1e-9) {
+  if (redis && total_gas <= max_all + 1e-9) {
     rs = solve_rs_plain(s, p, sw, 0.0, pv, total_gas, rs_sat);
     sg = 0.0;
     so = total_hc;
@@ -334,7 +359,7 @@ inline void split_gas_plain(const Sim& s, double p, double pv, double sw, double
   }
   const double denom = (1.0 / bg) - (rs_sat / bo_sat);
   const double sg_sat = std::fabs(denom) > 1e-12 ? ((total_gas / pv) - (total_hc * rs_sat / bo_sat)) / denom : sg_t;
-  sg = rclamp(sg_sat, 0.0, total_hc);
+  sg = rclamp(sg_sat, redis ? 0.0 : sg_t, total_hc);
   so = rmax(total_hc - sg, 0.0);
   rs = rs_sat;
 }
@@ -361,24 +386,45 @@ inline S solve_rs_g(const Sim& s, const S& p, const S& sw, const S& sg, const S&
   S g = dissolved_gas_g<S>(s, p, sc<S>(rs_star), so, pv) - target;
   return sc<S>(rs_star) - g / dgdrs;
 }
-// split_gas_inventory_after_transport_generic (flash_ad.rs:104-207), redissolution enabled
+// split_gas_inventory_after_transport_generic (flash_ad.rs:104-207); base_rs: the DRSDT0 cap
 template <class S>
 inline void split_gas_g(const Sim& s, const S& p, const S& pv, const S& sw, const S& free_sc, const S& dissolved_sc,
-                        S& sg, S& so, S& rs) {
+                        double base_rs, S& sg, S& so, S& rs) {
   const PvtTable& t = s.pvt;
   S total_hc = max_floor(sc<S>(1.0) - sw, 0.0);
   S bg = max_floor(pvt_saturated_g(t, p).bg, 1e-9);
   S free_t = max_floor(free_sc, 0.0);
   S sg_t = min_of(max_floor((free_t * bg) / max_floor(pv, 1e-9), 0.0), total_hc);
+  S so_t = max_floor(total_hc - sg_t, 0.0);
   S dissolved = max_floor(dissolved_sc, 0.0);
   S rs_max = max_floor(pvt_saturated_g(t, p).rs, 0.0);
+  const bool redis = s.gas_redissolution;
+  S cap = (redis || std::isnan(base_rs)) ? rs_max : min_of(sc<S>(rmax(base_rs, 0.0)), rs_max);
+  S bo_cap, mu;
+  pvt_oil_g(t, p, cap, bo_cap, mu);
+  bo_cap = max_floor(bo_cap, 1e-9);
+  if (!redis) {
+    S max_t = (so_t * pv / bo_cap) * cap;
+    if (val(dissolved) <= val(max_t) + 1e-9) {
+      rs = solve_rs_g(s, p, sw, sg_t, pv, dissolved, val(cap));
+      sg = sg_t;
+      so = so_t;
+      return;
+    }
+  }
   S total_gas = free_t + dissolved;
-  S bo_sat_raw, mu;
-  pvt_oil_g(t, p, rs_max, bo_sat_raw, mu);
-  S bo_sat = max_floor(bo_sat_raw, 1e-9);
-  S rs_sat = rs_max;
+  S rs_sat, bo_sat;
+  if (redis) {
+    S bo_sat_raw;
+    pvt_oil_g(t, p, rs_max, bo_sat_raw, mu);
+    rs_sat = rs_max;
+    bo_sat = max_floor(bo_sat_raw, 1e-9);
+  } else {
+    rs_sat = cap;
+    bo_sat = bo_cap;
+  }
   S max_all = (total_hc * pv / bo_sat) * rs_sat;
-  if (val(total_gas) <= val(max_all) + 1e-9) {
+  if (redis && val(total_gas) <= val(max_all) + 1e-9) {
     rs = solve_rs_g(s, p, sw, sc<S>(0.0), pv, total_gas, val(rs_sat));
     sg = sc<S>(0.0);
     so = total_hc;
@@ -386,16 +432,17 @@ inline void split_gas_g(const Sim& s, const S& p, const S& pv, const S& sw, cons
   }
   S denom = s_recip(bg) - (rs_sat / bo_sat);
   S sg_sat = std::fabs(val(denom)) > 1e-12 ? ((total_gas / pv) - (total_hc * rs_sat / bo_sat)) / denom : sg_t;
-  sg = min_of(max_of(sg_sat, sc<S>(0.0)), total_hc);
+  sg = min_of(max_of(sg_sat, redis ? sc<S>(0.0) : sg_t), total_hc);
   so = max_floor(total_hc - sg, 0.0);
   rs = rs_sat;
 }
 
-// classify_cell_regime (flash.rs:13-40): 0 saturated, 1 undersaturated
-inline int classify_cell_regime(const Sim& s, double p, double sg, double rs) {
+// classify_cell_regime (flash.rs:13-40): 0 saturated, 1 undersaturated; base_rs: DRSDT0 cap
+inline int classify_cell_regime(const Sim& s, double p, double sg, double rs, double base_rs = NAN) {
   if (!s.three_phase || !s.has_pvt) return 0;
   if (sg > 1e-9) return 0;
-  const double rs_sat = pvt_interpolate(s.pvt, p).rs;
+  double rs_sat = pvt_interpolate(s.pvt, p).rs;
+  if (!std::isnan(base_rs)) rs_sat = rmin(rs_sat, base_rs);
   return rs < rs_sat - 1e-6 ? 1 : 0;
 }
 
@@ -405,7 +452,7 @@ struct Props {
   S so, sg, rs, bo, bg;
 };
 template <class S>
-inline Props<S> cell_props_g(const Sim& s, int regime, const S& p, const S& sw, const S& hc) {
+inline Props<S> cell_props_g(const Sim& s, int regime, const S& p, const S& sw, const S& hc, double base_rs = NAN) {
   const S one = sc<S>(1.0);
   const S raw_total = one - sw;
   Props<S> pr;
@@ -423,12 +470,14 @@ inline Props<S> cell_props_g(const Sim& s, int regime, const S& p, const S& sw, 
   if (regime == 0) {
     pr.sg = hc;
     pr.rs = pvt_saturated_g(t, p).rs;
+    if (!std::isnan(base_rs)) pr.rs = min_ceil(pr.rs, base_rs);
     pr.so = raw_total - pr.sg;
     pvt_oil_g(t, p, pr.rs, pr.bo, mu);
     pr.bg = pvt_saturated_g(t, p).bg;
     return pr;
   }
   S rs_cap = max_floor(pvt_saturated_g(t, p).rs, 0.0);
+  if (!std::isnan(base_rs)) rs_cap = min_of(rs_cap, sc<S>(rmax(base_rs, 0.0)));
   const S& rs_trial = hc;
   if (val(rs_trial) <= val(rs_cap) + 1e-6) {
     pr.sg = sc<S>(0.0);
@@ -439,7 +488,7 @@ inline Props<S> cell_props_g(const Sim& s, int regime, const S& p, const S& sw, 
     pvt_oil_g(t, p, rs_trial, bo_t, mu);
     bo_t = max_floor(bo_t, 1e-9);
     S dissolved = raw_total * rs_trial / bo_t;
-    split_gas_g(s, p, sc<S>(1.0), sw, sc<S>(0.0), dissolved, pr.sg, pr.so, pr.rs);
+    split_gas_g(s, p, sc<S>(1.0), sw, sc<S>(0.0), dissolved, base_rs, pr.sg, pr.so, pr.rs);
   }
   pvt_oil_g(t, p, pr.rs, pr.bo, mu);
   pr.bg = pvt_saturated_g(t, p).bg;
@@ -462,12 +511,12 @@ inline void component_inventory_g(const Sim& s, const S& pv, const S& p, const S
 // properties.rs:171-212: the previous inventory is evaluated with the previous regime
 template <class S>
 inline void cell_accumulation_g(const Sim& s, int cell, int regime, const S& p, const S& sw, const S& hc,
-                                double pp, double psw, double phc, int pregime, S out[3]) {
-  Props<S> pr = cell_props_g(s, regime, p, sw, hc);
+                                double pp, double psw, double phc, int pregime, S out[3], double base_rs = NAN) {
+  Props<S> pr = cell_props_g(s, regime, p, sw, hc, base_rs);
   S pv = pore_volume_g(s, cell, p);
   S cur[3];
   component_inventory_g(s, pv, p, sw, pr, cur);
-  Props<double> ppr = cell_props_g<double>(s, pregime, pp, psw, phc);
+  Props<double> ppr = cell_props_g<double>(s, pregime, pp, psw, phc, base_rs);
   double ppv = pore_volume_g<double>(s, cell, pp);
   double prev[3];
   component_inventory_g<double>(s, ppv, pp, psw, ppr, prev);
@@ -480,6 +529,7 @@ struct FaceIn {
   S p, sw, hc;
   double depth;
   int regime;
+  double base_rs = NAN;  // DRSDT0 cap
 };
 template <class S>
 inline S gravity_head_g(const Sim& s, double di, double dj, const S& ri, const S& rj) {
@@ -496,8 +546,8 @@ inline S gas_oil_pc_g(const Sim& s, const S& sg) {
 template <class S>
 inline void face_flux_g(const Sim& s, double geom_t, const FaceIn<S>& i, const FaceIn<S>& j,
                         S flux[3]) {
-  Props<S> pi = cell_props_g(s, i.regime, i.p, i.sw, i.hc);
-  Props<S> pj = cell_props_g(s, j.regime, j.p, j.sw, j.hc);
+  Props<S> pi = cell_props_g(s, i.regime, i.p, i.sw, i.hc, i.base_rs);
+  Props<S> pj = cell_props_g(s, j.regime, j.p, j.sw, j.hc, j.base_rs);
   S rwi = water_density_g(s, i.p), rwj = water_density_g(s, j.p);
   S roi = oil_density_g(s, i.p, pi.rs), roj = oil_density_g(s, j.p, pj.rs);
   S rgi = gas_density_g(s, i.p), rgj = gas_density_g(s, j.p);
@@ -647,22 +697,24 @@ struct Flash {
   int regime;
   double so, sg, rs;
 };
-inline Flash resolve_cell_flash(const Sim& s, double p, double sw, double hc, int regime) {
+inline Flash resolve_cell_flash(const Sim& s, double p, double sw, double hc, int regime, double base_rs = NAN) {
   const double raw_total = 1.0 - sw;
   const double bounded_total = rmax(raw_total, 0.0);
   if (!s.three_phase || !s.has_pvt) return Flash{regime, bounded_total, 0.0, 0.0};
   if (regime == 0) {
     const double sg = hc;
-    const double rs = pvt_interpolate(s.pvt, p).rs;
+    double rs = pvt_interpolate(s.pvt, p).rs;
+    if (!std::isnan(base_rs)) rs = rmin(rs, base_rs);
     return Flash{regime, raw_total - sg, sg, rs};
   }
-  const double rs_cap = rmax(pvt_interpolate(s.pvt, p).rs, 0.0);
+  double rs_cap = rmax(pvt_interpolate(s.pvt, p).rs, 0.0);
+  if (!std::isnan(base_rs)) rs_cap = rmin(rs_cap, rmax(base_rs, 0.0));
   const double rs_trial = hc;
   if (rs_trial <= rs_cap + 1e-6) return Flash{regime, raw_total, 0.0, rs_trial};
   const double bo_trial = rmax(get_b_o_for_rs(s, p, rs_trial), 1e-9);
   const double dissolved = raw_total * rs_trial / bo_trial;
   Flash f;
-  split_gas_plain(s, p, 1.0, sw, 0.0, dissolved, f.sg, f.so, f.rs);
+  split_gas_plain(s, p, 1.0, sw, 0.0, dissolved, base_rs, f.sg, f.so, f.rs);
   f.regime = f.sg > 1e-12 ? 0 : 1;
   return f;
 }
@@ -672,7 +724,7 @@ struct Derived {
   double so, sg, rs, bo, bg;
 };
 inline Derived derive_cell(const Sim& s, const Cell& c) {
-  const Flash f = resolve_cell_flash(s, c.p, c.sw, c.hc, c.regime);
+  const Flash f = resolve_cell_flash(s, c.p, c.sw, c.hc, c.regime, c.base_rs);
   Derived d;
   d.so = f.so;
   d.sg = f.sg;
@@ -802,6 +854,7 @@ template <class S>
 struct WellCell {
   S p, sw, hc;
   int regime;
+  double base_rs = NAN;  // DRSDT0 cap
 };
 template <class S>
 struct Fractions {
@@ -811,7 +864,7 @@ struct Fractions {
 template <class S>
 inline Fractions<S> producer_fractions_g(const Sim& s, const WellCell<S>& c) {
   S lw = sc<S>(0.0), lo = sc<S>(0.0), lg = sc<S>(0.0);
-  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc, c.base_rs);
   Mob<S> m = phase_mobilities_g(s, c.sw, pr.sg, c.p, pr.rs);
   lw = lw + max_floor(m.w, 0.0);
   lo = lo + max_floor(m.o, 0.0);
@@ -827,7 +880,7 @@ inline Fractions<S> producer_fractions_g(const Sim& s, const WellCell<S>& c) {
 template <class S>
 inline S connection_rate_g(const Sim& s, double wi, double head, bool injector, const WellCell<S>& c,
                            const S& bhp) {
-  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc, c.base_rs);
   Mob<S> m = phase_mobilities_g(s, c.sw, pr.sg, c.p, pr.rs);
   S cm = max_floor(m.w + m.o + m.g, 0.0);
   S raw = (cm * (c.p - bhp - sc<S>(head))) * wi;
@@ -838,7 +891,7 @@ inline S connection_rate_g(const Sim& s, double wi, double head, bool injector, 
 template <class S>
 inline void component_coefficients_g(const Sim& s, bool injector, const WellCell<S>& c,
                                      const Fractions<S>* f, S out[3]) {
-  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc, c.base_rs);
   if (injector) {
     if (injected_fluid(s) == 1) {
       out[0] = sc<S>(0.0);
@@ -861,7 +914,7 @@ inline void component_coefficients_g(const Sim& s, bool injector, const WellCell
 template <class S>
 inline S perforation_surface_rate_g(const Sim& s, bool injector, const WellCell<S>& c,
                                     const Fractions<S>* f, const S& q) {
-  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc);
+  Props<S> pr = cell_props_g(s, c.regime, c.p, c.sw, c.hc, c.base_rs);
   if (injector) {
     S clamped = max_floor(-q, 0.0);
     if (injected_fluid(s) == 1) return clamped / max_floor(pr.bg, 1e-9);

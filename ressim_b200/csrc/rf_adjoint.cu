@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_accum(const __grid_constant__ Fl
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     Dual<3> cd[3];
     if (f.three_phase)
-      inventory3<Dual<3>>(f, pv[i], reg[i], dvar<3>(p[i], 0), dvar<3>(sw[i], 1), dvar<3>(hc[i], 2), cd);
+      inventory3<Dual<3>>(f, pv[i], reg[i], dvar<3>(p[i], 0), dvar<3>(sw[i], 1), dvar<3>(hc[i], 2), 0.0, cd);
     else
       inventory<Dual<3>>(f, pv[i], dvar<3>(p[i], 0), dvar<3>(sw[i], 1), dvar<3>(hc[i], 2), cd);
     const double l0 = lam[3 * i], l1 = lam[3 * i + 1], l2 = lam[3 * i + 2];

@@ -73,10 +73,12 @@ static WellControlH well_control(const Ctx& c, int w) {
 struct PerfCells {
   std::vector<double> v;
   std::vector<int> reg;
+  std::vector<double> rs0;  // gas redissolution off: the cell's Rs at the substep start (the cap)
   double p(int k) const { return v[3 * k]; }
   double sw(int k) const { return v[3 * k + 1]; }
   double hc(int k) const { return v[3 * k + 2]; }
   int regime(int k) const { return reg.empty() ? 0 : reg[k]; }
+  double base(int k) const { return rs0.empty() ? 0.0 : rs0[k]; }
 };
 
 static void gather_perf(Ctx& c, const double* p, const double* sw, const double* hc, PerfCells& pc) {
@@ -93,6 +95,12 @@ static void gather_perf(Ctx& c, const double* p, const double* sw, const double*
   for (int k = 0; k < P; ++k) {
     for (int e = 0; e < 3; ++e) pc.v[3 * k + e] = t[4 * k + e];
     pc.reg[k] = int(t[4 * k + 3]);
+  }
+  pc.rs0.clear();
+  if (c.fluid.drsdt0) {
+    gather_perf_cells3(c, c.d_rs.p, c.d_rs.p, c.d_rs.p, nullptr, t);
+    pc.rs0.resize(P);
+    for (int k = 0; k < P; ++k) pc.rs0[k] = t[4 * k];
   }
 }
 
@@ -118,7 +126,7 @@ static bool connection_rate_for_bhp(const Ctx& c, const PerfCells& pc, int k, do
   if (c.fluid.three_phase) {
     // fim/wells.rs:1098-1129 with the cell's flashed Sg and Rs
     const Fluid& f = c.hfluid;
-    const Derived3 d = derive_cell3(f, pc.p(k), pc.sw(k), pc.hc(k), pc.regime(k));
+    const Derived3 d = derive_cell3(f, pc.p(k), pc.sw(k), pc.hc(k), pc.regime(k), pc.base(k));
     const Mob3<double> m = mobilities3_f64(f, pc.sw(k), d.sg, pc.p(k), d.rs);
     if (!c.topo.perf_has_wi[k]) return false;
     const double mob = fmax(m.w + m.o + m.g, 0.0);
@@ -140,7 +148,7 @@ static double surface_rate_sc(const Ctx& c, const PerfCells& pc, int k, double q
   if (c.fluid.three_phase) {
     // perforation_surface_rate_sc_day (fim/wells.rs:1147-1170)
     const Fluid& f = c.hfluid;
-    const Derived3 d = derive_cell3(f, pc.p(k), pc.sw(k), pc.hc(k), pc.regime(k));
+    const Derived3 d = derive_cell3(f, pc.p(k), pc.sw(k), pc.hc(k), pc.regime(k), pc.base(k));
     if (c.topo.perf_inj[k]) {
       if (f.inject_gas) return fmax(-q, 0.0) / fmax(d.bg, 1e-9);
       return fmax(-q, 0.0) * inv_bw(f, pc.p(k));
@@ -571,7 +579,7 @@ static void record_step3(Ctx& c, const WellState& ws, double dt, double water_ch
   }
   for (int p = 0; p < c.topo.n_perfs; ++p) {
     const double q = ws.q[p];
-    const Derived3 d = derive_cell3(f, pc.p(p), pc.sw(p), pc.hc(p), pc.regime(p));
+    const Derived3 d = derive_cell3(f, pc.p(p), pc.sw(p), pc.hc(p), pc.regime(p), pc.base(p));
     if (c.topo.perf_inj[p]) {
       inj_res += fmax(-q, 0.0);
       if (f.inject_gas) {
@@ -884,10 +892,6 @@ static int load(Ctx& c, const RfDeck* d) {
   if (d->three_phase_mode) {
     if (d->n_pvt_rows < 1 || !d->pvt_rows) {
       c.err = "three-phase mode without a PVT table is not supported";
-      return RF_ERR_UNSUPPORTED;
-    }
-    if (!d->gas_redissolution_enabled) {
-      c.err = "three-phase mode with gas redissolution disabled (DRSDT0) is not supported";
       return RF_ERR_UNSUPPORTED;
     }
   } else if (d->n_pvt_rows > 0 && d->pvt_rows) {

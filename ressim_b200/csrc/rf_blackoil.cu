@@ -29,10 +29,12 @@ __global__ void __launch_bounds__(128) k_cells3(const __grid_constant__ Fluid f,
                                                  const double* __restrict__ hc, const double* __restrict__ pp,
                                                  const double* __restrict__ psw, const double* __restrict__ phc,
                                                  const int* __restrict__ row_ptr, const int* __restrict__ stencil,
-                                                 double* __restrict__ res, double* __restrict__ val) {
+                                                 double* __restrict__ res, double* __restrict__ val,
+                                                 const double* __restrict__ base_rs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nx * ny * nz) return;
-  cell_row3(f, nx, ny, nz, i, dt, pv, tx, ty, tz, depth, reg, p, sw, hc, pp, psw, phc, row_ptr, stencil, res, val);
+  cell_row3(f, nx, ny, nz, i, dt, pv, tx, ty, tz, depth, reg, p, sw, hc, pp, psw, phc, row_ptr, stencil, res, val,
+            base_rs);
 }
 
 __global__ void k_perfs3(const __grid_constant__ Fluid f, int n_wells, int n_perfs, double dt, const int* __restrict__ perf_cell,
@@ -42,11 +44,12 @@ __global__ void k_perfs3(const __grid_constant__ Fluid f, int n_wells, int n_per
                          const double* __restrict__ p, const double* __restrict__ sw, const double* __restrict__ hc,
                          const double* __restrict__ bhp, const double* __restrict__ q, const int* __restrict__ diag_pos,
                          double* __restrict__ res, double* __restrict__ val, double* __restrict__ res_tail,
-                         double* __restrict__ jrw, double* __restrict__ jwr_perf, double* __restrict__ jww_perf_bhp) {
+                         double* __restrict__ jrw, double* __restrict__ jwr_perf, double* __restrict__ jww_perf_bhp,
+                         const double* __restrict__ base_rs) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_perfs) return;
   perf_row3(f, n_wells, k, dt, perf_cell, perf_inj, perf_well, perf_has_wi, perf_wi, perf_head, reg, p, sw, hc, bhp,
-            q, diag_pos, res, val, res_tail, jrw, jwr_perf, jww_perf_bhp);
+            q, diag_pos, res, val, res_tail, jrw, jwr_perf, jww_perf_bhp, base_rs);
 }
 
 __global__ void k_wells3(const __grid_constant__ Fluid f, int n_wells, const WellControlH* __restrict__ ctrl, const int* __restrict__ well_ptr,
@@ -54,11 +57,11 @@ __global__ void k_wells3(const __grid_constant__ Fluid f, int n_wells, const Wel
                          const int* __restrict__ reg, const double* __restrict__ p, const double* __restrict__ sw,
                          const double* __restrict__ hc, const double* __restrict__ bhp, const double* __restrict__ q,
                          double* __restrict__ res_tail, double* __restrict__ jwr_ctrl, double* __restrict__ jww_ctrl_q,
-                         double* __restrict__ jww_ctrl_bhp) {
+                         double* __restrict__ jww_ctrl_bhp, const double* __restrict__ base_rs) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= n_wells) return;
   well_row3(f, w, ctrl[w], well_ptr, well_perfs, perf_cell, reg, p, sw, hc, bhp, q, res_tail, jwr_ctrl, jww_ctrl_q,
-            jww_ctrl_bhp);
+            jww_ctrl_bhp, base_rs);
 }
 
 // Scaled residual maxima, FVF sums, CNV maxima, residual sums and the pore-volume sum, as
@@ -146,7 +149,7 @@ __global__ void __launch_bounds__(kBlock) k_from_sim3(const __grid_constant__ Fl
                                                        const double* __restrict__ sg, const double* __restrict__ rs,
                                                        int* __restrict__ reg, double* __restrict__ hc) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int r = classify_regime(f, p[i], sg[i], rs[i]);
+    const int r = classify_regime(f, p[i], sg[i], rs[i], rs[i]);
     reg[i] = r;
     hc[i] = r == 0 ? sg[i] : rs[i];
   }
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(kBlock) k_derive3(const __grid_constant__ Flui
                                                      const int* __restrict__ reg, double* __restrict__ so,
                                                      double* __restrict__ sg, double* __restrict__ rs) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const Derived3 d = derive_cell3(f, p[i], sw[i], hc[i], reg[i]);
+    const Derived3 d = derive_cell3(f, p[i], sw[i], hc[i], reg[i], rs[i]);  // base: Rs before the write
     so[i] = d.so;
     sg[i] = d.sg;
     rs[i] = d.rs;
@@ -244,19 +247,20 @@ void launch_assembly3(Ctx& c, double dt) {
   k_cells3<<<blocks_for(c.n, 128), 128, 0, c.stream>>>(c.fluid, c.nx, c.ny, c.nz, dt, c.d_pv.p, c.d_tx.p, c.d_ty.p,
                                                         c.d_tz.p, c.d_depth.p, c.d_reg.p, c.d_p.p, c.d_sw.p, c.d_hc.p,
                                                         c.d_pp.p, c.d_psw.p, c.d_phc.p, c.d_row_ptr.p, c.d_stencil.p,
-                                                        c.d_res.p, c.d_val.p);
+                                                        c.d_res.p, c.d_val.p, c.d_rs.p);
   c.launches++;
   if (c.topo.n_perfs > 0) {
     k_perfs3<<<blocks_for(c.topo.n_perfs, 64), 64, 0, c.stream>>>(
         c.fluid, c.topo.n_wells, c.topo.n_perfs, dt, c.d_perf_cell.p, c.d_perf_inj.p, c.d_perf_well.p,
         c.d_perf_has_wi.p, c.d_perf_wi.p, c.d_perf_head.p, c.d_reg.p, c.d_p.p, c.d_sw.p, c.d_hc.p, c.d_bhp.p, c.d_q.p,
-        c.d_diag.p, c.d_res.p, c.d_val.p, c.d_res_tail.p, c.d_jrw.p, c.d_jwr_perf.p, c.d_jww_perf_bhp.p);
+        c.d_diag.p, c.d_res.p, c.d_val.p, c.d_res_tail.p, c.d_jrw.p, c.d_jwr_perf.p, c.d_jww_perf_bhp.p, c.d_rs.p);
     c.launches++;
   }
   if (c.topo.n_wells > 0) {
     k_wells3<<<blocks_for(c.topo.n_wells, 32), 32, 0, c.stream>>>(
         c.fluid, c.topo.n_wells, c.d_ctrl.p, c.d_well_ptr.p, c.d_well_perfs.p, c.d_perf_cell.p, c.d_reg.p, c.d_p.p,
-        c.d_sw.p, c.d_hc.p, c.d_bhp.p, c.d_q.p, c.d_res_tail.p, c.d_jwr_ctrl.p, c.d_jww_ctrl_q.p, c.d_jww_ctrl_bhp.p);
+        c.d_sw.p, c.d_hc.p, c.d_bhp.p, c.d_q.p, c.d_res_tail.p, c.d_jwr_ctrl.p, c.d_jww_ctrl_q.p, c.d_jww_ctrl_bhp.p,
+        c.d_rs.p);
     c.launches++;
   }
 }

@@ -554,21 +554,44 @@ RF_HD_CALL double solve_rs_plain(const Fluid& f, double p, double sw, double sg,
   return 0.5 * (lo + hi);
 }
 
-// split_gas_inventory_after_transport (step.rs:106-200), plain
+// split_gas_inventory_after_transport (step.rs:106-200), plain; base: the DRSDT0 Rs cap (read
+// only when f.drsdt0)
 RF_HD_CALL void split_gas_plain(const Fluid& f, double p, double pv, double sw, double free_sc, double dissolved_sc,
-                           double& sg, double& so, double& rs) {
+                                double base, double& sg, double& so, double& rs) {
   const double total_hc = fmax(1.0 - sw, 0.0);
   const double bg = fmax(get_b_g(f, p), 1e-9);
   const double free_t = fmax(free_sc, 0.0);
   const double sg_t = clamp01((free_t * bg) / fmax(pv, 1e-9), 0.0, total_hc);
+  const double so_t = fmax(total_hc - sg_t, 0.0);
   const double dissolved = fmax(dissolved_sc, 0.0);
   const double rs_max = fmax(pvt_interpolate(f, p).rs, 0.0);
+  const bool redis = !f.drsdt0;
+  const double cap = redis ? rs_max : fmin(fmax(base, 0.0), rs_max);
+  double bo_cap, mu;
+  pvt_interpolate_oil(f, p, cap, bo_cap, mu);
+  bo_cap = fmax(bo_cap, 1e-9);
+  if (!redis) {
+    const double max_t = (so_t * pv / bo_cap) * cap;
+    if (dissolved <= max_t + 1e-9) {
+      rs = solve_rs_plain(f, p, sw, sg_t, pv, dissolved, cap);
+      sg = sg_t;
+      so = so_t;
+      return;
+    }
+  }
   const double total_gas = free_t + dissolved;
-  double bo_sat_raw, mu;
-  pvt_interpolate_oil(f, p, rs_max, bo_sat_raw, mu);
-  const double bo_sat = fmax(bo_sat_raw, 1e-9), rs_sat = rs_max;
+  double rs_sat, bo_sat;
+  if (redis) {
+    double bo_sat_raw;
+    pvt_interpolate_oil(f, p, rs_max, bo_sat_raw, mu);
+    rs_sat = rs_max;
+    bo_sat = fmax(bo_sat_raw, 1e-9);
+  } else {
+    rs_sat = cap;
+    bo_sat = bo_cap;
+  }
   const double max_all = (total_hc * pv / bo_sat) * rs_sat;
-  if (total_gas <= max_all + 1e-9) {
+  if (redis && total_gas <= max_all + 1e-9) {
     rs = solve_rs_plain(f, p, sw, 0.0, pv, total_gas, rs_sat);
     sg = 0.0;
     so = total_hc;
@@ -576,7 +599,7 @@ RF_HD_CALL void split_gas_plain(const Fluid& f, double p, double pv, double sw, 
   }
   const double denom = (1.0 / bg) - (rs_sat / bo_sat);
   const double sg_sat = fabs(denom) > 1e-12 ? ((total_gas / pv) - (total_hc * rs_sat / bo_sat)) / denom : sg_t;
-  sg = clamp01(sg_sat, 0.0, total_hc);
+  sg = clamp01(sg_sat, redis ? 0.0 : sg_t, total_hc);
   so = fmax(total_hc - sg, 0.0);
   rs = rs_sat;
 }
@@ -605,22 +628,43 @@ RF_HD S solve_rs_g(const Fluid& f, const S& p, const S& sw, const S& sg, const S
 }
 // split_gas_inventory_after_transport_generic (flash_ad.rs:104-207)
 template <class S>
-RF_HD_CALL void split_gas_g(const Fluid& f, const S& p, const S& pv, const S& sw, const S& free_sc, const S& dissolved_sc,
-                       S& sg, S& so, S& rs) {
+RF_HD_CALL void split_gas_g(const Fluid& f, const S& p, const S& pv, const S& sw, const S& free_sc,
+                            const S& dissolved_sc, double base, S& sg, S& so, S& rs) {
   S total_hc = floor_at(lift<S>(1.0) - sw, 0.0);
   const SatProps<S> sat = pvt_saturated_g(f, p);
   S bg = floor_at(sat.bg, 1e-9);
   S free_t = floor_at(free_sc, 0.0);
   S sg_t = smin(floor_at((free_t * bg) / floor_at(pv, 1e-9), 0.0), total_hc);
+  S so_t = floor_at(total_hc - sg_t, 0.0);
   S dissolved = floor_at(dissolved_sc, 0.0);
   S rs_max = floor_at(sat.rs, 0.0);
+  const bool redis = !f.drsdt0;
+  S cap = redis ? rs_max : smin(lift<S>(fmax(base, 0.0)), rs_max);
+  S bo_cap, mu;
+  pvt_oil_sat_g(f, sat, p, cap, bo_cap, mu);
+  bo_cap = floor_at(bo_cap, 1e-9);
+  if (!redis) {
+    S max_t = (so_t * pv / bo_cap) * cap;
+    if (value(dissolved) <= value(max_t) + 1e-9) {
+      rs = solve_rs_g(f, p, sw, sg_t, pv, dissolved, value(cap));
+      sg = sg_t;
+      so = so_t;
+      return;
+    }
+  }
   S total_gas = free_t + dissolved;
-  S bo_sat_raw, mu;
-  pvt_oil_sat_g(f, sat, p, rs_max, bo_sat_raw, mu);
-  S bo_sat = floor_at(bo_sat_raw, 1e-9);
-  S rs_sat = rs_max;
+  S rs_sat, bo_sat;
+  if (redis) {
+    S bo_sat_raw;
+    pvt_oil_sat_g(f, sat, p, rs_max, bo_sat_raw, mu);
+    rs_sat = rs_max;
+    bo_sat = floor_at(bo_sat_raw, 1e-9);
+  } else {
+    rs_sat = cap;
+    bo_sat = bo_cap;
+  }
   S max_all = (total_hc * pv / bo_sat) * rs_sat;
-  if (value(total_gas) <= value(max_all) + 1e-9) {
+  if (redis && value(total_gas) <= value(max_all) + 1e-9) {
     rs = solve_rs_g(f, p, sw, lift<S>(0.0), pv, total_gas, value(rs_sat));
     sg = lift<S>(0.0);
     so = total_hc;
@@ -628,15 +672,16 @@ RF_HD_CALL void split_gas_g(const Fluid& f, const S& p, const S& pv, const S& sw
   }
   S denom = srecip(bg) - (rs_sat / bo_sat);
   S sg_sat = fabs(value(denom)) > 1e-12 ? ((total_gas / pv) - (total_hc * rs_sat / bo_sat)) / denom : sg_t;
-  sg = smin(smax(sg_sat, lift<S>(0.0)), total_hc);
+  sg = smin(smax(sg_sat, redis ? lift<S>(0.0) : sg_t), total_hc);
   so = floor_at(total_hc - sg, 0.0);
   rs = rs_sat;
 }
 
 // classify_cell_regime (flash.rs:13-40): 0 saturated, 1 undersaturated
-RF_HD int classify_regime(const Fluid& f, double p, double sg, double rs) {
+RF_HD int classify_regime(const Fluid& f, double p, double sg, double rs, double base) {
   if (sg > 1e-9) return 0;
-  const double rs_sat = pvt_interpolate(f, p).rs;
+  double rs_sat = pvt_interpolate(f, p).rs;
+  if (f.drsdt0) rs_sat = fmin(rs_sat, base);
   return rs < rs_sat - 1e-6 ? 1 : 0;
 }
 
@@ -645,16 +690,18 @@ struct Derived3 {
   int regime;
   double so, sg, rs, bo, bg;
 };
-RF_HD Derived3 derive_cell3(const Fluid& f, double p, double sw, double hc, int regime) {
+RF_HD Derived3 derive_cell3(const Fluid& f, double p, double sw, double hc, int regime, double base) {
   Derived3 d;
   const double raw_total = 1.0 - sw;
   d.regime = regime;
   if (regime == 0) {
     d.sg = hc;
     d.rs = pvt_interpolate(f, p).rs;
+    if (f.drsdt0) d.rs = fmin(d.rs, base);
     d.so = raw_total - d.sg;
   } else {
-    const double rs_cap = fmax(pvt_interpolate(f, p).rs, 0.0);
+    double rs_cap = fmax(pvt_interpolate(f, p).rs, 0.0);
+    if (f.drsdt0) rs_cap = fmin(rs_cap, fmax(base, 0.0));
     const double rs_trial = hc;
     if (rs_trial <= rs_cap + 1e-6) {
       d.so = raw_total;
@@ -663,7 +710,7 @@ RF_HD Derived3 derive_cell3(const Fluid& f, double p, double sw, double hc, int 
     } else {
       const double bo_trial = fmax(bo_for_rs(f, p, rs_trial), 1e-9);
       const double dissolved = raw_total * rs_trial / bo_trial;
-      split_gas_plain(f, p, 1.0, sw, 0.0, dissolved, d.sg, d.so, d.rs);
+      split_gas_plain(f, p, 1.0, sw, 0.0, dissolved, base, d.sg, d.so, d.rs);
       d.regime = d.sg > 1e-12 ? 0 : 1;
     }
   }
@@ -682,7 +729,7 @@ struct Props3 {
 };
 // cell_props_generic, black-oil branch (properties.rs:37-133)
 template <class S>
-RF_HD_CALL Props3<S> cell_props3(const Fluid& f, int regime, const S& p, const S& sw, const S& hc) {
+RF_HD_CALL Props3<S> cell_props3(const Fluid& f, int regime, const S& p, const S& sw, const S& hc, double base) {
   const S raw_total = lift<S>(1.0) - sw;
   const SatProps<S> sat = pvt_saturated_g(f, p);
   Props3<S> pr;
@@ -690,12 +737,14 @@ RF_HD_CALL Props3<S> cell_props3(const Fluid& f, int regime, const S& p, const S
   if (regime == 0) {
     pr.sg = hc;
     pr.rs = sat.rs;
+    if (f.drsdt0) pr.rs = ceil_at(pr.rs, base);
     pr.so = raw_total - pr.sg;
     pvt_oil_sat_g(f, sat, p, pr.rs, pr.bo, mu);
     pr.bg = sat.bg;
     return pr;
   }
   S rs_cap = floor_at(sat.rs, 0.0);
+  if (f.drsdt0) rs_cap = smin(rs_cap, lift<S>(fmax(base, 0.0)));
   const S& rs_trial = hc;
   if (value(rs_trial) <= value(rs_cap) + 1e-6) {
     pr.sg = lift<S>(0.0);
@@ -706,7 +755,7 @@ RF_HD_CALL Props3<S> cell_props3(const Fluid& f, int regime, const S& p, const S
     pvt_oil_sat_g(f, sat, p, rs_trial, bo_t, mu);
     bo_t = floor_at(bo_t, 1e-9);
     S dissolved = raw_total * rs_trial / bo_t;
-    split_gas_g(f, p, lift<S>(1.0), sw, lift<S>(0.0), dissolved, pr.sg, pr.so, pr.rs);
+    split_gas_g(f, p, lift<S>(1.0), sw, lift<S>(0.0), dissolved, base, pr.sg, pr.so, pr.rs);
   }
   pvt_oil_sat_g(f, sat, p, pr.rs, pr.bo, mu);
   pr.bg = sat.bg;
@@ -715,8 +764,9 @@ RF_HD_CALL Props3<S> cell_props3(const Fluid& f, int regime, const S& p, const S
 
 // component inventory [water, oil, gas] (properties.rs:157-169)
 template <class S>
-RF_HD void inventory3(const Fluid& f, double pv_ref, int regime, const S& p, const S& sw, const S& hc, S out[3]) {
-  Props3<S> pr = cell_props3(f, regime, p, sw, hc);
+RF_HD void inventory3(const Fluid& f, double pv_ref, int regime, const S& p, const S& sw, const S& hc, double base,
+                      S out[3]) {
+  Props3<S> pr = cell_props3(f, regime, p, sw, hc, base);
   S pv = lift<S>(pv_ref) * sexp((p - f.p_rref) * f.c_r);
   out[0] = pv * sw * inv_bw(f, p);
   out[1] = pv * pr.so / floor_at(pr.bo, 1e-9);
@@ -726,9 +776,10 @@ RF_HD void inventory3(const Fluid& f, double pv_ref, int regime, const S& p, con
 // face_flux_terms_generic, three-phase (flux.rs:42-191); slots 0-2 cell i, 3-5 cell j for Dual<6>
 template <class S>
 RF_HD void face_flux3(const Fluid& f, double trans, double depth_i, double depth_j, int reg_i, const S& pi,
-                      const S& swi, const S& hci, int reg_j, const S& pj, const S& swj, const S& hcj, S out[3]) {
-  Props3<S> ci = cell_props3(f, reg_i, pi, swi, hci);
-  Props3<S> cj = cell_props3(f, reg_j, pj, swj, hcj);
+                      const S& swi, const S& hci, int reg_j, const S& pj, const S& swj, const S& hcj, S out[3],
+                      double base_i = 0.0, double base_j = 0.0) {
+  Props3<S> ci = cell_props3(f, reg_i, pi, swi, hci, base_i);
+  Props3<S> cj = cell_props3(f, reg_j, pj, swj, hcj, base_j);
   S pcwi = pcow(f, swi), pcwj = pcow(f, swj);
   S pcgi = pc_og(f, ci.sg), pcgj = pc_og(f, cj.sg);
   S gw = lift<S>(0.0), go = lift<S>(0.0), gg = lift<S>(0.0);
@@ -788,8 +839,8 @@ RF_HD Frac3<S> producer_fractions3(const Fluid& f, const Props3<S>& pr, const S&
 }
 template <class S>
 RF_HD S connection_rate3(const Fluid& f, double wi, double head, bool injector, int regime, const S& p, const S& sw,
-                         const S& hc, const S& bhp) {
-  Props3<S> pr = cell_props3(f, regime, p, sw, hc);
+                         const S& hc, const S& bhp, double base = 0.0) {
+  Props3<S> pr = cell_props3(f, regime, p, sw, hc, base);
   Mob3<S> m = mobilities3(f, sw, pr.sg, p, pr.rs);
   S cm = floor_at(m.w + m.o + m.g, 0.0);
   S raw = (cm * (p - bhp - lift<S>(head))) * wi;
@@ -798,8 +849,8 @@ RF_HD S connection_rate3(const Fluid& f, double wi, double head, bool injector, 
 }
 template <class S>
 RF_HD void component_coefficients3(const Fluid& f, bool injector, int regime, const S& p, const S& sw, const S& hc,
-                                   S out[3]) {
-  Props3<S> pr = cell_props3(f, regime, p, sw, hc);
+                                   S out[3], double base = 0.0) {
+  Props3<S> pr = cell_props3(f, regime, p, sw, hc, base);
   if (injector) {
     if (f.inject_gas) {
       out[0] = lift<S>(0.0);
@@ -820,8 +871,9 @@ RF_HD void component_coefficients3(const Fluid& f, bool injector, int regime, co
   out[2] = fr.g / bg + oc * pr.rs;
 }
 template <class S>
-RF_HD S surface_rate3(const Fluid& f, bool injector, int regime, const S& p, const S& sw, const S& hc, const S& q) {
-  Props3<S> pr = cell_props3(f, regime, p, sw, hc);
+RF_HD S surface_rate3(const Fluid& f, bool injector, int regime, const S& p, const S& sw, const S& hc, const S& q,
+                      double base = 0.0) {
+  Props3<S> pr = cell_props3(f, regime, p, sw, hc, base);
   if (injector) {
     S clamped = floor_at(-q, 0.0);
     if (f.inject_gas) return clamped / floor_at(pr.bg, 1e-9);

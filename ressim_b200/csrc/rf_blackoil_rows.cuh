@@ -16,13 +16,14 @@ template <int DIR_SIGN>
 RF_HD_CALL void face_contrib3(const Fluid& f, double trans, double dt, double depth_lo,
                          double depth_hi, int reg_lo, double p_lo, double sw_lo, double hc_lo,
                          int reg_hi, double p_hi, double sw_hi, double hc_hi, double r[3],
-                         double diag[9], double* off) {
+                         double diag[9], double* off, double base_lo, double base_hi) {
   // lower-index cell = "i" (slots 0-2), higher = "j" (slots 3-5); DIR_SIGN +1: this cell is i
   double fv[3];
-  face_flux3<double>(f, trans, depth_lo, depth_hi, reg_lo, p_lo, sw_lo, hc_lo, reg_hi, p_hi, sw_hi, hc_hi, fv);
+  face_flux3<double>(f, trans, depth_lo, depth_hi, reg_lo, p_lo, sw_lo, hc_lo, reg_hi, p_hi, sw_hi, hc_hi, fv,
+                     base_lo, base_hi);
   Dual<6> fd[3];
   face_flux3<Dual<6>>(f, trans, depth_lo, depth_hi, reg_lo, dvar<6>(p_lo, 0), dvar<6>(sw_lo, 1), dvar<6>(hc_lo, 2),
-                      reg_hi, dvar<6>(p_hi, 3), dvar<6>(sw_hi, 4), dvar<6>(hc_hi, 5), fd);
+                      reg_hi, dvar<6>(p_hi, 3), dvar<6>(sw_hi, 4), dvar<6>(hc_hi, 5), fd, base_lo, base_hi);
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
     if (DIR_SIGN > 0) {
@@ -53,7 +54,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
                      const double* __restrict__ hc, const double* __restrict__ pp,
                      const double* __restrict__ psw, const double* __restrict__ phc,
                      const int* __restrict__ row_ptr, const int* __restrict__ stencil,
-                     double* __restrict__ res, double* __restrict__ val) {
+                     double* __restrict__ res, double* __restrict__ val,
+                     const double* __restrict__ base_rs) {
   const int nxy = nx * ny;
   const int ci = i % nx, cj = (i / nx) % ny, ck = i / nxy;
   for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
@@ -63,14 +65,17 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
   // accumulation; the previous inventory uses the same (frozen) regime, as the substep's
   // previous state and first iterate are the same classified state
   const int ri = reg[i];
+  // the DRSDT0 Rs cap of a cell: the simulator's Rs at the substep start
+  auto base = [&](int c) { return f.drsdt0 ? base_rs[c] : 0.0; };
+  const double bi = base(i);
   double cur[3], prev[3];
-  inventory3<double>(f, pv[i], ri, p[i], sw[i], hc[i], cur);
-  inventory3<double>(f, pv[i], ri, pp[i], psw[i], phc[i], prev);
+  inventory3<double>(f, pv[i], ri, p[i], sw[i], hc[i], bi, cur);
+  inventory3<double>(f, pv[i], ri, pp[i], psw[i], phc[i], bi, prev);
   double r[3] = {0.0 + (cur[0] - prev[0]), 0.0 + (cur[1] - prev[1]), 0.0 + (cur[2] - prev[2])};
   double diag[9];
   {
     Dual<3> cd[3];
-    inventory3<Dual<3>>(f, pv[i], ri, dvar<3>(p[i], 0), dvar<3>(sw[i], 1), dvar<3>(hc[i], 2), cd);
+    inventory3<Dual<3>>(f, pv[i], ri, dvar<3>(p[i], 0), dvar<3>(sw[i], 1), dvar<3>(hc[i], 2), bi, cd);
 #pragma unroll
     for (int e = 0; e < 3; ++e)
 #pragma unroll
@@ -84,7 +89,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
     const int nb = i - nxy;
     const double t = tz[nb];
     if (t > 0.0) {
-      face_contrib3<-1>(f, t, dt, depth[ck - 1], dk, reg[nb], p[nb], sw[nb], hc[nb], ri, pi, swi, hci, r, diag, off);
+      face_contrib3<-1>(f, t, dt, depth[ck - 1], dk, reg[nb], p[nb], sw[nb], hc[nb], ri, pi, swi, hci, r, diag, off,
+                        base(nb), bi);
 #pragma unroll
       for (int e = 0; e < 9; ++e) val[size_t(st[kZm]) * 9 + e] = off[e];
     }
@@ -93,7 +99,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
     const int nb = i - nx;
     const double t = ty[nb];
     if (t > 0.0) {
-      face_contrib3<-1>(f, t, dt, dk, dk, reg[nb], p[nb], sw[nb], hc[nb], ri, pi, swi, hci, r, diag, off);
+      face_contrib3<-1>(f, t, dt, dk, dk, reg[nb], p[nb], sw[nb], hc[nb], ri, pi, swi, hci, r, diag, off,
+                        base(nb), bi);
 #pragma unroll
       for (int e = 0; e < 9; ++e) val[size_t(st[kYm]) * 9 + e] = off[e];
     }
@@ -102,7 +109,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
     const int nb = i - 1;
     const double t = tx[nb];
     if (t > 0.0) {
-      face_contrib3<-1>(f, t, dt, dk, dk, reg[nb], p[nb], sw[nb], hc[nb], ri, pi, swi, hci, r, diag, off);
+      face_contrib3<-1>(f, t, dt, dk, dk, reg[nb], p[nb], sw[nb], hc[nb], ri, pi, swi, hci, r, diag, off,
+                        base(nb), bi);
 #pragma unroll
       for (int e = 0; e < 9; ++e) val[size_t(st[kXm]) * 9 + e] = off[e];
     }
@@ -111,7 +119,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
     const int nb = i + 1;
     const double t = tx[i];
     if (t > 0.0) {
-      face_contrib3<1>(f, t, dt, dk, dk, ri, pi, swi, hci, reg[nb], p[nb], sw[nb], hc[nb], r, diag, off);
+      face_contrib3<1>(f, t, dt, dk, dk, ri, pi, swi, hci, reg[nb], p[nb], sw[nb], hc[nb], r, diag, off,
+                       bi, base(nb));
 #pragma unroll
       for (int e = 0; e < 9; ++e) val[size_t(st[kXp]) * 9 + e] = off[e];
     }
@@ -120,7 +129,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
     const int nb = i + nx;
     const double t = ty[i];
     if (t > 0.0) {
-      face_contrib3<1>(f, t, dt, dk, dk, ri, pi, swi, hci, reg[nb], p[nb], sw[nb], hc[nb], r, diag, off);
+      face_contrib3<1>(f, t, dt, dk, dk, ri, pi, swi, hci, reg[nb], p[nb], sw[nb], hc[nb], r, diag, off,
+                       bi, base(nb));
 #pragma unroll
       for (int e = 0; e < 9; ++e) val[size_t(st[kYp]) * 9 + e] = off[e];
     }
@@ -129,7 +139,8 @@ RF_HD void cell_row3(const Fluid& f, int nx, int ny, int nz, int i, double dt,
     const int nb = i + nxy;
     const double t = tz[i];
     if (t > 0.0) {
-      face_contrib3<1>(f, t, dt, dk, depth[ck + 1], ri, pi, swi, hci, reg[nb], p[nb], sw[nb], hc[nb], r, diag, off);
+      face_contrib3<1>(f, t, dt, dk, depth[ck + 1], ri, pi, swi, hci, reg[nb], p[nb], sw[nb], hc[nb], r, diag, off,
+                       bi, base(nb));
 #pragma unroll
       for (int e = 0; e < 9; ++e) val[size_t(st[kZp]) * 9 + e] = off[e];
     }
@@ -148,19 +159,21 @@ RF_HD void perf_row3(const Fluid& f, int n_wells, int k, double dt, const int* _
                      const double* __restrict__ p, const double* __restrict__ sw, const double* __restrict__ hc,
                      const double* __restrict__ bhp, const double* __restrict__ q, const int* __restrict__ diag_pos,
                      double* __restrict__ res, double* __restrict__ val, double* __restrict__ res_tail,
-                     double* __restrict__ jrw, double* __restrict__ jwr_perf, double* __restrict__ jww_perf_bhp) {
+                     double* __restrict__ jrw, double* __restrict__ jwr_perf, double* __restrict__ jww_perf_bhp,
+                     const double* __restrict__ base_rs) {
   const int c = perf_cell[k], w = perf_well[k], rg = reg[c];
+  const double bc = f.drsdt0 ? base_rs[c] : 0.0;
   const bool inj = perf_inj[k] != 0;
   const double pc = p[c], swc = sw[c], hcc = hc[c], b = bhp[w], qk = q[k];
   double coef[3];
-  component_coefficients3<double>(f, inj, rg, pc, swc, hcc, coef);
+  component_coefficients3<double>(f, inj, rg, pc, swc, hcc, coef, bc);
 #pragma unroll
   for (int e = 0; e < 3; ++e) res[3 * c + e] += coef[e] * qk * dt;
   double* dblk = val + size_t(diag_pos[c]) * 9;
   {
     Dual<4> P = dvar<4>(pc, 0), SW = dvar<4>(swc, 1), HC = dvar<4>(hcc, 2), Q = dvar<4>(qk, 3);
     Dual<4> ca[3];
-    component_coefficients3<Dual<4>>(f, inj, rg, P, SW, HC, ca);
+    component_coefficients3<Dual<4>>(f, inj, rg, P, SW, HC, ca, bc);
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
       Dual<4> row = ca[e] * Q;
@@ -170,10 +183,10 @@ RF_HD void perf_row3(const Fluid& f, int n_wells, int k, double dt, const int* _
     }
   }
   if (perf_has_wi[k]) {
-    const double conn = connection_rate3<double>(f, perf_wi[k], perf_head[k], inj, rg, pc, swc, hcc, b);
+    const double conn = connection_rate3<double>(f, perf_wi[k], perf_head[k], inj, rg, pc, swc, hcc, b, bc);
     res_tail[n_wells + k] = 0.0 + (qk - conn);
     Dual<4> ca = connection_rate3<Dual<4>>(f, perf_wi[k], perf_head[k], inj, rg, dvar<4>(pc, 0), dvar<4>(swc, 1),
-                                           dvar<4>(hcc, 2), dvar<4>(b, 3));
+                                           dvar<4>(hcc, 2), dvar<4>(b, 3), bc);
 #pragma unroll
     for (int v = 0; v < 3; ++v) jwr_perf[3 * k + v] = filt3(-ca.d[v]);
     jww_perf_bhp[k] = filt3(-ca.d[3]);
@@ -191,8 +204,9 @@ RF_HD void well_row3(const Fluid& f, int w, const WellControlH& c, const int* __
                      const int* __restrict__ reg, const double* __restrict__ p, const double* __restrict__ sw,
                      const double* __restrict__ hc, const double* __restrict__ bhp, const double* __restrict__ q,
                      double* __restrict__ res_tail, double* __restrict__ jwr_ctrl, double* __restrict__ jww_ctrl_q,
-                     double* __restrict__ jww_ctrl_bhp) {
+                     double* __restrict__ jww_ctrl_bhp, const double* __restrict__ base_rs) {
   const bool inj = c.injector != 0;
+  auto base = [&](int cell) { return f.drsdt0 ? base_rs[cell] : 0.0; };
   const double b = bhp[w];
   for (int a = well_ptr[w]; a < well_ptr[w + 1]; ++a) {
     const int k = well_perfs[a];
@@ -214,7 +228,7 @@ RF_HD void well_row3(const Fluid& f, int w, const WellControlH& c, const int* __
   for (int a = well_ptr[w]; a < well_ptr[w + 1]; ++a) {
     const int k = well_perfs[a], cell = perf_cell[k];
     actual = actual + (c.uses_surface_target
-                           ? surface_rate3<double>(f, inj, reg[cell], p[cell], sw[cell], hc[cell], q[k])
+                           ? surface_rate3<double>(f, inj, reg[cell], p[cell], sw[cell], hc[cell], q[k], base(cell))
                            : reservoir_rate<double>(inj, q[k]));
   }
   const double bhp_slack = inj ? c.bhp_limit - b : b - c.bhp_limit;
@@ -229,7 +243,7 @@ RF_HD void well_row3(const Fluid& f, int w, const WellControlH& c, const int* __
   for (int a = well_ptr[w]; a < well_ptr[w + 1]; ++a) {
     const int k = well_perfs[a], cell = perf_cell[k];
     Dual<4> P = dvar<4>(p[cell], 0), SW = dvar<4>(sw[cell], 1), HC = dvar<4>(hc[cell], 2), Q = dvar<4>(q[k], 3);
-    Dual<4> rate = c.uses_surface_target ? surface_rate3<Dual<4>>(f, inj, reg[cell], P, SW, HC, Q)
+    Dual<4> rate = c.uses_surface_target ? surface_rate3<Dual<4>>(f, inj, reg[cell], P, SW, HC, Q, base(cell))
                                          : reservoir_rate<Dual<4>>(inj, Q);
 #pragma unroll
     for (int v = 0; v < 3; ++v) jwr_ctrl[3 * k + v] = filt3(factor * rate.d[v]);

@@ -46,6 +46,7 @@ inline int fluid_from_deck(const RfDeck* d, Fluid& f, std::vector<double>& h_pvt
   fill_knots(f);
   if (d->three_phase_mode) {
     f.three_phase = 1;
+    f.drsdt0 = d->gas_redissolution_enabled ? 0 : 1;
     f.rho_g = d->rho_g;
     f.mu_g = d->mu_g;
     f.inject_gas = d->injected_fluid == 1;

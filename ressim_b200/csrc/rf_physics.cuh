@@ -219,6 +219,7 @@ struct Fluid {
   double knot_x[kMaxKnots], knot_krw[kMaxKnots], knot_kro[kMaxKnots];
   // three-phase black-oil mode (rf_blackoil.cuh); zero in two-phase mode
   int three_phase, has_scal3, has_pc_og, inject_gas;
+  int drsdt0;  // gas redissolution off: Rs capped at the cell's Rs at the substep start
   double mu_g;
   double s3_wc, s3_or, s3_nw, s3_no, s3_krw, s3_kro, s3_gc, s3_gr, s3_org, s3_ng, s3_krg;
   double pcog_entry, pcog_lambda;

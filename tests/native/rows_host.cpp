@@ -23,7 +23,7 @@ int32_t rfh_assemble3(const RfDeck* deck, double dt, const double* tx, const dou
                       const double* perf_wi, const double* perf_head, const int32_t* well_ptr,
                       const int32_t* well_perfs, const double* ctrl, const double* bhp, const double* q, double* res,
                       double* blocks, double* jrw, double* jwr_perf, double* jww_perf_bhp, double* jwr_ctrl,
-                      double* jww_ctrl_q, double* jww_ctrl_bhp) {
+                      double* jww_ctrl_q, double* jww_ctrl_bhp, const double* base_rs) {
   rf::Fluid f;
   std::vector<double> pvt;
   std::string err;
@@ -51,16 +51,17 @@ int32_t rfh_assemble3(const RfDeck* deck, double dt, const double* tx, const dou
   for (size_t k = 0; k < 63 * size_t(n); ++k) blocks[k] = 0.0;
   for (int i = 0; i < n; ++i)
     rf::cell_row3(f, nx, ny, nz, i, dt, pv, tx, ty, tz, depth_layer, reg, p.data(), sw.data(), hc.data(), pp.data(),
-                  psw.data(), phc.data(), row_ptr.data(), stencil.data(), res, blocks);
+                  psw.data(), phc.data(), row_ptr.data(), stencil.data(), res, blocks, base_rs);
   double* res_tail = res + 3 * size_t(n);
   for (int k = 0; k < n_perfs; ++k)
     rf::perf_row3(f, n_wells, k, dt, perf_cell, perf_inj, perf_well, perf_has_wi, perf_wi, perf_head, reg, p.data(),
-                  sw.data(), hc.data(), bhp, q, diag.data(), res, blocks, res_tail, jrw, jwr_perf, jww_perf_bhp);
+                  sw.data(), hc.data(), bhp, q, diag.data(), res, blocks, res_tail, jrw, jwr_perf, jww_perf_bhp,
+                  base_rs);
   for (int w = 0; w < n_wells; ++w) {
     const double* c = ctrl + 8 * w;
     const rf::WellControlH k{int(c[0]), int(c[1]), int(c[2]), int(c[3]), int(c[4]), c[5], c[6], c[7]};
     rf::well_row3(f, w, k, well_ptr, well_perfs, perf_cell, reg, p.data(), sw.data(), hc.data(), bhp, q, res_tail,
-                  jwr_ctrl, jww_ctrl_q, jww_ctrl_bhp);
+                  jwr_ctrl, jww_ctrl_q, jww_ctrl_bhp, base_rs);
   }
   return RF_OK;
 }
@@ -68,25 +69,25 @@ int32_t rfh_assemble3(const RfDeck* deck, double dt, const double* tx, const dou
 // The cell flash and write-back of the device path (derive_cell3): out = (regime, so, sg, rs, bo, bg)
 // per cell; and the substep-start classification (classify_regime) of (p, sg, rs).
 int32_t rfh_derive3(const RfDeck* deck, int32_t n, const double* p, const double* sw, const double* hc,
-                    const int32_t* reg, double* out) {
+                    const int32_t* reg, const double* base_rs, double* out) {
   rf::Fluid f;
   std::vector<double> pvt;
   std::string err;
   if (rf::fluid_from_deck(deck, f, pvt, err) != RF_OK) return RF_ERR_UNSUPPORTED;
   for (int i = 0; i < n; ++i) {
-    const rf::Derived3 d = rf::derive_cell3(f, p[i], sw[i], hc[i], reg[i]);
+    const rf::Derived3 d = rf::derive_cell3(f, p[i], sw[i], hc[i], reg[i], base_rs[i]);
     const double o[6] = {double(d.regime), d.so, d.sg, d.rs, d.bo, d.bg};
     for (int e = 0; e < 6; ++e) out[6 * i + e] = o[e];
   }
   return RF_OK;
 }
 int32_t rfh_classify3(const RfDeck* deck, int32_t n, const double* p, const double* sg, const double* rs,
-                      int32_t* reg) {
+                      const double* base_rs, int32_t* reg) {
   rf::Fluid f;
   std::vector<double> pvt;
   std::string err;
   if (rf::fluid_from_deck(deck, f, pvt, err) != RF_OK) return RF_ERR_UNSUPPORTED;
-  for (int i = 0; i < n; ++i) reg[i] = rf::classify_regime(f, p[i], sg[i], rs[i]);
+  for (int i = 0; i < n; ++i) reg[i] = rf::classify_regime(f, p[i], sg[i], rs[i], base_rs[i]);
   return RF_OK;
 }
 

@@ -98,6 +98,7 @@ def _wells(d, abi):
 
 
 def _device_rows(host, d, dt, prev, cur, reg, bhp, q, heads):
+    base = np.ascontiguousarray(d.rs, dtype=float)  # the DRSDT0 cap: the simulator's Rs
     abi, keep = d.to_abi()
     n = d.n_cells
     tx, ty, tz, pv, depth = _geometry(d, abi)
@@ -115,7 +116,7 @@ def _device_rows(host, d, dt, prev, cur, reg, bhp, q, heads):
                             _p(pinj, C.c_int32), _p(pwell, C.c_int32), _p(phas, C.c_int32), _p(pwi), _p(head),
                             _p(wptr, C.c_int32), _p(wperfs, C.c_int32), _p(ctrl), _p(np.ascontiguousarray(bhp)),
                             _p(np.ascontiguousarray(q)), _p(res), _p(blocks), _p(jrw), _p(jwr_perf),
-                            _p(jww_perf_bhp), _p(jwr_ctrl), _p(jww_ctrl_q), _p(jww_ctrl_bhp))
+                            _p(jww_perf_bhp), _p(jwr_ctrl), _p(jww_ctrl_q), _p(jww_ctrl_bhp), _p(base))
     assert rc == 0
     J = np.zeros((N, N))
     nx, ny, nz = d.nx, d.ny, d.nz
@@ -162,11 +163,24 @@ def _state(d, seed):
     return cur, prev, reg
 
 
-@pytest.mark.parametrize("pc_og, fluid, gravity", [(False, "water", True), (True, "gas", True),
-                                                   (True, "water", False)])
-def test_blackoil_rows_match_oracle_assembly(host, pc_og, fluid, gravity):
+def _drsdt0(d, seed):
+    """Gas redissolution off, with each cell's Rs (the cap) below the saturated Rs at its pressure
+    in many cells, so that the cap binds in the flash, the regimes and the properties."""
+    d.set_gas_redissolution_enabled(False)
+    table = PvtTable(d.pvt_rows, d.pvt_c_o)
+    rng = np.random.default_rng(seed)
+    d.rs = np.array([table.interpolate(float(p)).rs_m3m3 for p in d.pressure]) * rng.uniform(0.6, 1.0, d.n_cells)
+    return d
+
+
+@pytest.mark.parametrize("pc_og, fluid, gravity, drsdt0", [(False, "water", True, False), (True, "gas", True, False),
+                                                           (True, "water", False, False), (False, "water", True, True),
+                                                           (True, "gas", True, True)])
+def test_blackoil_rows_match_oracle_assembly(host, pc_og, fluid, gravity, drsdt0):
     d = decks.black_oil_3d(4, 3, 3, seed=3, dz=4.0, pc_og=pc_og, injected_fluid=fluid, rate_per_perf=8.0,
                            gravity=gravity)
+    if drsdt0:
+        d = _drsdt0(d, 21)
     cur, prev, reg = _state(d, seed=5)
     sim = OracleSimulator(d)
     nw, npf = sim.topology()
@@ -200,7 +214,8 @@ def test_blackoil_derive_and_classify_match_oracle(host):
     n = d.n_cells
     p, sw, hc = (np.ascontiguousarray(cur[:, k]) for k in range(3))
     out = np.zeros(6 * n)
-    assert host.rfh_derive3(C.byref(abi), n, _p(p), _p(sw), _p(hc), _p(reg, C.c_int32), _p(out)) == 0
+    base = np.ascontiguousarray(d.rs, dtype=float)
+    assert host.rfh_derive3(C.byref(abi), n, _p(p), _p(sw), _p(hc), _p(reg, C.c_int32), _p(base), _p(out)) == 0
     rows = np.asarray(d.pvt_rows, dtype=float)
     for i in range(n):
         o = blackoil_probe(rows, d.pvt_c_o, 6, [p[i], sw[i], hc[i], reg[i]])
@@ -209,7 +224,8 @@ def test_blackoil_derive_and_classify_match_oracle(host):
     rs = np.array([PvtTable(d.pvt_rows, d.pvt_c_o).interpolate(p[i]).rs_m3m3 * (0.9 if i % 2 else 1.0)
                    for i in range(n)])
     got = np.zeros(n, dtype=np.int32)
-    assert host.rfh_classify3(C.byref(abi), n, _p(p), _p(sg), _p(np.ascontiguousarray(rs)), _p(got, C.c_int32)) == 0
+    assert host.rfh_classify3(C.byref(abi), n, _p(p), _p(sg), _p(np.ascontiguousarray(rs)), _p(base),
+                              _p(got, C.c_int32)) == 0
     for i in range(n):
         o = blackoil_probe(rows, d.pvt_c_o, 4, [p[i], sw[i], sg[i], rs[i]])
         assert got[i] == int(o[0]), i
