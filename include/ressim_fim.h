@@ -198,6 +198,21 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
                             const int32_t* block_cols, const double* block_vals,
                             const double* rhs, double* x, RfLinearReport* out);
 
+/* Linear-solver seam replacing solve_linearized_system for the full Newton system with its well
+ * tail (src/lib/ressim/src/fim/linear/mod.rs:252-300, tail elimination well_schur.rs:70-471):
+ * a scalar CSR matrix (the reference's CsMat) of n_rows = 3 cells + wells + perforations rows in
+ * FimLinearBlockLayout order (cells, then one BHP per physical well, then one rate per
+ * perforation, in this context's well and perforation order).  Entries are accumulated into the
+ * device's Newton-system storage: a cell block outside the stencil-plus-well pattern, a tail entry
+ * that is not one of a well's couplings (a perforation row to its own cell, BHP and rate; a
+ * control row to its well's BHP, perforation rates and perforated cells; a cell row to the rates
+ * of its own perforations), or a perforation diagonal other than 1 (0 without a well index) is
+ * rejected with RF_ERR_INVALID, explicit zeros excepted.  Systems of at most 512 rows go to the
+ * dense direct LU first; otherwise the wells are eliminated, the reduced system is solved by
+ * CPR-FGMRES and the tail recovered, exactly as inside rf_step.  x receives n_rows values. */
+int32_t rf_linear_solve_csr(RfCtx* ctx, int32_t n_rows, const int32_t* row_ptr, const int32_t* cols,
+                            const double* vals, const double* rhs, double* x, RfLinearReport* out);
+
 /* Precision of the CPR-FGMRES linear solver.  RF_PRECISION_FP64 (default) computes everything in
  * FP64, as the reference does.  RF_PRECISION_MIXED keeps the block-ILU0 factors, the pressure
  * matrix, its ILU0 factors and the pressure BiCGStab vectors in FP32 (dot products accumulate in

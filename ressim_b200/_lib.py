@@ -34,6 +34,7 @@ def load():
     L.rf_rate_history_len.argtypes = [C.c_void_p]
     L.rf_rate_history_get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(_abi.RfTimePointRates)]
     L.rf_linear_solve_bsr.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp, _dp, _dp, C.POINTER(_abi.RfLinearReport)]
+    L.rf_linear_solve_csr.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp, _dp, _dp, C.POINTER(_abi.RfLinearReport)]
     L.rf_kernel_launches.argtypes = [C.c_void_p]
     L.rf_kernel_launches.restype = C.c_int64
     L.rf_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32]
@@ -63,7 +64,7 @@ def last_error(handle) -> str:
 
 EXPORTED_SYMBOLS = (
     "rf_create", "rf_destroy", "rf_last_error", "rf_set_state", "rf_get_state", "rf_get_well_bhp",
-    "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_kernel_launches",
+    "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_linear_solve_csr", "rf_kernel_launches",
     "rf_profile", "rf_set_linear_precision", "rf_set_cluster_size", "rf_batch_create", "rf_batch_destroy", "rf_batch_size",
     "rf_batch_context", "rf_batch_step", "rf_dense_solve_noalloc", "rf_set_controller_options", "rf_adjoint_record",
     "rf_backward", "rf_well_count",

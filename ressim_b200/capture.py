@@ -10,9 +10,10 @@ checks `validate_capture_data` in flow_lifecycle.rs:153-224).
   error messages, including the v3 companion checks.
 - `format_capture` / `write_capture` write byte-for-byte what the reference writes for the same
   system: numbers in Rust's shortest `{:e}` form, matrix rows in CSR order.
-- `replay` solves a captured tail-free system (reservoir cells only, three unknowns per cell)
-  through `rf_linear_solve_bsr` on a simulator of the deck it came from.  Systems with a well
-  tail are rejected: the device seam takes the cell block only and eliminates wells itself.
+- `replay` solves a captured system on a simulator of the deck it came from: a tail-free system
+  (reservoir cells only, three unknowns per cell) through `rf_linear_solve_bsr`, a system with a
+  well tail (one BHP per well, one rate per perforation) through `rf_linear_solve_csr`, which
+  eliminates the wells, solves and recovers the tail on the device as a Newton step does.
 """
 from __future__ import annotations
 
@@ -426,7 +427,8 @@ def to_bsr(s: CapturedSystem):
     if lay.well_bhp_count != 0 or j.rows != 3 * n or j.cols != 3 * n:
         raise CaptureError(
             f"replay takes tail-free systems of 3 x {n} rows; this one has {j.rows} rows and "
-            f"{lay.well_bhp_count} well BHP unknowns (the device seam eliminates wells itself)")
+            f"{lay.well_bhp_count} well BHP unknowns (systems with a well tail replay through "
+            f"rf_linear_solve_csr)")
     blocks = [dict() for _ in range(n)]
     for r in range(j.rows):
         for k in range(int(j.ptr[r]), int(j.ptr[r + 1])):
@@ -444,9 +446,24 @@ def to_bsr(s: CapturedSystem):
 
 
 def replay(sim, s: CapturedSystem):
-    """Solve a captured tail-free system with the device CPR-FGMRES (`rf_linear_solve_bsr`) on
-    `sim`, a ReservoirSimulator of the deck the capture came from.  Returns (x, report)."""
-    from .simulator import linear_solve_bsr
+    """Solve a captured system on the device, on `sim`, a ReservoirSimulator of the deck the
+    capture came from.  Tail-free systems go through `rf_linear_solve_bsr`; systems with a well
+    tail through `rf_linear_solve_csr`, whose unknowns must follow the layout's order (cells,
+    well BHPs from `perforation_tail_start - well_bhp_count`, perforation rates from
+    `perforation_tail_start`) with `sim`'s wells and perforations.  Returns (x, report)."""
+    from .simulator import linear_solve_bsr, linear_solve_csr
 
-    rp, cols, vals, rhs = to_bsr(s)
-    return linear_solve_bsr(sim, rp, cols, vals, rhs)
+    lay = s.layout
+    if lay is None or lay.cell_block_size != 3:
+        raise CaptureError("replay needs a block layout with 3 unknowns per cell")
+    j = s.jacobian
+    n = lay.cell_block_count
+    if lay.well_bhp_count == 0 and j.rows == 3 * n:
+        rp, cols, vals, rhs = to_bsr(s)
+        return linear_solve_bsr(sim, rp, cols, vals, rhs)
+    if j.rows != j.cols or lay.perforation_tail_start != 3 * n + lay.well_bhp_count:
+        raise CaptureError(
+            f"replay needs a square system whose perforation tail starts after the cells and the "
+            f"{lay.well_bhp_count} well BHP unknowns; this one is {j.rows} x {j.cols} with the "
+            f"tail at {lay.perforation_tail_start}")
+    return linear_solve_csr(sim, j.ptr, j.col, j.val, s.rhs)

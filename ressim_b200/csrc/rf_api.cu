@@ -1431,6 +1431,122 @@ int32_t rf_linear_solve_bsr(RfCtx* ctx, int32_t n_block_rows, const int32_t* blo
   });
 }
 
+int32_t rf_linear_solve_csr(RfCtx* ctx, int32_t n_rows, const int32_t* row_ptr, const int32_t* cols,
+                            const double* vals, const double* rhs, double* x, RfLinearReport* out) {
+  if (!ctx || !row_ptr || !cols || !vals || !rhs || !x) return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t {
+    rf::Ctx& c = ctx->c;
+    const rf::Topology& t = c.topo;
+    const int n = c.n, n3 = 3 * n, W = t.n_wells, P = t.n_perfs, pts = n3 + W;
+    if (n_rows != n3 + W + P) {
+      c.err = "the full-system seam takes 3 x cells + wells + perforations rows (" + std::to_string(n3 + W + P) +
+              " on this context), got " + std::to_string(n_rows);
+      return RF_ERR_INVALID;
+    }
+    if (row_ptr[0] != 0) {
+      c.err = "row_ptr[0] must be 0";
+      return RF_ERR_INVALID;
+    }
+    for (int r = 0; r < n_rows; ++r)
+      if (row_ptr[r + 1] < row_ptr[r]) {
+        c.err = "row_ptr is not non-decreasing at row " + std::to_string(r);
+        return RF_ERR_INVALID;
+      }
+    std::vector<int> cell_perf(n, -1);  // one completion per cell (checked at creation)
+    for (int k = 0; k < P; ++k) cell_perf[t.perf_cell[k]] = k;
+    std::vector<double> val(size_t(c.nnzb) * 9, 0.0), jrw(3 * size_t(P), 0.0), jwr_perf(3 * size_t(P), 0.0),
+        jwr_ctrl(3 * size_t(P), 0.0), jww_perf_bhp(P, 0.0), jww_ctrl_q(P, 0.0), jww_ctrl_bhp(W, 0.0), diag(P, 0.0),
+        res(n3), res_tail(size_t(W) + P);
+    for (int r = 0; r < n_rows; ++r)
+      for (int e = row_ptr[r]; e < row_ptr[r + 1]; ++e) {
+        const int j = cols[e];
+        const double v = vals[e];
+        if (j < 0 || j >= n_rows) {
+          c.err = "column " + std::to_string(j) + " of row " + std::to_string(r) + " is out of range";
+          return RF_ERR_INVALID;
+        }
+        double* slot = nullptr;
+        if (r < n3) {
+          const int i = r / 3;
+          if (j < n3) {
+            auto b = c.h_col.begin() + c.h_row_ptr[i], end = c.h_col.begin() + c.h_row_ptr[i + 1];
+            auto it = std::lower_bound(b, end, j / 3);
+            if (it != end && *it == j / 3) slot = &val[size_t(it - c.h_col.begin()) * 9 + 3 * (r % 3) + j % 3];
+          } else if (j >= pts && t.perf_cell[j - pts] == i) {
+            slot = &jrw[3 * size_t(j - pts) + r % 3];
+          }
+        } else if (r < pts) {
+          const int w = r - n3;
+          if (j < n3) {
+            const int k = cell_perf[j / 3];
+            if (k >= 0 && t.perf_well[k] == w) slot = &jwr_ctrl[3 * size_t(k) + j % 3];
+          } else if (j < pts) {
+            if (j - n3 == w) slot = &jww_ctrl_bhp[w];
+          } else if (t.perf_well[j - pts] == w) {
+            slot = &jww_ctrl_q[j - pts];
+          }
+        } else {
+          const int k = r - pts;
+          if (j < n3) {
+            if (j / 3 == t.perf_cell[k]) slot = &jwr_perf[3 * size_t(k) + j % 3];
+          } else if (j < pts) {
+            if (j - n3 == t.perf_well[k]) slot = &jww_perf_bhp[k];
+          } else if (j - pts == k) {
+            slot = &diag[k];
+          }
+        }
+        if (slot) {
+          *slot += v;
+        } else if (v != 0.0) {
+          c.err = "entry (" + std::to_string(r) + ", " + std::to_string(j) +
+                  ") lies outside the device's cell pattern and well couplings";
+          return RF_ERR_INVALID;
+        }
+      }
+    for (int k = 0; k < P; ++k) {
+      const double want = t.perf_has_wi[k] ? 1.0 : 0.0;
+      if (diag[k] != want) {
+        c.err = "perforation " + std::to_string(k) + " has diagonal " + std::to_string(diag[k]) +
+                "; the device's perforation rows have " + std::to_string(want);
+        return RF_ERR_INVALID;
+      }
+    }
+    // the step path's storage holds residuals: rhs = -residual
+    for (int r = 0; r < n3; ++r) res[r] = -rhs[r];
+    for (int r = n3; r < n_rows; ++r) res_tail[r - n3] = -rhs[r];
+    auto up = [&](double* dst, const std::vector<double>& src) {
+      if (!src.empty())
+        RF_CUDA(cudaMemcpyAsync(dst, src.data(), sizeof(double) * src.size(), cudaMemcpyHostToDevice, c.stream));
+    };
+    up(c.d_val.p, val);
+    up(c.d_res.p, res);
+    if (W > 0) {
+      up(c.d_res_tail.p, res_tail);
+      up(c.d_jrw.p, jrw);
+      up(c.d_jwr_perf.p, jwr_perf);
+      up(c.d_jwr_ctrl.p, jwr_ctrl);
+      up(c.d_jww_perf_bhp.p, jww_perf_bhp);
+      up(c.d_jww_ctrl_q.p, jww_ctrl_q);
+      up(c.d_jww_ctrl_bhp.p, jww_ctrl_bhp);
+    }
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<double> dx_tail;
+    const rf::LinResult r = rf::linear_solve_full(c, dx_tail);
+    RF_CUDA(cudaMemcpyAsync(x, c.d_x.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, c.stream));
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+    for (size_t k = 0; k < dx_tail.size() && n3 + k < size_t(n_rows); ++k) x[n3 + k] = dx_tail[k];
+    if (out) {
+      out->converged = r.converged && r.finite;
+      out->iterations = r.iterations;
+      out->rhs_norm = r.rhs_norm;
+      out->final_residual_norm = r.final_residual_norm;
+      out->used_fallback = r.used_fallback;
+      out->backend = r.backend;
+    }
+    return RF_OK;
+  });
+}
+
 int64_t rf_kernel_launches(const RfCtx* ctx) { return ctx ? ctx->c.launches : 0; }
 
 int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas) {

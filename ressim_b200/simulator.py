@@ -222,6 +222,28 @@ def linear_solve_bsr(sim: ReservoirSimulator, row_ptr, cols, vals, rhs):
     return x, rep
 
 
+def linear_solve_csr(sim: ReservoirSimulator, row_ptr, cols, vals, rhs):
+    """Linear-solver seam on the full Newton system with its well tail (scalar CSR, rows ordered
+    cells x 3, well BHPs, perforation rates): direct LU for at most 512 rows, else well
+    elimination, CPR-FGMRES and tail recovery on the device."""
+    h = sim._context()
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    cl = np.ascontiguousarray(cols, dtype=np.int32)
+    vl = np.ascontiguousarray(vals, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    n_rows = len(rp) - 1
+    if len(b) != n_rows:
+        raise ValueError(f"rhs has {len(b)} values for {n_rows} rows")
+    x = np.zeros(n_rows)
+    rep = _abi.RfLinearReport()
+    rc = _lib.load().rf_linear_solve_csr(h, n_rows, rp.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         cl.ctypes.data_as(C.POINTER(C.c_int32)), _ptr(vl), _ptr(b), _ptr(x),
+                                         C.byref(rep))
+    if rc != _abi.RF_OK:
+        raise DeviceError(f"rf_linear_solve_csr failed ({rc}): {_lib.last_error(h)}")
+    return x, rep
+
+
 def dense_solve_noalloc(n: int, a_ptr: int, b_ptr: int, x_ptr: int, stream: int = 0) -> None:
     """x = A^{-1} b through rf_dense_solve_noalloc, for callers that may not allocate device
     memory.  `a_ptr` (dense row-major n x n), `b_ptr` and `x_ptr` are device addresses of float64

@@ -216,6 +216,12 @@ def test_to_bsr_blocks_and_tail_rejection():
         cap.to_bsr(tail)
     with pytest.raises(cap.CaptureError, match="block layout"):
         cap.to_bsr(cap.CapturedSystem(0, "x", "water", 0, None, jac, s.rhs))
+    # replay routes tail systems to the full-system seam only when the tail follows the cells and
+    # the well BHP unknowns; these checks run before the device is touched
+    with pytest.raises(cap.CaptureError, match="perforation tail"):
+        cap.replay(None, tail)
+    with pytest.raises(cap.CaptureError, match="block layout"):
+        cap.replay(None, cap.CapturedSystem(0, "x", "water", 0, None, jac, s.rhs))
 
 
 def oracle_capture(dims=(10, 9, 3), seed=11):
