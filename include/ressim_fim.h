@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define RF_ABI_VERSION 3
+#define RF_ABI_VERSION 4
 
 /* status codes */
 #define RF_OK 0
@@ -109,6 +109,14 @@ typedef struct RfDeck {
   /* gas properties (setGasFluidProperties) and redissolution (setGasRedissolutionEnabled) */
   double mu_g, c_g, rho_g;
   int32_t gas_redissolution_enabled;
+  /* SWOF / SGOF tables (setThreePhaseScalTables, relperm.rs:43-122): rows of three doubles,
+   * (sw, krw, krow) and (sg, krg, krog), at least two each with strictly increasing saturations;
+   * when present they replace the three-phase Corey curves (relperm.rs:391-429) and need
+   * has_scal_3p.  The tables' capillary-pressure columns are not read by the FIM path. */
+  int32_t n_swof_rows;
+  const double* swof_rows;
+  int32_t n_sgof_rows;
+  const double* sgof_rows;
 } RfDeck;
 
 /* Per-report-step outcome (FimStepStats subset, src/lib/ressim/src/reporting.rs:191-243). */

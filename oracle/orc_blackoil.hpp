@@ -384,26 +384,67 @@ inline void pvt_oil_g(const PvtTable& t, const S& p, const S& rs, S& bo, S& mu) 
   mu = sat.mu_o;
 }
 
-// ---- three-phase relative permeability (relperm.rs:199-458), Corey without SWOF/SGOF tables ----
+// ---- three-phase relative permeability (relperm.rs:199-458): Corey, or the SWOF/SGOF tables ----
 struct Scal3 {
   double s_wc, s_or, n_w, n_o, krw_max, kro_max, s_gc, s_gr, s_org, n_g, krg_max;
+  // SWOF rows (sw, krw, krow) and SGOF rows (sg, krg, krog); empty: the Corey curves
+  std::vector<double> swof, sgof;
 };
 
+// interpolate_piecewise (relperm.rs:124-147) on column `y` of rows of three doubles (x first)
+inline double table_interp(const std::vector<double>& t, int y, double x) {
+  const int n = int(t.size() / 3);
+  if (n == 0) return 0.0;
+  if (x <= t[0]) return t[y];
+  for (int r = 0; r + 1 < n; ++r) {
+    const double x0 = t[3 * r], x1 = t[3 * r + 3];
+    if (x <= x1) {
+      if (std::fabs(x1 - x0) <= 2.220446049250313e-16) return t[3 * r + 3 + y];
+      const double f = rclamp((x - x0) / (x1 - x0), 0.0, 1.0);
+      return t[3 * r + y] + f * (t[3 * r + 3 + y] - t[3 * r + y]);
+    }
+  }
+  return t[3 * (n - 1) + y];
+}
+// interpolate_piecewise_generic (relperm.rs:9-40): the segment from the value, the derivative of
+// the active segment
+template <class S>
+inline S table_interp_g(const std::vector<double>& t, int y, const S& x) {
+  const int n = int(t.size() / 3);
+  if (n == 0) return sc<S>(0.0);
+  const double xv = val(x);
+  if (xv <= t[0]) return sc<S>(t[y]);
+  for (int r = 0; r + 1 < n; ++r) {
+    const double x0 = t[3 * r], x1 = t[3 * r + 3];
+    if (xv <= x1) {
+      if (std::fabs(x1 - x0) <= 2.220446049250313e-16) return sc<S>(t[3 * r + 3 + y]);
+      S f = min_ceil(max_floor((x - x0) / (x1 - x0), 0.0), 1.0);
+      const double y0 = t[3 * r + y], y1 = t[3 * r + 3 + y];
+      return f * (y1 - y0) + y0;
+    }
+  }
+  return sc<S>(t[3 * (n - 1) + y]);
+}
+
 inline double k_rw3(const Scal3& s, double sw) {
+  if (!s.swof.empty()) return table_interp(s.swof, 1, sw);
   const double e = rclamp((sw - s.s_wc) / (1.0 - s.s_wc - s.s_or), 0.0, 1.0);
   return s.krw_max * std::pow(e, s.n_w);
 }
 inline double k_rg3(const Scal3& s, double sg) {
+  if (!s.sgof.empty()) return table_interp(s.sgof, 1, sg);
   const double denom = 1.0 - s.s_wc - s.s_gc - s.s_gr;
   if (denom <= 0.0) return 0.0;
   const double e = rclamp((sg - s.s_gc) / denom, 0.0, 1.0);
   return s.krg_max * std::pow(e, s.n_g);
 }
 inline double k_ro_water3(const Scal3& s, double sw) {
+  if (!s.swof.empty()) return table_interp(s.swof, 2, sw);
   const double e = rclamp((1.0 - sw - s.s_or) / (1.0 - s.s_wc - s.s_or), 0.0, 1.0);
   return s.kro_max * std::pow(e, s.n_o);
 }
 inline double k_ro_gas3(const Scal3& s, double sg) {
+  if (!s.sgof.empty()) return table_interp(s.sgof, 2, sg);
   const double denom = 1.0 - s.s_wc - s.s_org;
   if (denom <= 0.0) return 0.0;
   const double e = rclamp((1.0 - s.s_wc - sg - s.s_org) / denom, 0.0, 1.0);
@@ -419,24 +460,28 @@ inline double k_ro_stone2(const Scal3& s, double sw, double sg) {
 
 template <class S>
 inline S k_rw3_g(const Scal3& s, const S& sw) {
+  if (!s.swof.empty()) return table_interp_g(s.swof, 1, sw);
   const double denom = 1.0 - s.s_wc - s.s_or;
   S e = min_ceil(max_floor((sw - s.s_wc) / denom, 0.0), 1.0);
   return s_powf(e, s.n_w) * s.krw_max;
 }
 template <class S>
 inline S k_rg3_g(const Scal3& s, const S& sg) {
+  if (!s.sgof.empty()) return table_interp_g(s.sgof, 1, sg);
   const double denom = 1.0 - s.s_wc - s.s_gc - s.s_gr;
   S e = min_ceil(max_floor((sg - s.s_gc) / denom, 0.0), 1.0);
   return s_powf(e, s.n_g) * s.krg_max;
 }
 template <class S>
 inline S k_ro_water3_g(const Scal3& s, const S& sw) {
+  if (!s.swof.empty()) return table_interp_g(s.swof, 2, sw);
   const double denom = 1.0 - s.s_wc - s.s_or;
   S e = min_ceil(max_floor((sc<S>(1.0 - s.s_or) - sw) / denom, 0.0), 1.0);
   return s_powf(e, s.n_o) * s.kro_max;
 }
 template <class S>
 inline S k_ro_gas3_g(const Scal3& s, const S& sg) {
+  if (!s.sgof.empty()) return table_interp_g(s.sgof, 2, sg);
   const double denom = 1.0 - s.s_wc - s.s_org;
   S e = min_ceil(max_floor((sc<S>(1.0 - s.s_wc - s.s_org) - sg) / denom, 0.0), 1.0);
   return s_powf(e, s.n_o) * s.kro_max;

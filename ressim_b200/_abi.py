@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-RF_ABI_VERSION = 3
+RF_ABI_VERSION = 4
 RF_BACKEND_FGMRES_CPR = 0
 RF_BACKEND_SPARSE_LU = 1
 
@@ -80,6 +80,8 @@ class RfDeck(C.Structure):
         ("pc_og_entry", C.c_double), ("pc_og_lambda", C.c_double),
         ("mu_g", C.c_double), ("c_g", C.c_double), ("rho_g", C.c_double),
         ("gas_redissolution_enabled", C.c_int32),
+        ("n_swof_rows", C.c_int32), ("swof_rows", C.POINTER(C.c_double)),
+        ("n_sgof_rows", C.c_int32), ("sgof_rows", C.POINTER(C.c_double)),
     ]
 
 

@@ -910,7 +910,10 @@ static int load(Ctx& c, const RfDeck* d) {
   c.kx.assign(d->perm_x, d->perm_x + n);
   c.ky.assign(d->perm_y, d->perm_y + n);
   c.kz.assign(d->perm_z, d->perm_z + n);
-  if (fluid_from_deck(d, c.fluid, c.h_pvt, c.err) != RF_OK) return RF_ERR_UNSUPPORTED;
+  {
+    const int rc = fluid_from_deck(d, c.fluid, c.h_pvt, c.err);
+    if (rc != RF_OK) return rc;
+  }
   c.hfluid = c.fluid;
   c.wells.assign(d->wells, d->wells + d->n_wells);
   c.inj_rate_ctl = d->injector_rate_controlled;

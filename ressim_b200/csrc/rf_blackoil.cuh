@@ -383,21 +383,56 @@ RF_HD void pvt_oil_g(const Fluid& f, const S& p, const S& rs, S& bo, S& mu) {
 // ---------------------------------------------------------------------------------------------
 // Three-phase relative permeability (Corey + Stone II) and gas-oil capillary pressure
 // ---------------------------------------------------------------------------------------------
+// interpolate_piecewise (relperm.rs:124-147) on column y of n rows of three doubles (x first)
+RF_HD double table3(const double* t, int n, int y, double x) {
+  if (x <= t[0]) return t[y];
+  for (int r = 0; r + 1 < n; ++r) {
+    const double x0 = t[3 * r], x1 = t[3 * r + 3];
+    if (x <= x1) {
+      if (fabs(x1 - x0) <= 2.220446049250313e-16) return t[3 * r + 3 + y];
+      const double fr = clamp01((x - x0) / (x1 - x0), 0.0, 1.0);
+      return t[3 * r + y] + fr * (t[3 * r + 3 + y] - t[3 * r + y]);
+    }
+  }
+  return t[3 * (n - 1) + y];
+}
+// interpolate_piecewise_generic (relperm.rs:9-40): segment from the value, derivative of the
+// active segment
+template <class S>
+RF_HD S table3_g(const double* t, int n, int y, const S& x) {
+  const double xv = value(x);
+  if (xv <= t[0]) return lift<S>(t[y]);
+  for (int r = 0; r + 1 < n; ++r) {
+    const double x0 = t[3 * r], x1 = t[3 * r + 3];
+    if (xv <= x1) {
+      if (fabs(x1 - x0) <= 2.220446049250313e-16) return lift<S>(t[3 * r + 3 + y]);
+      S fr = ceil_at(floor_at((x - x0) / (x1 - x0), 0.0), 1.0);
+      const double y0 = t[3 * r + y], y1 = t[3 * r + 3 + y];
+      return fr * (y1 - y0) + y0;
+    }
+  }
+  return lift<S>(t[3 * (n - 1) + y]);
+}
+
 RF_HD double k_rw3(const Fluid& s, double sw) {
+  if (s.n_swof) return table3(s.pvt + s.swof_off, s.n_swof, 1, sw);
   const double e = clamp01((sw - s.s3_wc) / (1.0 - s.s3_wc - s.s3_or), 0.0, 1.0);
   return s.s3_krw * pow(e, s.s3_nw);
 }
 RF_HD double k_rg3(const Fluid& s, double sg) {
+  if (s.n_sgof) return table3(s.pvt + s.sgof_off, s.n_sgof, 1, sg);
   const double denom = 1.0 - s.s3_wc - s.s3_gc - s.s3_gr;
   if (denom <= 0.0) return 0.0;
   const double e = clamp01((sg - s.s3_gc) / denom, 0.0, 1.0);
   return s.s3_krg * pow(e, s.s3_ng);
 }
 RF_HD double k_ro_water3(const Fluid& s, double sw) {
+  if (s.n_swof) return table3(s.pvt + s.swof_off, s.n_swof, 2, sw);
   const double e = clamp01((1.0 - sw - s.s3_or) / (1.0 - s.s3_wc - s.s3_or), 0.0, 1.0);
   return s.s3_kro * pow(e, s.s3_no);
 }
 RF_HD double k_ro_gas3(const Fluid& s, double sg) {
+  if (s.n_sgof) return table3(s.pvt + s.sgof_off, s.n_sgof, 2, sg);
   const double denom = 1.0 - s.s3_wc - s.s3_org;
   if (denom <= 0.0) return 0.0;
   const double e = clamp01((1.0 - s.s3_wc - sg - s.s3_org) / denom, 0.0, 1.0);
@@ -413,24 +448,28 @@ RF_HD double k_ro_stone2(const Fluid& s, double sw, double sg) {
 
 template <class S>
 RF_HD S k_rw3_g(const Fluid& s, const S& sw) {
+  if (s.n_swof) return table3_g(s.pvt + s.swof_off, s.n_swof, 1, sw);
   const double denom = 1.0 - s.s3_wc - s.s3_or;
   S e = ceil_at(floor_at((sw - s.s3_wc) / denom, 0.0), 1.0);
   return spow(e, s.s3_nw) * s.s3_krw;
 }
 template <class S>
 RF_HD S k_rg3_g(const Fluid& s, const S& sg) {
+  if (s.n_sgof) return table3_g(s.pvt + s.sgof_off, s.n_sgof, 1, sg);
   const double denom = 1.0 - s.s3_wc - s.s3_gc - s.s3_gr;
   S e = ceil_at(floor_at((sg - s.s3_gc) / denom, 0.0), 1.0);
   return spow(e, s.s3_ng) * s.s3_krg;
 }
 template <class S>
 RF_HD S k_ro_water3_g(const Fluid& s, const S& sw) {
+  if (s.n_swof) return table3_g(s.pvt + s.swof_off, s.n_swof, 2, sw);
   const double denom = 1.0 - s.s3_wc - s.s3_or;
   S e = ceil_at(floor_at((lift<S>(1.0 - s.s3_or) - sw) / denom, 0.0), 1.0);
   return spow(e, s.s3_no) * s.s3_kro;
 }
 template <class S>
 RF_HD S k_ro_gas3_g(const Fluid& s, const S& sg) {
+  if (s.n_sgof) return table3_g(s.pvt + s.sgof_off, s.n_sgof, 2, sg);
   const double denom = 1.0 - s.s3_wc - s.s3_org;
   S e = ceil_at(floor_at((lift<S>(1.0 - s.s3_wc - s.s3_org) - sg) / denom, 0.0), 1.0);
   return spow(e, s.s3_no) * s.s3_kro;

@@ -110,6 +110,36 @@ inline int fluid_from_deck(const RfDeck* d, Fluid& f, std::vector<double>& h_pvt
     for (const Branch& b : br)
       for (const auto& r : b.rows) h_pvt.insert(h_pvt.end(), r.begin(), r.end());
     f.pvt_c_o = d->pvt_c_o;
+    // SWOF / SGOF tables (relperm.rs:43-122), appended to the same flat array
+    if (d->n_swof_rows > 0 || d->n_sgof_rows > 0) {
+      if (!f.has_scal3 || d->n_swof_rows < 2 || d->n_sgof_rows < 2 || !d->swof_rows || !d->sgof_rows) {
+        err = "SWOF/SGOF tables need the three-phase relperm props and at least two rows each";
+        return RF_ERR_INVALID;
+      }
+      const double* tabs[2] = {d->swof_rows, d->sgof_rows};
+      const int counts[2] = {d->n_swof_rows, d->n_sgof_rows};
+      const char* names[2] = {"SWOF", "SGOF"};
+      int offs[2];
+      for (int t = 0; t < 2; ++t) {
+        double prev = -INFINITY;
+        for (int r = 0; r < counts[t]; ++r) {
+          const double* v = tabs[t] + 3 * size_t(r);
+          if (!(std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2])) || v[0] < 0.0 || v[0] > 1.0 ||
+              v[1] < 0.0 || v[1] > 1.0 || v[2] < 0.0 || v[2] > 1.0 || v[0] <= prev) {
+            err = std::string(names[t]) + " row " + std::to_string(r) +
+                  " must hold finite values within [0, 1] with strictly increasing saturation";
+            return RF_ERR_INVALID;
+          }
+          prev = v[0];
+        }
+        offs[t] = int(h_pvt.size());
+        h_pvt.insert(h_pvt.end(), tabs[t], tabs[t] + 3 * size_t(counts[t]));
+      }
+      f.swof_off = offs[0];
+      f.n_swof = counts[0];
+      f.sgof_off = offs[1];
+      f.n_sgof = counts[1];
+    }
     f.pvt = h_pvt.data();
   }
   return RF_OK;

@@ -229,6 +229,9 @@ struct Fluid {
   const double* pvt;
   int pvt_n_sat, pvt_n_br, pvt_hdr, pvt_rows;
   double pvt_c_o;
+  // SWOF rows (sw, krw, krow) at pvt + swof_off and SGOF rows (sg, krg, krog) at pvt + sgof_off
+  // in the same flat array; n_swof = 0: the three-phase Corey curves
+  int swof_off, n_swof, sgof_off, n_sgof;
 };
 
 // analytic Corey values (relperm.rs:491-520), used to sample the table knots on the host

@@ -96,6 +96,7 @@ class Deck:
     pvt_rows: list = None
     pvt_c_o: float = 0.0
     scal_3p: tuple = None
+    scal_tables: tuple = None  # (swof rows (sw, krw, krow), sgof rows (sg, krg, krog))
     pc_og: tuple = None
     mu_g: float = 0.02
     c_g: float = 1e-4
@@ -276,6 +277,36 @@ class Deck:
             raise ValueError(f"Corey exponents must be positive, got n_w={n_w}, n_o={n_o}, n_g={n_g}")
         self.scal_3p = tuple(float(v) for v in (s_wc, s_or, n_w, n_o, k_rw_max, k_ro_max, s_gc, s_gr, s_org, n_g,
                                                  k_rg_max))
+        self.scal_tables = None  # new Corey props drop the tables, as the reference's setter does
+
+    def set_three_phase_scal_tables(self, swof, sgof):
+        """setThreePhaseScalTables (frontend.rs:1145-1158, checks relperm.rs:65-122): SWOF rows
+        (sw, krw, krow[, pcow]) and SGOF rows (sg, krg, krog[, pcog]), as tuples or as dicts with
+        those keys; the capillary columns are accepted and not used by the FIM path."""
+
+        def rows(table, name, keys):
+            out = []
+            for r in table:
+                v = [r[k] for k in keys] if isinstance(r, dict) else list(r)[:3]
+                out.append([float(x) for x in v])
+            if len(out) < 2:
+                raise ValueError(f"{name} table must contain at least two rows")
+            prev = -math.inf
+            for i, (s, kr, kro) in enumerate(out):
+                if not (math.isfinite(s) and math.isfinite(kr) and math.isfinite(kro)):
+                    raise ValueError(f"{name} row {i} must contain finite values")
+                if not (0.0 <= s <= 1.0 and 0.0 <= kr <= 1.0 and 0.0 <= kro <= 1.0):
+                    raise ValueError(f"{name} row {i} must stay within [0, 1]")
+                if s <= prev:
+                    raise ValueError(f"{name} saturation must be strictly increasing at row {i}")
+                prev = s
+            return np.array(out, dtype=np.float64)
+
+        w = rows(swof, "SWOF", ("sw", "krw", "krow"))
+        g = rows(sgof, "SGOF", ("sg", "krg", "krog"))
+        if self.scal_3p is None:
+            raise ValueError("Three-phase relperm props must be configured before SWOF/SGOF tables")
+        self.scal_tables = (w, g)
 
     def set_gas_oil_capillary_params(self, p_entry, lam):
         if p_entry < 0.0:
@@ -464,4 +495,8 @@ class Deck:
             d.pc_og_entry, d.pc_og_lambda = self.pc_og
         d.mu_g, d.c_g, d.rho_g = self.mu_g, self.c_g, self.rho_g
         d.gas_redissolution_enabled = int(self.gas_redissolution_enabled)
+        if self.scal_tables is not None:
+            w, g = (np.ascontiguousarray(t, dtype=np.float64) for t in self.scal_tables)
+            d.n_swof_rows, d.swof_rows = len(w), arr(w, 3 * len(w))
+            d.n_sgof_rows, d.sgof_rows = len(g), arr(g, 3 * len(g))
         return d, keep

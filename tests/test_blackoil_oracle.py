@@ -246,3 +246,52 @@ def test_blackoil_drsdt0_gas_does_not_redissolve():
     pore_volume = float(np.sum(d.porosity) * 20.0 * 20.0 * 2.0)
     assert h["material_balance_error_m3"] < 1e-4 * pore_volume
     assert h["material_balance_error_oil_m3"] < 1e-4 * pore_volume
+
+
+# ---- SPE1 Case 1: the reference's own acceptance test against the published series ----
+def _spe1_run(sim, years, check):
+    """Report steps of at most 30 days to each year end (spe1_acceptance.rs:176-187), `check`
+    called at each."""
+    t = 0.0
+    for year in range(1, years + 1):
+        target = 365.0 * year
+        while t < target - 1e-9:
+            rc, rep = sim.step(min(30.0, target - t))
+            assert rc == 0 and rep.warning == 0, ("solver warning", t, rc, rep.warning)
+            t = rep.time_days
+        check(target, t, sim.rate_history()[-1])
+
+
+@pytest.mark.parametrize("years", [1, 10])
+def test_spe1_acceptance_against_published_series(years):
+    """spe1_first_year_matches_published_reference / spe1_full_horizon_matches_published_reference
+    (spe1_acceptance.rs:277-396): the oracle on the SPE1 deck (10x10x3, SWOF/SGOF tables, gas
+    injection, DRSDT0) holds the producer's surface-oil plateau through the first year and stays
+    within the reference test's bands of the published field pressure, oil rate and GOR at every
+    year end, with oil and gas material-balance drift within 1 %."""
+    from _spe1 import checkpoint_errors, fixture, in_place, material_balance_drift, spe1_deck
+
+    sc = fixture()["scalars"]
+    d = spe1_deck(10)
+    stoiip, giip = in_place(d)
+    sim = OracleSimulator(d)
+    worst = {"pressure": 0.0, "oil_rate": 0.0, "gor": 0.0}
+
+    def check(target, t, pt):
+        if target == 365.0:
+            plateau = abs(pt["total_production_oil"] - sc["TARGET_OIL_RATE_SC_DAY"]) / sc["TARGET_OIL_RATE_SC_DAY"]
+            assert plateau <= sc["PLATEAU_TOLERANCE"], plateau
+        e = checkpoint_errors(pt, target)
+        print(f"t={target:7.1f} pressure_err={100 * e['pressure']:.3f}% oil_rate_err={100 * e['oil_rate']:.3f}% "
+              f"gor_err={100 * e['gor']:.3f}%")
+        assert e["pressure"] <= sc["PRESSURE_TOLERANCE"], (target, e)
+        assert e["oil_rate"] <= sc["OIL_RATE_TOLERANCE"], (target, e)
+        assert e["gor"] <= sc["GOR_TOLERANCE"], (target, e)
+        for k in worst:
+            worst[k] = max(worst[k], e[k])
+        oil, gas = material_balance_drift(pt, t, stoiip, giip)
+        assert oil <= sc["OIL_MATERIAL_BALANCE_TOLERANCE"] and gas <= sc["GAS_MATERIAL_BALANCE_TOLERANCE"], (oil, gas)
+
+    _spe1_run(sim, years, check)
+    print("worst:", {k: f"{100 * v:.3f}%" for k, v in worst.items()})
+    sim.close()

@@ -173,14 +173,29 @@ def _drsdt0(d, seed):
     return d
 
 
-@pytest.mark.parametrize("pc_og, fluid, gravity, drsdt0", [(False, "water", True, False), (True, "gas", True, False),
-                                                           (True, "water", False, False), (False, "water", True, True),
-                                                           (True, "gas", True, True)])
-def test_blackoil_rows_match_oracle_assembly(host, pc_og, fluid, gravity, drsdt0):
+def _tables(d):
+    """SWOF/SGOF tables whose curves differ from the deck's Corey ones (exponents 2.5 / 1.8 and
+    1.7 / 2.2), with knots the test states land on both sides of."""
+    sw = np.array([0.1, 0.2, 0.3, 0.45, 0.6, 0.75, 0.9, 1.0])
+    swof = np.stack([sw, np.clip((sw - 0.1) / 0.8, 0, 1) ** 2.5, np.clip((0.9 - sw) / 0.8, 0, 1) ** 1.8], axis=1)
+    sg = np.array([0.0, 0.05, 0.15, 0.3, 0.5, 0.7, 0.85])
+    sgof = np.stack([sg, np.clip((sg - 0.05) / 0.8, 0, 1) ** 1.7, np.clip((0.75 - sg) / 0.75, 0, 1) ** 2.2], axis=1)
+    d.set_three_phase_scal_tables(swof, sgof)
+    return d
+
+
+@pytest.mark.parametrize("pc_og, fluid, gravity, drsdt0, tables",
+                         [(False, "water", True, False, False), (True, "gas", True, False, False),
+                          (True, "water", False, False, False), (False, "water", True, True, False),
+                          (True, "gas", True, True, False), (False, "water", True, False, True),
+                          (True, "gas", True, True, True)])
+def test_blackoil_rows_match_oracle_assembly(host, pc_og, fluid, gravity, drsdt0, tables):
     d = decks.black_oil_3d(4, 3, 3, seed=3, dz=4.0, pc_og=pc_og, injected_fluid=fluid, rate_per_perf=8.0,
                            gravity=gravity)
     if drsdt0:
         d = _drsdt0(d, 21)
+    if tables:
+        d = _tables(d)
     cur, prev, reg = _state(d, seed=5)
     sim = OracleSimulator(d)
     nw, npf = sim.topology()
