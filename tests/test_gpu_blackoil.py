@@ -197,3 +197,35 @@ def test_spe1_on_device_matches_oracle_and_published_series():
             assert e[k] <= tol, (target, k, e[k], same_path)
     gpu.close()
     cpu.close()
+
+
+def test_gas_drive_on_device_matches_oracle_and_opm_flow():
+    """The reference's solution-gas-drive acceptance case (three_phase_acceptance.rs:209-290) on
+    the device: inside every band of the reference test at the eleven OPM Flow points, with the
+    fields within 1e-6 of the oracle at each."""
+    from _gas_drive import TOLERANCE_KEYS, checkpoint, fixture, gas_drive_deck, in_place
+
+    f = fixture()
+    deck = gas_drive_deck()
+    stoiip, giip = in_place(deck)
+    gpu = ReservoirSimulator.from_deck(deck)
+    cpu = OracleSimulator(deck)
+    t = 0.0
+    for row in f["opm_series"]:
+        while t < row[0] - 1e-9:
+            dt = min(f["max_dt_days"], row[0] - t)
+            rg = gpu.step(dt)
+            rc_, rc = cpu.step(dt)
+            assert rc_ == 0 and rg["warning"] == 0
+            assert abs(rg["newton_iterations"] - rc.newton_iterations) <= 1
+            t = rg["time_days"]
+        e = checkpoint(gpu.get_rate_history(), row[0], stoiip, giip)
+        fe = _fields_err(gpu.state(), cpu.state())
+        print(f"t={row[0]:6.1f} " + " ".join(f"{k} {100 * v:.3f}%" for k, v in e.items()) + "; vs oracle "
+              + ", ".join(f"{k} {v:.1e}" for k, v in fe.items()))
+        for k, v in e.items():
+            assert v <= f["scalars"][TOLERANCE_KEYS[k]], (row[0], k, v)
+        for k in FIELDS:
+            assert fe[k] <= RTOL, (row[0], k, fe[k])
+    gpu.close()
+    cpu.close()
