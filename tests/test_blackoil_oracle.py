@@ -336,3 +336,30 @@ def test_gas_drive_acceptance_against_opm_flow_and_the_reference_engine():
 
     _gas_drive_errors(sim, per_point)
     sim.close()
+
+
+def test_gas_drive_liberates_solution_gas_as_pressure_falls():
+    """three_phase_gas_drive_liberates_solution_gas_as_pressure_falls
+    (three_phase_acceptance.rs:335-377): at 50, 100, 200, 400 and 600 days the field pressure is
+    below the bubble point while the producing GOR and the mean gas saturation keep rising; the
+    mean Rs ends below its start and the free gas above."""
+    from _gas_drive import fixture, gas_drive_deck
+
+    f = fixture()
+    sim = OracleSimulator(gas_drive_deck())
+    st0 = sim.state()
+    rs0, sg0 = float(np.mean(st0["rs"])), float(np.mean(st0["sat_gas"]))
+    prev_gor, prev_sg, t = -np.inf, sg0, 0.0
+    for target in (50.0, 100.0, 200.0, 400.0, 600.0):
+        while t < target - 1e-9:
+            rc, rep = sim.step(min(f["max_dt_days"], target - t))
+            assert rc == 0 and rep.warning == 0
+            t = rep.time_days
+        pt = sim.rate_history()[-1]
+        assert pt["avg_reservoir_pressure"] < f["scalars"]["GAS_DRIVE_BUBBLE_POINT_BAR"], (target, pt)
+        assert pt["producing_gor"] > prev_gor, (target, prev_gor, pt["producing_gor"])
+        assert pt["avg_gas_saturation"] > prev_sg, (target, prev_sg, pt["avg_gas_saturation"])
+        prev_gor, prev_sg = pt["producing_gor"], pt["avg_gas_saturation"]
+    assert float(np.mean(sim.state()["rs"])) < rs0
+    assert prev_sg > sg0
+    sim.close()
