@@ -14,5 +14,5 @@ import os as _os
 _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 from .deck import Deck, Well  # noqa: F401
-from .simulator import ReservoirSimulator, linear_solve_bsr  # noqa: F401
+from .simulator import ReservoirSimulator, linear_solve_bsr, linear_solve_csr  # noqa: F401
 from .ensemble import Ensemble  # noqa: F401
