@@ -87,3 +87,37 @@ def test_deck_digest_is_seeded():
     b = decks.waterflood_3d(8, 8, 2, seed=4)
     c = decks.waterflood_3d(8, 8, 2, seed=5)
     assert decks.deck_digest(a) == decks.deck_digest(b) != decks.deck_digest(c)
+
+
+def test_scal_table_setter_checks_and_abi_fields():
+    """setThreePhaseScalTables (frontend.rs:1145-1158) with ThreePhaseScalTables::validate
+    (relperm.rs:65-122): at least two rows, finite values within [0, 1], strictly increasing
+    saturation, and the Corey props first; new Corey props drop the tables."""
+    import numpy as np
+    import pytest
+
+    from ressim_b200 import Deck
+
+    swof = [(0.1, 0.0, 1.0), (0.5, 0.2, 0.3), (0.9, 0.8, 0.0)]
+    sgof = [{"sg": 0.0, "krg": 0.0, "krog": 1.0, "pcog": 0.0}, {"sg": 0.8, "krg": 0.9, "krog": 0.0, "pcog": 0.0}]
+    d = Deck(3, 1, 1, 0.2)
+    with pytest.raises(ValueError, match="must be configured before SWOF/SGOF"):
+        d.set_three_phase_scal_tables(swof, sgof)
+    d.set_three_phase_rel_perm_props(0.1, 0.1, 0.05, 0.05, 0.15, 2.0, 2.0, 1.5, 1.0, 1.0, 1.0)
+    with pytest.raises(ValueError, match="SWOF table must contain at least two rows"):
+        d.set_three_phase_scal_tables(swof[:1], sgof)
+    with pytest.raises(ValueError, match="SWOF saturation must be strictly increasing at row 2"):
+        d.set_three_phase_scal_tables([swof[0], swof[1], swof[1]], sgof)
+    with pytest.raises(ValueError, match="SGOF row 1 must stay within"):
+        d.set_three_phase_scal_tables(swof, [sgof[0], {"sg": 0.8, "krg": 1.2, "krog": 0.0}])
+    with pytest.raises(ValueError, match="SWOF row 0 must contain finite values"):
+        d.set_three_phase_scal_tables([(0.1, float("nan"), 1.0), swof[1]], sgof)
+    d.set_three_phase_scal_tables(swof, sgof)
+    raw, keep = d.to_abi()
+    assert raw.n_swof_rows == 3 and raw.n_sgof_rows == 2
+    assert [raw.swof_rows[i] for i in range(9)] == list(np.ravel(swof))
+    assert [raw.sgof_rows[i] for i in range(6)] == [0.0, 0.0, 1.0, 0.8, 0.9, 0.0]
+    d.set_three_phase_rel_perm_props(0.1, 0.1, 0.05, 0.05, 0.15, 2.0, 2.0, 1.5, 1.0, 1.0, 1.0)
+    assert d.scal_tables is None
+    raw, keep = d.to_abi()
+    assert raw.n_swof_rows == 0 and raw.n_sgof_rows == 0
