@@ -15,7 +15,9 @@ import numpy as np
 from ressim_b200 import _abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_SO = os.path.join(_HERE, "_build", "liborc_fim.so")
+# RESSIM_ORACLE_SO selects another build of the same sources (the CPU baseline's -march=native one)
+_SO = os.environ.get("RESSIM_ORACLE_SO") or os.path.join(_HERE, "_build", "liborc_fim.so")
+NATIVE_SO = os.path.join(_HERE, "_build", "liborc_fim_native.so")
 _lib = None
 
 _dp = C.POINTER(C.c_double)
@@ -24,6 +26,13 @@ _ip = C.POINTER(C.c_int32)
 
 def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def build_native() -> str | None:
+    """Builds the oracle with -O3 -march=native for the host that runs it (the timed CPU baseline)
+    and returns its path, or None when the build fails."""
+    r = subprocess.run(["make", "-s", "-B", "-C", _HERE, "native"], capture_output=True)
+    return NATIVE_SO if r.returncode == 0 and os.path.exists(NATIVE_SO) else None
 
 
 def lib():

@@ -7,7 +7,7 @@ src/lib/ressim/src/tests/three_phase_acceptance.rs grades the solution-gas-drive
 errors the reference's engine printed on that test.  This script reads both as text and stores
 those items unchanged as a fixture.
 
-    python tests/golden/make_gas_drive_fixture.py [reference root]
+    python tests/golden/make_gas_drive_fixture.py <reference root>
 """
 from __future__ import annotations
 
@@ -17,15 +17,14 @@ import re
 import sys
 
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from make_spe1_fixture import arg, split_top  # noqa: E402
+from make_spe1_fixture import arg, reference_root, split_top  # noqa: E402
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-SRC = os.path.join(ROOT, "src/lib/ressim/src/tests/three_phase_acceptance.rs")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "gas_drive_case.json")
 
 
 def main() -> None:
-    text = open(SRC).read()
+    root = reference_root()
+    text = open(os.path.join(root, "src/lib/ressim/src/tests/three_phase_acceptance.rs")).read()
     consts = {k: float(v.replace("_", "")) for k, v in re.findall(r"const (\w+): f64 = ([-\d._eE+]+);", text)}
     rows_body = re.search(r"fn gas_drive_pvt_rows\(\).*?const ROWS: \[.*?\] = \[(.*?)\];", text, re.S).group(1)
     pvt = [[float(v) for v in t.split(",")] for t in re.findall(r"\(([^()]*)\)", rows_body)]
@@ -44,7 +43,7 @@ def main() -> None:
     test = text[text.index("fn three_phase_gas_drive_matches_opm_flow_reference()"):]
     max_dt = float(re.search(r"step_to\(&mut sim, t_days, ([\d.]+)\)", test).group(1))
     # the errors the reference's own engine printed for this test (docs/THREE_PHASE_VALIDATION.md)
-    doc = open(os.path.join(ROOT, "docs/THREE_PHASE_VALIDATION.md")).read()
+    doc = open(os.path.join(root, "docs/THREE_PHASE_VALIDATION.md")).read()
     recorded = []
     for m in re.finditer(r"t=\s*([\d.]+) pressure_err=\s*([\d.]+)% oil_rate_err=\s*([\d.]+%|--) "
                          r"cum_oil_err=\s*([\d.]+)% gor_err=\s*([\d.]+)%", doc):

@@ -6,7 +6,7 @@ src/lib/ressim/src/tests/spe1_acceptance.rs (series, targets and tolerances) on 
 setter calls).  This script reads both files as text and stores what they hold, unchanged, as a
 fixture, so that the tests can replay the acceptance check without the reference's sources.
 
-    python tests/golden/make_spe1_fixture.py [reference root]
+    python tests/golden/make_spe1_fixture.py <reference root>
 """
 from __future__ import annotations
 
@@ -15,8 +15,6 @@ import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-SRC = os.path.join(ROOT, "src/lib/ressim/src")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "spe1_case.json")
 
 
@@ -68,8 +66,16 @@ def rows(text: str, kind: str, keys):
     return out
 
 
+def reference_root() -> str:
+    """The reference checkout's root, the script's one required argument."""
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.basename(sys.argv[0])} <reference root>")
+    return sys.argv[1]
+
+
 def main() -> None:
-    lib = open(os.path.join(SRC, "lib.rs")).read()
+    src = os.path.join(reference_root(), "src/lib/ressim/src")
+    lib = open(os.path.join(src, "lib.rs")).read()
     start = lib.index("fn make_spe1_like_grid_sim(")
     end = lib.index("fn make_spe1_like_sim(", start)
     helper = lib[start:end]
@@ -79,7 +85,7 @@ def main() -> None:
     calls = []
     for name, body in re.findall(r"\bsim\.(\w+)\((.*?)\)\s*(?:\.unwrap\(\))?;", helper, re.S):
         calls.append([name, [arg(t, consts) for t in split_top(body)]])
-    acc = open(os.path.join(SRC, "tests/spe1_acceptance.rs")).read()
+    acc = open(os.path.join(src, "tests/spe1_acceptance.rs")).read()
     series = {}
     for name, body in re.findall(r"const (REF_\w+): \[\(f64, f64\); \d+\] = \[(.*?)\];", acc, re.S):
         series[name] = [[float(a), float(b)] for a, b in re.findall(r"\(([-\d.]+),\s*([-\d.]+)\)", body)]
