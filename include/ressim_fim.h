@@ -236,6 +236,20 @@ int32_t rf_set_linear_precision(RfCtx* ctx, int32_t mode);
  * and differ between sizes only by rounding.  No counterpart in the reference. */
 int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas);
 
+/* Tuning: the kernels of the CPR's level-scheduled solves (the pressure BiCGStab with pressure
+ * ILU0, and the block-ILU0 sweep).  RF_PRESSURE_SOLVER_CLUSTER runs them on the thread-block
+ * cluster of rf_set_cluster_size; RF_PRESSURE_SOLVER_LEVEL runs each as one thread block with its
+ * vectors in level order and the sweeps' dependencies in shared memory (`threads` threads,
+ * 32..512 in steps of 32, 0 automatic); RF_PRESSURE_SOLVER_AUTO (default) takes the level-order
+ * kernels whenever their level window fits shared memory.  Both compute the same preconditioner;
+ * the solves differ only in the summation order of their dot products.  Takes effect at the next
+ * linear solve; RF_ERR_UNSUPPORTED when the level-order kernels cannot run this deck.  No
+ * counterpart in the reference. */
+#define RF_PRESSURE_SOLVER_AUTO 0
+#define RF_PRESSURE_SOLVER_CLUSTER 1
+#define RF_PRESSURE_SOLVER_LEVEL 2
+int32_t rf_set_pressure_solver(RfCtx* ctx, int32_t kind, int32_t threads);
+
 /* Number of kernel launches this context has issued since creation (device work counter). */
 int64_t rf_kernel_launches(const RfCtx* ctx);
 

@@ -40,6 +40,7 @@ def load():
     L.rf_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32]
     L.rf_set_linear_precision.argtypes = [C.c_void_p, C.c_int32]
     L.rf_set_cluster_size.argtypes = [C.c_void_p, C.c_int32]
+    L.rf_set_pressure_solver.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
     L.rf_batch_create.argtypes = [C.POINTER(C.POINTER(_abi.RfDeck)), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
     L.rf_batch_destroy.argtypes = [C.c_void_p]
     L.rf_batch_size.argtypes = [C.c_void_p]
@@ -67,7 +68,7 @@ EXPORTED_SYMBOLS = (
     "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_linear_solve_csr", "rf_kernel_launches",
     "rf_profile", "rf_set_linear_precision", "rf_set_cluster_size", "rf_batch_create", "rf_batch_destroy", "rf_batch_size",
     "rf_batch_context", "rf_batch_step", "rf_dense_solve_noalloc", "rf_set_controller_options", "rf_adjoint_record",
-    "rf_backward", "rf_well_count",
+    "rf_backward", "rf_well_count", "rf_set_pressure_solver",
 )
 
 PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",

@@ -1181,6 +1181,7 @@ static void free_ctx(Ctx& c) {
   for (auto* b : {&c.d_dir_a, &c.d_dir_lu, &c.d_dir_vec}) b->free();
   c.d_dir_perm.free();
   c.dir_rows = 0;
+  free_level_plan(c);
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
   if (c.levels.d_long_rows) cudaFree(c.levels.d_long_rows);
@@ -1556,6 +1557,27 @@ int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas) {
   if (!ctx || ctas < 0 || ctas > 16) return RF_ERR_INVALID;
   return guarded(ctx, [&]() -> int32_t {
     return rf::set_cluster_size(ctx->c, ctas == 0 ? rf::auto_cluster_size(ctx->c) : ctas);
+  });
+}
+
+int32_t rf_set_pressure_solver(RfCtx* ctx, int32_t kind, int32_t threads) {
+  if (!ctx || kind < RF_PRESSURE_SOLVER_AUTO || kind > RF_PRESSURE_SOLVER_LEVEL || threads < 0 || threads > 512)
+    return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t {
+    rf::Ctx& c = ctx->c;
+    if (kind == RF_PRESSURE_SOLVER_LEVEL && !c.lvl.built) {
+      c.err = "the level-order solver does not support this pattern (level too wide or too many far rows)";
+      return RF_ERR_UNSUPPORTED;
+    }
+    c.pressure_solver = kind;
+    c.level_threads = threads;
+    rf::level_plan_reshape(c);
+    if (kind == RF_PRESSURE_SOLVER_LEVEL && !c.lvl.fits[c.precision == 1 ? 1 : 0]) {
+      c.err = "the level-order pressure solver's window does not fit shared memory on this device";
+      c.pressure_solver = RF_PRESSURE_SOLVER_AUTO;
+      return RF_ERR_UNSUPPORTED;
+    }
+    return RF_OK;
   });
 }
 

@@ -53,6 +53,42 @@ struct DBuf {
   }
 };
 
+// Level-order plan of the single-CTA pressure BiCGStab and block-ILU0 sweep (rf_level.cu).
+// Positions number the rows level by level (rows ascending within a level); every vector of those
+// solves is stored in position order.  A sweep row reads the rows of the neighbouring level through
+// a shared-memory window of the previous level, and the rows a dependency reaches from further away
+// ("far" rows: the well fill) through a small shared-memory cache.  Per position, a 64-bit code word
+// holds up to three dependency codes (bit 15 set: far-cache slot, else offset in the neighbouring
+// level) and a meta field (bits 0-2 entry count, 7 = long row listed separately; bits 3-15 own far
+// slot + 1).
+struct LevelPlan {
+  int built = 0;          // structure present
+  int n_levels = 0, width = 0, nfar_f = 0, nfar_b = 0, n_flong = 0, n_blong = 0, nnz = 0;
+  DBuf<int> d_lstart, d_pos_row;
+  DBuf<unsigned long long> d_fcode, d_bcode;
+  DBuf<int> d_flong_ptr, d_blong_ptr;                  // long rows: entry ranges
+  DBuf<unsigned short> d_flong_code, d_blong_code;     // long rows: dependency codes
+  DBuf<int> d_sp_ptr, d_sp_col;                        // pressure matrix in position space
+  // gather maps of the value packing: packed value i = T(src[map[i]]) (0 when map[i] < 0)
+  //   factor map over plu: [fwd 3n | bwd 3n | fwd long | bwd long]; matrix map over pval: [nnz]
+  DBuf<int> d_fmap, d_smap;
+  DBuf<double> d_vals64;  // [fwd 3n | bwd 3n | fwd long | bwd long | piv n | spmv nnz]
+  DBuf<float> d_vals32;
+  DBuf<unsigned char> d_work;  // BiCGStab vectors in position order (9 x T) and x (double)
+  size_t work_bytes = 0;
+  // launch shape per value type (0 double, 1 float): threads, staging depth, dynamic shared memory
+  int threads[2] = {0, 0}, stages[2] = {0, 0};
+  size_t smem[2] = {0, 0};
+  int fits[2] = {0, 0};
+  int packed = -1;  // value type of the last packing (-1: none since the last factorisation)
+  // the block-ILU0 sweep in the same level order: CSR index of each position's first lower and
+  // first upper block, the forward result in position order, launch shape per value type
+  DBuf<int> d_blk_f0, d_blk_b0;
+  DBuf<unsigned char> d_blk_y;
+  int blk_threads[2] = {0, 0}, blk_fits[2] = {0, 0};
+  size_t blk_smem[2] = {0, 0};
+};
+
 struct Ctx {
   std::string err;
   cudaStream_t stream = nullptr;
@@ -164,6 +200,10 @@ struct Ctx {
   int precision = 0;
   DBuf<float> d_lu32, d_dinv32, d_plu32, d_pval32, d_pdiag32, d_pvec32, d_sweep32;
   DBuf<int> d_flag_dense;
+  // pressure-stage solver: 0 automatic, 1 the cluster kernels, 2 the single-CTA level-order kernels
+  int pressure_solver = 0;
+  int level_threads = 0;  // threads of the level-order kernels (0: automatic)
+  LevelPlan lvl;
 
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

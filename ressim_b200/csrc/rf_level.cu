@@ -1,0 +1,861 @@
+// rf_level.cu — the CPR's level-scheduled solves as ONE thread block working in level order:
+// the pressure stage's BiCGStab (solve_pressure_with_bicgstab, gmres_block_jacobi.rs:622-729) and
+// the block-ILU0 sweep (FimBlockIlu0Factors::apply, gmres_block_jacobi.rs:190-237).
+//
+// The ILU0 sweeps are chains of dependent levels (a natural-order 7-point grid has nx+ny+nz-2 of
+// them), so a sweep costs levels x (one dependent step).  The cluster kernels of rf_linear.cu pay
+// for each step a cross-SM signal plus a round of dependent global loads.  These kernels keep a
+// whole solve on one SM:
+//   - every vector of the solve is stored in position order (rows numbered level by level,
+//     ascending within a level), so a level's rows are contiguous in every array;
+//   - a row of level l reads its dependencies from a shared-memory window holding the values of
+//     the level processed just before (l-1 forward, l+1 backward); the few rows a dependency
+//     reaches from further away (the wells' fill) are kept in a shared-memory cache;
+//   - the pressure solve copies the per-row data of the levels ahead (factor values, dependency
+//     codes, pivots and the input vectors) into shared memory with cp.async, `stages - 1` levels
+//     ahead of use, so a level step is a block barrier, shared-memory reads and the row arithmetic;
+//   - the BiCGStab updates are fused into the sweeps that read them (the search direction p into
+//     the first forward sweep, s = r - alpha v and its norm into the second).
+// Every row is computed with the same operations in the same order as the natural-order
+// sequential sweep (entries in column order, pivot division as the reference does it), so the
+// preconditioner equals the reference's; only the dot products are summed in another order (a
+// fixed tree for a given thread count, hence deterministic).
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "rf_ops.hpp"
+
+namespace rf {
+
+namespace {
+
+constexpr double kEpsL = kF64Eps;
+constexpr int kLvlMaxThreads = 512;
+constexpr int kLvlMaxStages = 4;
+constexpr unsigned kFarBit = 0x8000u;
+constexpr unsigned kLongCnt = 7u;
+
+__device__ __forceinline__ unsigned smem_u32a(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async(void* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async(void* dst, const unsigned long long* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async(void* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// wait until at most `pending` of this thread's newest copy groups are still in flight
+__device__ __forceinline__ void cp_wait_dyn(int pending) {
+  switch (pending) {
+    case 0: cp_wait<0>(); break;
+    case 1: cp_wait<1>(); break;
+    case 2: cp_wait<2>(); break;
+    default: cp_wait<3>(); break;
+  }
+}
+
+template <class T>
+struct LvlArgs {
+  int n, L, width, stages;
+  const int* lstart;   // [L + 1] first position of each level
+  const int* pos_row;  // [n] natural row of each position
+  const unsigned long long* fcode;  // [n] forward (lower part) code words
+  const unsigned long long* bcode;  // [n] backward (upper part) code words
+  const int* flong_ptr;
+  const unsigned short* flong_code;
+  const int* blong_ptr;
+  const unsigned short* blong_code;
+  const int* sp_ptr;  // [n + 1] pressure matrix rows in position space
+  const int* sp_col;  // positions of the columns, in the rows' column order
+  const T* fval;      // [3][n] lower factor entries of short rows
+  const T* bval;      // [3][n] upper factor entries of short rows
+  const T* flong_val;
+  const T* blong_val;
+  const T* piv;    // [n] pressure ILU pivots
+  const T* spval;  // pressure matrix values in sp order
+  const double* rhs;  // natural order
+  double* x;          // natural order
+  double* xq;         // the iterate in position order
+  T* r;
+  T* rh;
+  T* p;
+  T* v;
+  T* s;
+  T* t;
+  T* y;
+  T* ph;
+  T* sh;
+  int max_iters;
+  long long* iter_counter;
+};
+
+// Sums of two per-thread values over the block with a fixed tree; every thread gets both totals.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* red) {
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
+    red[wid] = a;
+    red[32 + wid] = b;
+  }
+  __syncthreads();
+  if (t < 32) {
+    double ra = t < nw ? red[t] : 0.0, rb = t < nw ? red[32 + t] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ra += __shfl_down_sync(0xffffffffu, ra, o);
+      rb += __shfl_down_sync(0xffffffffu, rb, o);
+    }
+    if (t == 0) {
+      red[64] = ra;
+      red[65] = rb;
+    }
+  }
+  __syncthreads();
+  a = red[64];
+  b = red[65];
+}
+
+template <class T>
+__device__ __forceinline__ T dep_value(unsigned c, const T* nb, const T* far) {
+  return (c & kFarBit) ? far[c & 0x7fffu] : nb[c];
+}
+
+// One triangular sweep over all levels.  MODE 0: forward sweep of p = r + beta (p - omega v)
+// (p = r on the first iteration), p stored; MODE 1: forward sweep of s = r - alpha v, s stored and
+// its squares summed into acc; MODE 2: backward sweep of y.  The result goes to `out` (position
+// order).  Each thread handles the offsets t, t + NT, ... of every level and stages exactly those
+// offsets' data, so the staging needs no barrier of its own.
+template <class T, int MODE>
+__device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* win, T* far, T* out, double& acc,
+                          double beta, double omega, double alpha, bool first) {
+  constexpr bool FWD = MODE != 2;
+  const int t = threadIdx.x, NT = blockDim.x, L = a.L, W = a.width, D = a.stages, n = a.n;
+  const unsigned long long* codes = FWD ? a.fcode : a.bcode;
+  const T* vals = FWD ? a.fval : a.bval;
+  const int* lptr = FWD ? a.flong_ptr : a.blong_ptr;
+  const unsigned short* lcode = FWD ? a.flong_code : a.blong_code;
+  const T* lval = FWD ? a.flong_val : a.blong_val;
+  const T* in0 = MODE == 2 ? a.piv : a.r;
+  const T* in1 = MODE == 2 ? a.y : a.v;
+  const T* in2 = a.p;  // MODE 0 only
+  const size_t slot_bytes = size_t(W) * (8 + 6 * sizeof(T));
+  auto level_at = [&](int k) { return FWD ? k : L - 1 - k; };
+  auto issue = [&](int k) {
+    if (k >= L) return;
+    const int l = level_at(k), lst = a.lstart[l], w = a.lstart[l + 1] - lst;
+    unsigned char* base = stage + size_t(k % D) * slot_bytes;
+    unsigned long long* sc = reinterpret_cast<unsigned long long*>(base);
+    T* tp = reinterpret_cast<T*>(base + size_t(W) * 8);
+    for (int off = t; off < w; off += NT) {
+      const int q = lst + off;
+      cp_async(sc + off, codes + q);
+      cp_async(tp + off, vals + q);
+      cp_async(tp + W + off, vals + n + q);
+      cp_async(tp + 2 * W + off, vals + 2 * n + q);
+      cp_async(tp + 3 * W + off, in0 + q);
+      cp_async(tp + 4 * W + off, in1 + q);
+      if (MODE == 0) cp_async(tp + 5 * W + off, in2 + q);
+    }
+  };
+  if (D > 0)
+    for (int k = 0; k < D - 1; ++k) {
+      issue(k);
+      cp_commit();
+    }
+  for (int k = 0; k < L; ++k) {
+    const int l = level_at(k), lst = a.lstart[l], w = a.lstart[l + 1] - lst;
+    const unsigned long long* sc;
+    const T *v0, *v1, *v2, *i0, *i1, *i2;
+    if (D > 0) {
+      issue(k + D - 1);
+      cp_commit();
+      cp_wait_dyn(D - 1);
+      const unsigned char* base = stage + size_t(k % D) * slot_bytes;
+      sc = reinterpret_cast<const unsigned long long*>(base);
+      const T* tp = reinterpret_cast<const T*>(base + size_t(W) * 8);
+      v0 = tp;
+      v1 = tp + W;
+      v2 = tp + 2 * W;
+      i0 = tp + 3 * W;
+      i1 = tp + 4 * W;
+      i2 = tp + 5 * W;
+    } else {
+      sc = codes + lst;
+      v0 = vals + lst;
+      v1 = vals + n + lst;
+      v2 = vals + 2 * n + lst;
+      i0 = in0 + lst;
+      i1 = in1 + lst;
+      i2 = in2 + lst;
+    }
+    const T* nb = win + size_t((k + 1) & 1) * W;  // the level processed before this one
+    T* cur = win + size_t(k & 1) * W;
+    for (int off = t; off < w; off += NT) {
+      const int q = lst + off;
+      const unsigned long long code = sc[off];
+      const unsigned meta = unsigned(code >> 48);
+      const unsigned cnt = meta & 7u;
+      T s;
+      if (MODE == 0) {
+        const T rr = i0[off];
+        s = first ? rr : T(double(rr) + beta * (double(i2[off]) - omega * double(i1[off])));
+        a.p[q] = s;
+      } else if (MODE == 1) {
+        s = T(double(i0[off]) - alpha * double(i1[off]));
+        a.s[q] = s;
+        acc += double(s) * double(s);
+      } else {
+        s = i1[off];
+      }
+      if (cnt != kLongCnt) {
+        const unsigned c0 = unsigned(code) & 0xffffu, c1 = unsigned(code >> 16) & 0xffffu,
+                       c2 = unsigned(code >> 32) & 0xffffu;
+        T d0 = T(0), d1 = T(0), d2 = T(0);
+        if (cnt > 0u) d0 = dep_value(c0, nb, far);
+        if (cnt > 1u) d1 = dep_value(c1, nb, far);
+        if (cnt > 2u) d2 = dep_value(c2, nb, far);
+        if (cnt > 0u) s -= v0[off] * d0;
+        if (cnt > 1u) s -= v1[off] * d1;
+        if (cnt > 2u) s -= v2[off] * d2;
+      } else {
+        const int li = int(code & 0xffffu);
+        for (int e = lptr[li]; e < lptr[li + 1]; ++e) s -= lval[e] * dep_value(unsigned(lcode[e]), nb, far);
+      }
+      if (MODE == 2) {
+        const T d = i0[off];
+        s = fabs(double(d)) > kEpsL ? s / d : s;
+      }
+      cur[off] = s;
+      out[q] = s;
+      const unsigned fs = meta >> 3;
+      if (fs) far[fs - 1] = s;
+    }
+    __syncthreads();
+  }
+  if (D > 0) cp_wait<0>();
+}
+
+// out = A in (pressure matrix, position space), with the dot products the solve needs next:
+// MODE 0: acc0 += rh . out;  MODE 1: acc0 += out . out, acc1 += out . s
+template <class T, int MODE>
+__device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0, double& acc1) {
+  for (int q = threadIdx.x; q < a.n; q += blockDim.x) {
+    T s = T(0);
+    const int k1 = a.sp_ptr[q + 1];
+    for (int k = a.sp_ptr[q]; k < k1; ++k) s += a.spval[k] * in[a.sp_col[k]];
+    out[q] = s;
+    if (MODE == 0) {
+      acc0 += double(a.rh[q]) * double(s);
+    } else {
+      const double ti = double(s);
+      acc0 += ti * ti;
+      acc1 += ti * double(a.s[q]);
+    }
+  }
+}
+
+// The whole BiCGStab solve (at most max_iters iterations, tol = max(|rhs|, EPS) * 1e-6) in one
+// thread block.  Dot products accumulate in double and the iterate is kept in double for either
+// storage type T, as in the cluster kernels.
+template <class T>
+__device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem, double* red) {
+  const int W = a.width, n = a.n, t = threadIdx.x, NT = blockDim.x;
+  unsigned char* stage = lvl_smem;
+  T* win = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * W * (8 + 6 * sizeof(T)));
+  T* far = win + 2 * size_t(W);
+  double d0 = 0.0, d1 = 0.0;
+  for (int q = t; q < n; q += NT) {
+    const double ri = a.rhs[a.pos_row[q]] - 0.0;
+    const T rt = T(ri);
+    a.xq[q] = 0.0;
+    a.r[q] = rt;
+    a.rh[q] = rt;
+    a.v[q] = T(0);
+    a.p[q] = T(0);
+    d0 += double(rt) * double(rt);
+  }
+  block_sum2(d0, d1, red);
+  const double rnorm0 = sqrt(d0);
+  const double tol = fmax(rnorm0, kEpsL) * 1e-6;
+  const int max_iters = rnorm0 <= tol ? 0 : a.max_iters;
+  double rho = d0, rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  int started = 0;
+  for (int it = 0; it < max_iters; ++it) {
+    started = it + 1;
+    if (!isfinite(rho) || fabs(rho) < kEpsL) break;
+    const double beta = it == 0 ? 0.0 : (rho / rho_prev) * (alpha / omega);
+    d0 = 0.0;
+    d1 = 0.0;
+    lvl_sweep<T, 0>(a, stage, win, far, a.y, d0, beta, omega, 0.0, it == 0);
+    lvl_sweep<T, 2>(a, stage, win, far, a.ph, d0, 0.0, 0.0, 0.0, false);
+    lvl_spmv<T, 0>(a, a.ph, a.v, d0, d1);
+    block_sum2(d0, d1, red);
+    const double vd = d0;
+    if (!isfinite(vd) || fabs(vd) < kEpsL) break;
+    alpha = rho / vd;
+    d0 = 0.0;
+    d1 = 0.0;
+    lvl_sweep<T, 1>(a, stage, win, far, a.y, d0, 0.0, 0.0, alpha, false);
+    block_sum2(d0, d1, red);
+    if (sqrt(d0) <= tol) {
+      for (int q = t; q < n; q += NT) a.xq[q] += alpha * double(a.ph[q]);
+      break;
+    }
+    lvl_sweep<T, 2>(a, stage, win, far, a.sh, d0, 0.0, 0.0, 0.0, false);
+    d0 = 0.0;
+    d1 = 0.0;
+    lvl_spmv<T, 1>(a, a.sh, a.t, d0, d1);
+    block_sum2(d0, d1, red);
+    const double tt = d0;
+    if (!isfinite(tt) || tt <= kEpsL) break;
+    omega = d1 / tt;
+    if (!isfinite(omega) || fabs(omega) < kEpsL) break;
+    d0 = 0.0;
+    d1 = 0.0;
+    for (int q = t; q < n; q += NT) {
+      a.xq[q] += alpha * double(a.ph[q]) + omega * double(a.sh[q]);
+      const T ri = T(double(a.s[q]) - omega * double(a.t[q]));
+      a.r[q] = ri;
+      d0 += double(ri) * double(ri);
+      d1 += double(a.rh[q]) * double(ri);
+    }
+    block_sum2(d0, d1, red);
+    if (sqrt(d0) <= tol) break;
+    rho_prev = rho;
+    rho = d1;
+  }
+  __syncthreads();
+  for (int q = t; q < n; q += NT) a.x[a.pos_row[q]] = a.xq[q];
+  if (t == 0 && a.iter_counter) atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kLvlMaxThreads, 1) k_bicgstab_level(const __grid_constant__ LvlArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char lvl_smem[];
+  __shared__ double red[72];
+  bicgstab_level_body(a, lvl_smem, red);
+}
+
+// ============================================================================================
+// Block ILU0 sweep in level order
+// ============================================================================================
+// x = U^-1 L^-1 cr for the 3x3 block factors, one thread block.  The structure is the pressure
+// plan's (the same block pattern, levels, dependency codes and far rows); each row reads its factor
+// blocks straight from the CSR-ordered factors (the row's lower or upper blocks are contiguous) and
+// its dependencies, three values per row, from the shared-memory window of the neighbouring level
+// or the far cache.  Row arithmetic as block_fwd_row / block_bwd_row: same products and sums in
+// the same order.
+template <class T>
+struct BlkArgs {
+  int n, L, width;
+  const int* lstart;
+  const int* pos_row;
+  const int* f0;  // [n] CSR index of each position's first lower block
+  const int* b0;  // [n] CSR index of each position's first upper block
+  const unsigned long long* fcode;
+  const unsigned long long* bcode;
+  const int* flong_ptr;
+  const unsigned short* flong_code;
+  const int* blong_ptr;
+  const unsigned short* blong_code;
+  const T* lu;    // nnzb x 9
+  const T* dinv;  // n x 9
+  const double* cr;  // natural order, 3 per row
+  T* y;              // position order, 3 per row
+  double* x;         // natural order, 3 per row
+};
+
+template <class T>
+__device__ __forceinline__ const T* dep3(unsigned c, const T* nb, const T* far) {
+  return (c & kFarBit) ? far + 3 * (c & 0x7fffu) : nb + 3 * c;
+}
+
+template <class T>
+__device__ __forceinline__ void blk_sub(T& b0, T& b1, T& b2, const T* B, const T* v) {
+  const T v0 = v[0], v1 = v[1], v2 = v[2];
+  b0 -= B[0] * v0 + B[1] * v1 + B[2] * v2;
+  b1 -= B[3] * v0 + B[4] * v1 + B[5] * v2;
+  b2 -= B[6] * v0 + B[7] * v1 + B[8] * v2;
+}
+
+template <class T>
+__device__ void block_sweep_level_body(const BlkArgs<T>& a, unsigned char* blk_smem) {
+  const int W = a.width, L = a.L, t = threadIdx.x, NT = blockDim.x;
+  T* win = reinterpret_cast<T*>(blk_smem);  // [2][3 W]
+  T* far = win + 6 * size_t(W);
+  // forward: y = L^-1 cr
+  for (int l = 0; l < L; ++l) {
+    const int lst = a.lstart[l], w = a.lstart[l + 1] - lst;
+    const T* nb = win + 3 * size_t(W) * ((l + 1) & 1);
+    T* cur = win + 3 * size_t(W) * (l & 1);
+    for (int off = t; off < w; off += NT) {
+      const int q = lst + off, i = a.pos_row[q], k0 = a.f0[q];
+      const unsigned long long code = a.fcode[q];
+      const unsigned meta = unsigned(code >> 48), cnt = meta & 7u;
+      T b0 = T(a.cr[3 * size_t(i)]), b1 = T(a.cr[3 * size_t(i) + 1]), b2 = T(a.cr[3 * size_t(i) + 2]);
+      if (cnt != kLongCnt) {
+#pragma unroll
+        for (unsigned j = 0; j < 3; ++j)
+          if (j < cnt)
+            blk_sub(b0, b1, b2, a.lu + size_t(k0 + int(j)) * 9, dep3(unsigned(code >> (16 * j)) & 0xffffu, nb, far));
+      } else {
+        const int li = int(code & 0xffffu), e0 = a.flong_ptr[li], e1 = a.flong_ptr[li + 1];
+        for (int e = e0; e < e1; ++e)
+          blk_sub(b0, b1, b2, a.lu + size_t(k0 + e - e0) * 9, dep3(unsigned(a.flong_code[e]), nb, far));
+      }
+      cur[3 * off] = b0;
+      cur[3 * off + 1] = b1;
+      cur[3 * off + 2] = b2;
+      a.y[3 * size_t(q)] = b0;
+      a.y[3 * size_t(q) + 1] = b1;
+      a.y[3 * size_t(q) + 2] = b2;
+      const unsigned fs = meta >> 3;
+      if (fs) {
+        far[3 * (fs - 1)] = b0;
+        far[3 * (fs - 1) + 1] = b1;
+        far[3 * (fs - 1) + 2] = b2;
+      }
+    }
+    __syncthreads();
+  }
+  // backward: x = U^-1 y with the inverse diagonal blocks
+  for (int k = 0; k < L; ++k) {
+    const int l = L - 1 - k, lst = a.lstart[l], w = a.lstart[l + 1] - lst;
+    const T* nb = win + 3 * size_t(W) * ((k + 1) & 1);
+    T* cur = win + 3 * size_t(W) * (k & 1);
+    for (int off = t; off < w; off += NT) {
+      const int q = lst + off, i = a.pos_row[q], k0 = a.b0[q];
+      const unsigned long long code = a.bcode[q];
+      const unsigned meta = unsigned(code >> 48), cnt = meta & 7u;
+      T b0 = a.y[3 * size_t(q)], b1 = a.y[3 * size_t(q) + 1], b2 = a.y[3 * size_t(q) + 2];
+      if (cnt != kLongCnt) {
+#pragma unroll
+        for (unsigned j = 0; j < 3; ++j)
+          if (j < cnt)
+            blk_sub(b0, b1, b2, a.lu + size_t(k0 + int(j)) * 9, dep3(unsigned(code >> (16 * j)) & 0xffffu, nb, far));
+      } else {
+        const int li = int(code & 0xffffu), e0 = a.blong_ptr[li], e1 = a.blong_ptr[li + 1];
+        for (int e = e0; e < e1; ++e)
+          blk_sub(b0, b1, b2, a.lu + size_t(k0 + e - e0) * 9, dep3(unsigned(a.blong_code[e]), nb, far));
+      }
+      const T* D = a.dinv + 9 * size_t(i);
+      const T o0 = D[0] * b0 + D[1] * b1 + D[2] * b2;
+      const T o1 = D[3] * b0 + D[4] * b1 + D[5] * b2;
+      const T o2 = D[6] * b0 + D[7] * b1 + D[8] * b2;
+      cur[3 * off] = o0;
+      cur[3 * off + 1] = o1;
+      cur[3 * off + 2] = o2;
+      a.x[3 * size_t(i)] = double(o0);
+      a.x[3 * size_t(i) + 1] = double(o1);
+      a.x[3 * size_t(i) + 2] = double(o2);
+      const unsigned fs = meta >> 3;
+      if (fs) {
+        far[3 * (fs - 1)] = o0;
+        far[3 * (fs - 1) + 1] = o1;
+        far[3 * (fs - 1) + 2] = o2;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kLvlMaxThreads, 1) k_block_sweep_level(const __grid_constant__ BlkArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char blk_smem[];
+  block_sweep_level_body(a, blk_smem);
+}
+
+template <class T>
+size_t blk_smem_bytes(int W, int nfar) {
+  return (6 * size_t(W) + 3 * size_t(std::max(nfar, 1))) * sizeof(T);
+}
+
+// dst[i] = T(src[map[i]]), or 0 where map[i] < 0
+template <class T>
+__global__ void k_lvl_gather(long long m, const int* __restrict__ map, const double* __restrict__ src,
+                             T* __restrict__ dst) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += stride) {
+    const int k = map[i];
+    dst[i] = k >= 0 ? T(src[k]) : T(0);
+  }
+}
+
+template <class T>
+size_t lvl_smem_bytes(int W, int stages, int nfar) {
+  return size_t(stages) * W * (8 + 6 * sizeof(T)) + (2 * size_t(W) + size_t(std::max(nfar, 1))) * sizeof(T);
+}
+
+// offsets of the packed value segments (elements)
+struct LvlSeg {
+  size_t fval, bval, flong, blong, piv, sp, total;
+};
+LvlSeg lvl_segments(const LevelPlan& P, int n) {
+  LvlSeg s;
+  s.fval = 0;
+  s.bval = 3 * size_t(n);
+  s.flong = 6 * size_t(n);
+  s.blong = s.flong + size_t(P.n_flong);
+  s.piv = s.blong + size_t(P.n_blong);
+  s.sp = s.piv + size_t(n);
+  s.total = s.sp + size_t(P.nnz);
+  return s;
+}
+
+int auto_threads(const Ctx& c) {
+  const int nt = c.level_threads > 0 ? c.level_threads
+                                     : std::min(kLvlMaxThreads, std::max(64, (c.lvl.width + 31) / 32 * 32));
+  return std::max(32, std::min(kLvlMaxThreads, nt / 32 * 32));
+}
+
+template <class T>
+void choose_block_shape(Ctx& c, int f) {
+  LevelPlan& P = c.lvl;
+  int optin = 0;
+  RF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+  const size_t bytes = blk_smem_bytes<T>(P.width, std::max(P.nfar_f, P.nfar_b));
+  P.blk_fits[f] = 0;
+  if (bytes + 1024 > size_t(optin)) return;
+  P.blk_smem[f] = bytes;
+  P.blk_threads[f] = auto_threads(c);
+  raise_dynamic_smem((const void*)k_block_sweep_level<T>, bytes);
+  P.blk_fits[f] = 1;
+}
+
+template <class T>
+void choose_shape(Ctx& c, int f) {
+  LevelPlan& P = c.lvl;
+  int optin = 0;
+  RF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+  cudaFuncAttributes fa;
+  RF_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_bicgstab_level<T>));
+  const size_t budget = size_t(optin) > fa.sharedSizeBytes + 1024 ? size_t(optin) - fa.sharedSizeBytes - 1024 : 0;
+  const int nfar = std::max(P.nfar_f, P.nfar_b);
+  P.fits[f] = 0;
+  if (lvl_smem_bytes<T>(P.width, 0, nfar) > budget) return;
+  int st = kLvlMaxStages;
+  while (st > 0 && lvl_smem_bytes<T>(P.width, st, nfar) > budget) --st;
+  if (st == 1) st = 0;  // one stage only re-reads what it just copied: direct loads do the same
+  P.stages[f] = st;
+  P.smem[f] = lvl_smem_bytes<T>(P.width, st, nfar);
+  P.threads[f] = auto_threads(c);
+  raise_dynamic_smem((const void*)k_bicgstab_level<T>, P.smem[f]);
+  P.fits[f] = 1;
+}
+
+}  // namespace
+
+// Level-order structure of the current block pattern and level schedule (built once per topology).
+void build_level_plan(Ctx& c) {
+  LevelPlan& P = c.lvl;
+  P.built = 0;
+  const int n = c.n, L = c.levels.n_levels;
+  if (n <= 0 || L <= 0) return;
+  const std::vector<int>& lp = c.levels.h_ptr;
+  const std::vector<int>& rows = c.levels.h_rows;
+  std::vector<int> lvl(n), pos(n);
+  int W = 1;
+  for (int l = 0; l < L; ++l) {
+    W = std::max(W, lp[l + 1] - lp[l]);
+    for (int q = lp[l]; q < lp[l + 1]; ++q) {
+      lvl[rows[q]] = l;
+      pos[rows[q]] = q;
+    }
+  }
+  if (W >= int(kFarBit)) return;
+  // far-cache slots: rows a dependency reaches from further than the neighbouring level
+  std::vector<int> ffar(n, -1), bfar(n, -1);
+  int nff = 0, nfb = 0;
+  for (int r = 0; r < n; ++r) {
+    for (int k = c.h_row_ptr[r]; k < c.h_diag[r]; ++k) {
+      const int col = c.h_col[k];
+      if (lvl[col] != lvl[r] - 1 && ffar[col] < 0) ffar[col] = nff++;
+    }
+    for (int k = c.h_diag[r] + 1; k < c.h_row_ptr[r + 1]; ++k) {
+      const int col = c.h_col[k];
+      if (lvl[col] != lvl[r] + 1 && bfar[col] < 0) bfar[col] = nfb++;
+    }
+  }
+  if (nff >= 8191 || nfb >= 8191) return;
+  std::vector<unsigned long long> fcode(n), bcode(n);
+  std::vector<int> fmap(6 * size_t(n), -1), flong_ptr{0}, blong_ptr{0}, flong_map, blong_map;
+  std::vector<unsigned short> flong_code, blong_code;
+  auto pack_row = [&](bool fwd, int q, int r) {
+    const int l = lvl[r];
+    const int k0 = fwd ? c.h_row_ptr[r] : c.h_diag[r] + 1;
+    const int k1 = fwd ? c.h_diag[r] : c.h_row_ptr[r + 1];
+    const int cnt = k1 - k0;
+    auto code_of = [&](int col) -> unsigned {
+      const int lc = lvl[col];
+      if (lc == (fwd ? l - 1 : l + 1)) return unsigned(pos[col] - lp[lc]);
+      return kFarBit | unsigned(fwd ? ffar[col] : bfar[col]);
+    };
+    unsigned long long word = 0;
+    unsigned meta;
+    const size_t seg = fwd ? 0 : 3 * size_t(n);
+    if (cnt <= 3) {
+      for (int j = 0; j < cnt; ++j) {
+        word |= (unsigned long long)code_of(c.h_col[k0 + j]) << (16 * j);
+        fmap[seg + size_t(j) * n + q] = k0 + j;
+      }
+      meta = unsigned(cnt);
+    } else {
+      std::vector<int>& ptr = fwd ? flong_ptr : blong_ptr;
+      std::vector<int>& map = fwd ? flong_map : blong_map;
+      std::vector<unsigned short>& code = fwd ? flong_code : blong_code;
+      word = (unsigned long long)(ptr.size() - 1);
+      for (int k = k0; k < k1; ++k) {
+        code.push_back(static_cast<unsigned short>(code_of(c.h_col[k])));
+        map.push_back(k);
+      }
+      ptr.push_back(int(map.size()));
+      meta = kLongCnt;
+    }
+    meta |= unsigned((fwd ? ffar[r] : bfar[r]) + 1) << 3;
+    word |= (unsigned long long)meta << 48;
+    (fwd ? fcode : bcode)[q] = word;
+  };
+  for (int q = 0; q < n; ++q) {
+    pack_row(true, q, rows[q]);
+    pack_row(false, q, rows[q]);
+  }
+  if (flong_ptr.size() > 65536 || blong_ptr.size() > 65536) return;
+  P.n_levels = L;
+  P.width = W;
+  P.nfar_f = nff;
+  P.nfar_b = nfb;
+  P.n_flong = int(flong_map.size());
+  P.n_blong = int(blong_map.size());
+  P.nnz = c.h_row_ptr[n];
+  fmap.insert(fmap.end(), flong_map.begin(), flong_map.end());
+  fmap.insert(fmap.end(), blong_map.begin(), blong_map.end());
+  std::vector<int> sp_ptr(n + 1, 0), sp_col(P.nnz), smap(P.nnz), f0(n), b0(n);
+  for (int q = 0; q < n; ++q) {
+    const int r = rows[q];
+    int e = sp_ptr[q];
+    for (int k = c.h_row_ptr[r]; k < c.h_row_ptr[r + 1]; ++k, ++e) {
+      sp_col[e] = pos[c.h_col[k]];
+      smap[e] = k;
+    }
+    sp_ptr[q + 1] = e;
+    f0[q] = c.h_row_ptr[r];
+    b0[q] = c.h_diag[r] + 1;
+  }
+  auto up_i = [](DBuf<int>& b, const std::vector<int>& h) {
+    b.free();
+    b.alloc(h.size());
+    if (!h.empty()) RF_CUDA(cudaMemcpy(b.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  };
+  auto up_u64 = [](DBuf<unsigned long long>& b, const std::vector<unsigned long long>& h) {
+    b.free();
+    b.alloc(h.size());
+    RF_CUDA(cudaMemcpy(b.p, h.data(), sizeof(unsigned long long) * h.size(), cudaMemcpyHostToDevice));
+  };
+  auto up_u16 = [](DBuf<unsigned short>& b, const std::vector<unsigned short>& h) {
+    b.free();
+    b.alloc(h.size());
+    if (!h.empty()) RF_CUDA(cudaMemcpy(b.p, h.data(), sizeof(unsigned short) * h.size(), cudaMemcpyHostToDevice));
+  };
+  up_i(P.d_lstart, lp);
+  up_i(P.d_pos_row, rows);
+  up_u64(P.d_fcode, fcode);
+  up_u64(P.d_bcode, bcode);
+  up_i(P.d_flong_ptr, flong_ptr);
+  up_i(P.d_blong_ptr, blong_ptr);
+  up_u16(P.d_flong_code, flong_code);
+  up_u16(P.d_blong_code, blong_code);
+  up_i(P.d_sp_ptr, sp_ptr);
+  up_i(P.d_sp_col, sp_col);
+  up_i(P.d_fmap, fmap);
+  up_i(P.d_smap, smap);
+  up_i(P.d_blk_f0, f0);
+  up_i(P.d_blk_b0, b0);
+  P.d_vals64.free();
+  P.d_vals32.free();
+  P.d_work.free();
+  P.work_bytes = size_t(n) * (9 * sizeof(double) + sizeof(double));
+  P.d_work.alloc(P.work_bytes);
+  P.d_blk_y.free();
+  P.d_blk_y.alloc(3 * size_t(n) * sizeof(double));
+  P.packed = -1;
+  choose_shape<double>(c, 0);
+  choose_shape<float>(c, 1);
+  choose_block_shape<double>(c, 0);
+  choose_block_shape<float>(c, 1);
+  P.built = 1;
+}
+
+void free_level_plan(Ctx& c) {
+  LevelPlan& P = c.lvl;
+  for (auto* b : {&P.d_lstart, &P.d_pos_row, &P.d_flong_ptr, &P.d_blong_ptr, &P.d_sp_ptr, &P.d_sp_col, &P.d_fmap,
+                  &P.d_smap, &P.d_blk_f0, &P.d_blk_b0})
+    b->free();
+  P.d_fcode.free();
+  P.d_bcode.free();
+  P.d_flong_code.free();
+  P.d_blong_code.free();
+  P.d_vals64.free();
+  P.d_vals32.free();
+  P.d_work.free();
+  P.d_blk_y.free();
+  P.built = 0;
+}
+
+// Re-derive the launch shapes (thread count changed).
+void level_plan_reshape(Ctx& c) {
+  if (!c.lvl.built) return;
+  choose_shape<double>(c, 0);
+  choose_shape<float>(c, 1);
+  choose_block_shape<double>(c, 0);
+  choose_block_shape<float>(c, 1);
+}
+
+bool level_solver_active(const Ctx& c) {
+  const int f = c.precision == 1 ? 1 : 0;
+  if (!c.lvl.built || !c.lvl.fits[f]) return false;
+  return c.pressure_solver == 2 || c.pressure_solver == 0;
+}
+
+bool level_block_sweep_active(const Ctx& c) {
+  const int f = c.precision == 1 ? 1 : 0;
+  return c.lvl.built && c.lvl.blk_fits[f] && (c.pressure_solver == 2 || c.pressure_solver == 0);
+}
+
+void level_pack(Ctx& c) {
+  LevelPlan& P = c.lvl;
+  const int n = c.n;
+  const LvlSeg g = lvl_segments(P, n);
+  const long long mf = (long long)g.piv;  // factor entries: fval, bval, long rows
+  if (c.precision == 1) {
+    if (!P.d_vals32.p) P.d_vals32.alloc(g.total);
+    float* v = P.d_vals32.p;
+    k_lvl_gather<float><<<blocks_for(mf), kBlock, 0, c.stream>>>(mf, P.d_fmap.p, c.d_plu.p, v);
+    k_lvl_gather<float><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_pos_row.p, c.d_pdiag.p, v + g.piv);
+    k_lvl_gather<float><<<blocks_for(P.nnz), kBlock, 0, c.stream>>>(P.nnz, P.d_smap.p, c.d_pval.p, v + g.sp);
+    P.packed = 1;
+  } else {
+    if (!P.d_vals64.p) P.d_vals64.alloc(g.total);
+    double* v = P.d_vals64.p;
+    k_lvl_gather<double><<<blocks_for(mf), kBlock, 0, c.stream>>>(mf, P.d_fmap.p, c.d_plu.p, v);
+    k_lvl_gather<double><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_pos_row.p, c.d_pdiag.p, v + g.piv);
+    k_lvl_gather<double><<<blocks_for(P.nnz), kBlock, 0, c.stream>>>(P.nnz, P.d_smap.p, c.d_pval.p, v + g.sp);
+    P.packed = 0;
+  }
+  c.launches += 3;
+}
+
+template <class T>
+static void launch_level(Ctx& c, const double* rhs, double* x) {
+  LevelPlan& P = c.lvl;
+  const int f = sizeof(T) == 4 ? 1 : 0;
+  if (P.packed != f) throw CudaError("level-order pressure solve: factors not packed for this precision");
+  const int n = c.n;
+  const LvlSeg g = lvl_segments(P, n);
+  const T* vals;
+  if constexpr (sizeof(T) == 4)
+    vals = P.d_vals32.p;
+  else
+    vals = P.d_vals64.p;
+  LvlArgs<T> a;
+  a.n = n;
+  a.L = P.n_levels;
+  a.width = P.width;
+  a.stages = P.stages[f];
+  a.lstart = P.d_lstart.p;
+  a.pos_row = P.d_pos_row.p;
+  a.fcode = P.d_fcode.p;
+  a.bcode = P.d_bcode.p;
+  a.flong_ptr = P.d_flong_ptr.p;
+  a.flong_code = P.d_flong_code.p;
+  a.blong_ptr = P.d_blong_ptr.p;
+  a.blong_code = P.d_blong_code.p;
+  a.sp_ptr = P.d_sp_ptr.p;
+  a.sp_col = P.d_sp_col.p;
+  a.fval = vals + g.fval;
+  a.bval = vals + g.bval;
+  a.flong_val = vals + g.flong;
+  a.blong_val = vals + g.blong;
+  a.piv = vals + g.piv;
+  a.spval = vals + g.sp;
+  a.rhs = rhs;
+  a.x = x;
+  double* xq = reinterpret_cast<double*>(P.d_work.p);
+  T* vb = reinterpret_cast<T*>(P.d_work.p + sizeof(double) * size_t(n));
+  a.xq = xq;
+  a.r = vb;
+  a.rh = vb + size_t(n);
+  a.p = vb + 2 * size_t(n);
+  a.v = vb + 3 * size_t(n);
+  a.s = vb + 4 * size_t(n);
+  a.t = vb + 5 * size_t(n);
+  a.y = vb + 6 * size_t(n);
+  a.ph = vb + 7 * size_t(n);
+  a.sh = vb + 8 * size_t(n);
+  a.max_iters = 50;
+  a.iter_counter = c.d_bicg_iters;
+  c.launches++;
+  k_bicgstab_level<T><<<1, P.threads[f], P.smem[f], c.stream>>>(a);
+  RF_CUDA(cudaGetLastError());
+}
+
+void launch_bicgstab_level(Ctx& c, const double* rhs, double* x) {
+  if (c.precision == 1)
+    launch_level<float>(c, rhs, x);
+  else
+    launch_level<double>(c, rhs, x);
+}
+
+// x = BlockILU(cr) with the level-order sweep kernel and the factors of the current precision.
+void launch_block_sweep_level(Ctx& c, const double* cr, double* x, const void* lu, const void* dinv) {
+  LevelPlan& P = c.lvl;
+  const int f = c.precision == 1 ? 1 : 0;
+  auto fill = [&](auto& a) {
+    a.n = c.n;
+    a.L = P.n_levels;
+    a.width = P.width;
+    a.lstart = P.d_lstart.p;
+    a.pos_row = P.d_pos_row.p;
+    a.f0 = P.d_blk_f0.p;
+    a.b0 = P.d_blk_b0.p;
+    a.fcode = P.d_fcode.p;
+    a.bcode = P.d_bcode.p;
+    a.flong_ptr = P.d_flong_ptr.p;
+    a.flong_code = P.d_flong_code.p;
+    a.blong_ptr = P.d_blong_ptr.p;
+    a.blong_code = P.d_blong_code.p;
+    a.cr = cr;
+    a.x = x;
+  };
+  c.launches++;
+  if (f == 1) {
+    BlkArgs<float> a;
+    fill(a);
+    a.lu = static_cast<const float*>(lu);
+    a.dinv = static_cast<const float*>(dinv);
+    a.y = reinterpret_cast<float*>(P.d_blk_y.p);
+    k_block_sweep_level<float><<<1, P.blk_threads[1], P.blk_smem[1], c.stream>>>(a);
+  } else {
+    BlkArgs<double> a;
+    fill(a);
+    a.lu = static_cast<const double*>(lu);
+    a.dinv = static_cast<const double*>(dinv);
+    a.y = reinterpret_cast<double*>(P.d_blk_y.p);
+    k_block_sweep_level<double><<<1, P.blk_threads[0], P.blk_smem[0], c.stream>>>(a);
+  }
+  RF_CUDA(cudaGetLastError());
+}
+
+}  // namespace rf

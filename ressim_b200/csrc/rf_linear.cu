@@ -1818,7 +1818,10 @@ static void cpr_build(Ctx& c) {
   double* pdiag = c.d_pdiag.p;
   void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
   cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
-  if (c.dsm_bytes[c.precision == 1 ? 1 : 0] != 0) {
+  c.lvl.packed = -1;
+  const bool level = level_solver_active(c);
+  if (level) level_pack(c);
+  if (!level && c.dsm_bytes[c.precision == 1 ? 1 : 0] != 0) {
     if (c.precision == 1)
       k_pack_sweeps<float><<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_own_rows.p, c.d_row_ptr.p, c.d_diag.p,
                                                                    c.d_fcnt.p, c.d_bcnt.p, c.d_plu.p, c.d_pdiag.p,
@@ -1914,6 +1917,10 @@ static bool launch_bicgstab_dsmem(Ctx& c, const T* pval, const T* plu, const T* 
 template <class T>
 static void launch_bicgstab(Ctx& c, const T* pval, const T* plu, const T* pdiag, const double* rhs, double* x,
                             T* base) {
+  if (level_solver_active(c)) {
+    launch_bicgstab_level(c, rhs, x);
+    return;
+  }
   if (launch_bicgstab_dsmem<T>(c, pval, plu, pdiag, rhs, x, base)) return;
   const size_t n = c.n;
   BicgArgs<T> a;
@@ -1975,7 +1982,12 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
   LevelSched L = level_sched(c);
   const double* crp = cr;
   double* xo = c.d_w.p;
-  if (c.precision == 1) {
+  if (level_block_sweep_active(c)) {
+    if (c.precision == 1)
+      launch_block_sweep_level(c, crp, xo, c.d_lu32.p, c.d_dinv32.p);
+    else
+      launch_block_sweep_level(c, crp, xo, c.d_lu.p, c.d_dinv.p);
+  } else if (c.precision == 1) {
     const float* lu = c.d_lu32.p;
     const float* dinv = c.d_dinv32.p;
     float* y32 = c.d_sweep32.p;
@@ -2341,7 +2353,7 @@ int auto_cluster_size(const Ctx& c) {
 // Dynamic shared memory limits are attributes of a kernel, shared by every context in the process:
 // only ever raise them, so a context created later with smaller needs cannot undercut an earlier
 // one's launches.
-static void raise_dynamic_smem(const void* fn, size_t bytes) {
+void raise_dynamic_smem(const void* fn, size_t bytes) {
   static std::mutex mu;
   std::lock_guard<std::mutex> lk(mu);
   cudaFuncAttributes fa;
@@ -2563,6 +2575,7 @@ void setup_linear_workspace(Ctx& c) {
   RF_CUDA(cudaMemset(c.d_bicg_iters, 0, sizeof(long long)));
   // the largest cluster (16 CTAs, non-portable; else 8) that every level-scheduled kernel can run
   set_cluster_size(c, auto_cluster_size(c));
+  build_level_plan(c);
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
   if (smem > 48 * 1024) raise_dynamic_smem((const void*)k_schur, smem);

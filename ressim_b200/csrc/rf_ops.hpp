@@ -76,5 +76,21 @@ void set_linear_precision(Ctx& c, int mode);
 // <= want (1..16); returns it.
 int set_cluster_size(Ctx& c, int want);
 int auto_cluster_size(const Ctx& c);
+// Raise a kernel's dynamic shared-memory limit (never lowers it: the limit is shared by every
+// context in the process).
+void raise_dynamic_smem(const void* fn, size_t bytes);
+
+// Single-CTA level-order kernels (rf_level.cu): structure of the current pattern (once per
+// topology), launch shapes after a thread-count change, whether they serve the pressure stage and
+// the block-ILU0 sweep at the current precision, packing of the pressure factors after each
+// factorisation, and the solves.
+void build_level_plan(Ctx& c);
+void free_level_plan(Ctx& c);
+void level_plan_reshape(Ctx& c);
+bool level_solver_active(const Ctx& c);
+bool level_block_sweep_active(const Ctx& c);
+void level_pack(Ctx& c);
+void launch_bicgstab_level(Ctx& c, const double* rhs, double* x);
+void launch_block_sweep_level(Ctx& c, const double* cr, double* x, const void* lu, const void* dinv);
 
 }  // namespace rf

@@ -165,6 +165,17 @@ class ReservoirSimulator(Deck):
             raise DeviceError(f"rf_set_cluster_size failed ({rc}): {_lib.last_error(self._context())}")
         return rc
 
+    def set_pressure_solver(self, kind: str = "auto", threads: int = 0) -> None:
+        """Kernels of the CPR's level-scheduled solves: "cluster" (the thread-block cluster
+        kernels), "level" (one thread block in level order, `threads` threads, 0 automatic) or
+        "auto"."""
+        codes = {"auto": 0, "cluster": 1, "level": 2}
+        if kind not in codes:
+            raise ValueError(f"pressure solver must be one of {sorted(codes)}")
+        rc = _lib.load().rf_set_pressure_solver(self._context(), codes[kind], int(threads))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_set_pressure_solver failed ({rc}): {_lib.last_error(self._context())}")
+
     def set_controller_options(self, one_substep_per_report_step: bool = False, cnv_tol: float = 0.0,
                                mb_tol: float = 0.0) -> None:
         """Controller options of the device path (no counterpart in the reference): take every
