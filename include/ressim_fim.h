@@ -2,10 +2,12 @@
  * ressim_fim.h — C ABI of the B200-native fully implicit (FIM) Newton step.
  *
  * This is the drop-in boundary under the simulator's step API.  Every entry point takes plain
- * pointers and sizes, returns an int32_t status (0 ok, >0 recoverable solver status, <0 usage or
- * device error) and never allocates on the caller's behalf.  A context owns one CUDA stream and
- * its device buffers; calls on one context must be serialised by the caller (the reference
- * simulator object is `&mut self`, single threaded).
+ * pointers and sizes and returns an int32_t status (0 ok, >0 recoverable solver status, <0 usage
+ * or device error).  rf_create and rf_batch_create allocate the context's device buffers (freed
+ * by rf_destroy / rf_batch_destroy); the other entry points work in those buffers and in the
+ * caller's memory.  A context owns one CUDA stream and its device buffers; calls on one context
+ * must be serialised by the caller (the reference simulator object is `&mut self`, single
+ * threaded).
  *
  * Units follow the reference (bar, m, day, mD, cP).  Cell order is natural:
  * idx = k*nx*ny + j*nx + i (src/lib/ressim/src/grid.rs:25-27).
@@ -291,18 +293,18 @@ int32_t rf_backward(RfCtx* ctx, const RfObjective* objective, double* value, dou
                     int32_t n_controls);
 int32_t rf_well_count(const RfCtx* ctx);
 
-/* ---- Dense pressure solve that allocates nothing.  No counterpart in the reference, where the
- * dense inverse of a pressure block of at most 299 rows runs inside the preconditioner
- * (gmres_block_jacobi.rs:903-917); this exposes that solve alone for callers that may not call
+/* ---- Dense pressure solve that allocates nothing.  No counterpart in the reference.  It is the
+ * dense coarse solve of the CPR pressure stage, offered alone for callers that may not call
  * cudaMalloc (a host that reserves its device memory up front for its own pool, an embedding
  * framework that owns the allocator, a loop that must not block on an allocation).
  * x = A^{-1} b, A dense row-major n x n; a, b and x are device memory owned by the caller; the
  * call runs on `stream` (a cudaStream_t, NULL for the default stream) and synchronises it before
- * returning.  n must lie in 1..RF_NOALLOC_MAX_ROWS, otherwise RF_ERR_INVALID; an exactly zero
- * pivot also returns RF_ERR_INVALID.  Its scratch is one fixed device array of about 1.4 MB that
- * every GPU loading the library keeps until exit.  The first call on a device looks up that
- * array's address, so make it before any stream capture.  Calls share the array: calls that
- * overlap on the GPU race.  On failure a message is written to err (may be NULL, err_len bytes). */
+ * returning, so it may not be called while that stream is being captured into a CUDA graph.
+ * n must lie in 1..RF_NOALLOC_MAX_ROWS, otherwise RF_ERR_INVALID.  An exactly zero pivot returns
+ * RF_ERR_INVALID ("singular") and leaves x unchanged.  Its scratch is one fixed device array of
+ * about 1.4 MB that every GPU loading the library keeps until exit; the first call on a device
+ * looks up that array's address.  Calls share the array: calls that overlap on the GPU race.  On
+ * failure a message is written to err (may be NULL, err_len bytes). */
 #define RF_NOALLOC_MAX_ROWS 299
 int32_t rf_dense_solve_noalloc(int32_t n, const double* a, const double* b, double* x, void* stream,
                                char* err, size_t err_len);

@@ -1622,9 +1622,12 @@ __global__ void k_prolong_t(int nb, const double* __restrict__ w, const double* 
   out[3 * i + 1] = w[3 * i + 1] * c;
   out[3 * i + 2] = w[3 * i + 2] * c;
 }
-__global__ void k_dense_matvec(int n, const double* __restrict__ a, const double* __restrict__ x, double* __restrict__ y) {
+// y = a x for a dense row-major n x n matrix.  When `ok` is given and holds 0 (the inverse that
+// produced `a` hit an exactly zero pivot), y is left untouched.
+__global__ void k_dense_matvec(int n, const double* __restrict__ a, const double* __restrict__ x, double* __restrict__ y,
+                               const int* __restrict__ ok) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
+  if (r >= n || (ok != nullptr && *ok == 0)) return;
   double s = 0.0;
   for (int c = 0; c < n; ++c) s += a[size_t(r) * n + c] * x[c];
   y[r] = s;
@@ -1959,7 +1962,7 @@ static void cpr_apply(Ctx& c, const double* v, double* z) {
     k_restrict<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_cpr_w.p, v, prhs);
   c.launches++;
   if (c.dense_ok) {
-    k_dense_matvec<<<blocks_for(n, 64), 64, 0, c.stream>>>(n, c.d_dense.p, prhs, corr);
+    k_dense_matvec<<<blocks_for(n, 64), 64, 0, c.stream>>>(n, c.d_dense.p, prhs, corr, nullptr);
     c.launches++;
   } else {
     PhaseScope pk(c, kPhBicgKernel);

@@ -5,7 +5,7 @@
 // allocator owns the GPU, or a time-critical loop that must not block, since cudaMalloc and
 // cudaFree can synchronise the device.  For them this file offers x = A^{-1} b for a dense
 // row-major n x n pressure matrix, n <= RF_NOALLOC_MAX_ROWS (299, the size up to which the
-// reference inverts the pressure block densely, gmres_block_jacobi.rs:903-917).  It runs the same
+// reference's CPR inverts its pressure block densely, gmres_block_jacobi.rs:903-917).  It runs the same
 // two kernels as a context's CPR coarse stage (k_dense_invert, LU with partial pivoting in
 // nalgebra's order, then k_dense_matvec), with all scratch (the LU work copy, the inverse, the row
 // permutation and a status word) in one file-scope static device array.  The caller passes A, b
@@ -14,10 +14,12 @@
 // The array is part of the loaded library, so every GPU that loads it keeps about 1.4 MB for it
 // until the process exits.  Host code may not pass the array's name to a kernel (on the host it is
 // only a stand-in symbol): the first call on each device, with that device current, looks up the
-// device address with cudaGetSymbolAddress and keeps it.  Make that first call before any stream
-// capture.  All calls share the one array and it keeps the previous call's contents: the status
-// word is cleared on every call, everything else is overwritten before it is read.  Calls that
-// overlap on the GPU (other host threads, or unordered streams) race on the array; serialise them.
+// device address with cudaGetSymbolAddress and keeps it.  Every call synchronises its stream and
+// reads a status word back into host memory, so no call may be made while its stream is being
+// captured into a CUDA graph.  All calls share the one array and it keeps the previous call's
+// contents: the status word is cleared on every call, everything else is overwritten before it is
+// read.  Calls that overlap on the GPU (other host threads, or unordered streams) race on the
+// array; serialise them.  When a pivot is exactly zero the call fails and leaves x as it was.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -28,7 +30,7 @@
 namespace rf {
 __global__ void __launch_bounds__(1024) k_dense_invert(int n, double* a, double* inv, int* perm, int* ok);
 __global__ void k_dense_matvec(int n, const double* __restrict__ a, const double* __restrict__ x,
-                               double* __restrict__ y);
+                               double* __restrict__ y, const int* __restrict__ ok);
 }  // namespace rf
 
 namespace {
@@ -88,7 +90,8 @@ extern "C" int32_t rf_dense_solve_noalloc(int32_t n, const double* a, const doub
       (e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess)
     return report(err, err_len, RF_ERR_CUDA, cudaGetErrorString(e));
   rf::k_dense_invert<<<1, 1024, 0, s>>>(n, lu, inv, perm, status);
-  rf::k_dense_matvec<<<(n + 63) / 64, 64, 0, s>>>(n, inv, b, x);
+  // the product skips its writes when the factorisation failed, so x keeps the caller's values
+  rf::k_dense_matvec<<<(n + 63) / 64, 64, 0, s>>>(n, inv, b, x, status);
   if ((e = cudaGetLastError()) != cudaSuccess) return report(err, err_len, RF_ERR_CUDA, cudaGetErrorString(e));
   int ok = 0;
   if ((e = cudaMemcpyAsync(&ok, status, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

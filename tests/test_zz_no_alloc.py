@@ -89,3 +89,25 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     torch.cuda.synchronize()
     with pytest.raises(DeviceError, match="299"):
         dense_solve_noalloc(n, a_d.data_ptr(), b_d.data_ptr(), x_d.data_ptr())
+
+
+def test_noalloc_singular_matrix_fails_cleanly_and_leaves_x_unchanged():
+    """A matrix with an all-zero first column has an exactly zero first pivot: the call reports
+    the singular matrix, x keeps the caller's values, and the next call on a good system is still
+    correct (the shared scratch carries nothing over)."""
+    n = 40
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((n, n)) + n * np.eye(n)
+    A[:, 0] = 0.0
+    a_d = torch.tensor(A, dtype=torch.float64, device="cuda")
+    b_d = torch.ones(n, dtype=torch.float64, device="cuda")
+    x_d = torch.full((n,), 7.5, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    with pytest.raises(DeviceError, match="singular"):
+        dense_solve_noalloc(n, a_d.data_ptr(), b_d.data_ptr(), x_d.data_ptr())
+    torch.cuda.synchronize()
+    assert np.all(x_d.cpu().numpy() == 7.5)
+    G = rng.standard_normal((n, n)) + n * np.eye(n)
+    rhs = rng.standard_normal(n)
+    x = _noalloc(G, rhs)
+    assert np.max(np.abs(G @ x - rhs)) <= 1e-10 * max(float(np.max(np.abs(rhs))), 1.0)
