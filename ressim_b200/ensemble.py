@@ -81,6 +81,32 @@ class Ensemble:
         d["nnzb"] = int(out[k + 2])
         return d
 
+    def set_controller_options(self, one_substep_per_report_step: bool = False, cnv_tol: float = 0.0,
+                               mb_tol: float = 0.0) -> None:
+        """rf_set_controller_options on every variant (see ReservoirSimulator.set_controller_options)."""
+        L = _lib.load()
+        for i, c in enumerate(self._ctx):
+            rc = L.rf_set_controller_options(c, int(bool(one_substep_per_report_step)), float(cnv_tol), float(mb_tol))
+            if rc != _abi.RF_OK:
+                raise DeviceError(f"rf_set_controller_options failed for variant {i}: {_lib.last_error(c)}")
+
+    def well_bhp(self, i: int) -> np.ndarray:
+        n = len(self.decks[i].wells)
+        out = np.zeros(n)
+        rc = _lib.load().rf_get_well_bhp(self._ctx[i], _ptr(out), n)
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_get_well_bhp failed for variant {i}: {_lib.last_error(self._ctx[i])}")
+        return out
+
+    def rate_history(self, i: int) -> list[dict]:
+        L = _lib.load()
+        out = []
+        for k in range(L.rf_rate_history_len(self._ctx[i])):
+            r = _abi.RfTimePointRates()
+            L.rf_rate_history_get(self._ctx[i], k, C.byref(r))
+            out.append(r.as_dict())
+        return out
+
     def close(self):
         if self._h is not None:
             _lib.load().rf_batch_destroy(self._h)
