@@ -20,18 +20,21 @@ Legs of the `--impl ours` run:
             `rf_batch_step`, which returns when every variant's stream has finished;
   e2e       the same metric through the public API with host buffers: every step uploads each
             state from pinned host memory (`rf_set_state`), steps, and reads it back
-            (`rf_get_state`), timed from before the uploads to after the read-backs.  Single deck:
-            the same K steps on a second simulator after the same warm-up; ensemble: the K steps
-            after the timed ones;
-  roofline  the pressure BiCGStab kernel (the dominant kernel): algorithmic bytes per iteration
-            x iterations / kernel time (CUDA events), against the measured HBM copy bandwidth;
-  cpu_baseline  the CPU restatement (C++, single thread, like the reference) on the same deck
-            (ensemble: variant 0) and the same report steps after the same warm-up, in a spawned
-            process beside the GPU legs.
+            (`rf_get_state`), timed from before the uploads to after the read-backs, on the same K
+            report steps as `value` (a second simulator or ensemble after the same warm-up);
+  roofline  the pressure BiCGStab kernel (the dominant kernel): algorithmic bytes of one launch /
+            that launch's duration (CUDA events on the launching stream, averaged over the
+            launches), against the measured HBM copy bandwidth;
+  cpu_baseline  the CPU restatement (C++, single thread, like the reference, built with
+            -march=native on this host) on the same deck (ensemble: variant 0) and the same report
+            steps after the same warm-up, in a spawned process beside the GPU legs;
+  matched_comparison  (ensemble) the batched mixed form over all variants against the plain FP64
+            path one variant at a time, both with Newton accepted at CNV 1e-9 / MB 1e-11, and the
+            field error between them.
 
 The reference arm (`--impl reference`) times the CPU restatement on the host cores: the single
 deck on one core (the reference is single-threaded), the ensemble as one single-threaded process
-per core over the first `cores` variants.
+per core, each on a variant of a sample spread over the size range, their throughputs summed.
 
 Multi-GPU (torchrun): a single deck does not shard, so each rank runs a replica; the ensemble
 shards by variant, every rank stepping its own `--variants` variants.  Both are weak scaling with
@@ -99,6 +102,8 @@ def parse():
     ap.add_argument("--tune-variants", type=int, default=0,
                     help="ensemble: first tune this many variants spread over the size range into --cluster-table")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-matched", action="store_true",
+                    help="ensemble: skip the matched-profile comparison (batched mixed vs plain FP64)")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="wall budget of the CPU baseline sample")
     return ap.parse_args()
 
@@ -235,6 +240,28 @@ def bicgstab_bytes_per_iteration(n_cells, nnzb):
     return 2 * (12 * nnzb + 64 * n_cells) + 2 * (12 * nnzb + 20 * n_cells) + 160 * n_cells
 
 
+def use_native_oracle():
+    """Builds the CPU oracle for this host (-O3 -march=native) and points the CPU legs, which run in
+    spawned processes started after this call, at that build.  Returns the compiler flags used."""
+    from oracle import oracle_py
+
+    so = oracle_py.build_native()
+    if so:
+        os.environ["RESSIM_ORACLE_SO"] = so
+        return "g++ -O3 -march=native -ffp-contract=off"
+    return "g++ -O3 -ffp-contract=off (the -march=native build failed on this host)"
+
+
+def spread_sample(sizes, k):
+    """k indices spread over the size order of `sizes` (smallest to largest, evenly), so a sample of
+    the ensemble has its size distribution."""
+    order = sorted(range(len(sizes)), key=lambda i: (sizes[i], i))
+    k = max(1, min(k, len(sizes)))
+    if k == 1:
+        return [order[len(order) // 2]]
+    return sorted({order[round(j * (len(order) - 1) / (k - 1))] for j in range(k)})
+
+
 def cpu_leg(workload, dt, warmup, steps, budget_s):
     """The CPU restatement of the reference FIM (C++, one thread, like the reference) on the same
     deck and the same report steps as the GPU legs: `warmup` untimed report steps from the initial
@@ -291,32 +318,39 @@ def _ref_variant_worker(index, dt, warmup, steps):
 
 def run_reference_ensemble(args):
     """Reference arm of the ensemble: the reference steps one deck per simulator, single-threaded,
-    so a multi-core host runs one variant per core.  One process per host core (spawned) steps the
-    first `cores` variants (a bounded sample of the ensemble: W untimed and K timed report steps
-    each); throughput = cells x K summed over the sample / the slowest worker's timed seconds."""
+    so a multi-core host runs one variant per core.  One process per host core (spawned) steps one
+    variant of a sample spread over the ensemble's size range (a bounded sample: W untimed and K
+    timed report steps each).  Each core's throughput is its variant's cells x K / its own timed
+    seconds; the host's throughput is their sum (every core kept busy with variants like its
+    sample)."""
     import multiprocessing as mp
 
+    from ressim_b200 import decks
+
+    flags = use_native_oracle()
     cores = max(1, min(os.cpu_count() or 1, args.variants))
     dt = args.dt if args.dt is not None else WORKLOADS["ensemble"][3]
     k = max(1, args.steps)
-    with mp.get_context("spawn").Pool(cores) as pool:
-        res = pool.starmap(_ref_variant_worker, [(i, dt, args.warmup, k) for i in range(cores)])
+    sizes = [decks.ensemble_variant(i).n_cells for i in range(args.variants)]
+    sample = spread_sample(sizes, cores)
+    with mp.get_context("spawn").Pool(len(sample)) as pool:
+        res = pool.starmap(_ref_variant_worker, [(i, dt, args.warmup, k) for i in sample])
     cells = sum(r[0] for r in res)
-    slowest = max(r[1] for r in res)
     newton = sum(r[2] for r in res)
-    v = cells * k / slowest
+    v = sum(r[0] * k / r[1] for r in res)
     desc = WORKLOADS["ensemble"][4].format(nv=args.variants)
     line = {
         "metric": "FIM cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * slowest / k,
+        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * cells / v,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded deck generator)",
-        "config": {"workload": desc, "sample_variants": cores, "sample_cells": cells, "dt_days": dt,
+        "config": {"workload": desc, "sample_variants": sample, "sample_cells": cells, "dt_days": dt,
                    "newton_iterations": newton},
-        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"variants 0..{cores - 1} ({cells} cells), one single-threaded process per "
-                                   f"core, report steps {args.warmup}..{args.warmup + k - 1} after {args.warmup} "
-                                   f"untimed ones; C++ restatement of the reference FIM"},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": len(sample), "kind": "port",
+                         "sample": f"{len(sample)} variants spread over the size range ({cells} cells), one "
+                                   f"single-threaded process per core, report steps {args.warmup}.."
+                                   f"{args.warmup + k - 1} after {args.warmup} untimed ones; throughput summed "
+                                   f"over the cores; C++ restatement of the reference FIM, {flags}"},
         "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -339,7 +373,11 @@ def run_reference(args):
         return 0
     _, dt_default, desc = make_deck(args.workload)
     dt = args.dt if args.dt is not None else dt_default
-    v, k, el, newton, _ = cpu_leg(args.workload, dt, args.warmup, args.steps, float("inf"))
+    flags = use_native_oracle()
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(1) as pool:
+        v, k, el, newton, _ = pool.apply(cpu_leg, (args.workload, dt, args.warmup, args.steps, float("inf")))
     n = make_deck(args.workload)[0].n_cells
     if args.workload == "ensemble":
         desc = desc.format(nv=args.variants) + "; the reference steps one deck per simulator, so its arm times " \
@@ -352,20 +390,105 @@ def run_reference(args):
         "config": {"workload": desc, "cells": n, "dt_days": dt, "newton_iterations": newton},
         "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                          "sample": f"report steps {args.warmup}..{args.warmup + k - 1} of the deck "
-                                   f"({newton} Newton iterations), C++ restatement of the reference FIM, 1 thread"},
+                                   f"({newton} Newton iterations), C++ restatement of the reference FIM, 1 thread, "
+                                   f"{flags}"},
         "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+MATCHED_CNV, MATCHED_MB = 1e-9, 1e-11
+
+
+def ensemble_roofline(ds, profs, peak, peak_kind, batch=None):
+    """Roofline of the dominant kernel (the pressure BiCGStab): algorithmic bytes of one launch / its
+    duration (CUDA events on the launching stream), averaged over the launches (bytes and time
+    pooled, then divided by the launches).  With batched stepping one launch carries a whole
+    group's solves and `batch` holds those launches' count and time; otherwise every variant's own
+    launches are timed by its profile."""
+    from ressim_b200 import _lib
+
+    it = sum(p["bicgstab_iterations"] for p in profs)
+    byts = sum(bicgstab_bytes_per_iteration(d.n_cells, p["nnzb"]) * p["bicgstab_iterations"] for d, p in zip(ds, profs))
+    if batch is not None and batch.get("pressure_launches", 0) > 0 and batch.get("pressure_ms", 0) > 0:
+        nl, kms = batch["pressure_launches"], batch["pressure_ms"]
+        kernel = "k_bicgstab_level_batch (one launch = a group's pressure solves, one thread block each)"
+        solves = batch["pressure_items"]
+    else:
+        nl = sum(p["bicgstab_launches"] for p in profs)
+        kms = sum(p["bicgstab_kernel"] for p in profs)
+        kernel = "k_bicgstab_level (one launch = one variant's pressure solve, one thread block)"
+        solves = nl
+    if nl <= 0 or kms <= 0:
+        return None
+    phase_ms = sum(sum(p[k] for k in _lib.PHASES if k != "bicgstab_kernel") for p in profs)
+    achieved = (byts / nl) / (kms / nl / 1e3) / 1e9
+    return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": None, "bytes_per_launch": byts / nl,
+            "ms_per_launch": kms / nl, "launches": nl, "solves": solves, "iterations_per_solve": it / max(solves, 1),
+            "share_of_phase_time": sum(p["bicgstab_kernel"] for p in profs) / max(phase_ms, 1e-9)}
+
+
+def matched_comparison(ds, dt, sample):
+    """The north-star comparison on the ensemble at the matched profile (Newton accepted at CNV 1e-9
+    / MB 1e-11 on both paths, the reference's controller otherwise): the batched mixed form over all
+    variants against the plain FP64 path stepping variants one at a time through rf_step.  One
+    untimed and one timed report step each; the plain path runs on `sample` (variants spread over
+    the size range), the batched path on all of them; field error of the batched mixed states
+    against the plain FP64 ones on the sample."""
+    import numpy as np
+    import torch
+
+    from ressim_b200 import Ensemble, ReservoirSimulator
+
+    seq_cells = seq_ms = 0.0
+    fp64_states = {}
+    for i in sample:
+        sim = ReservoirSimulator.from_deck(ds[i])
+        sim.set_controller_options(False, MATCHED_CNV, MATCHED_MB)
+        sim.step(dt)
+        r = sim.step(dt)
+        seq_ms += r["device_ms"]
+        seq_cells += ds[i].n_cells
+        fp64_states[i] = sim.state()
+        sim.close()
+    ens = Ensemble(ds, precision="mixed")
+    ens.set_controller_options(False, MATCHED_CNV, MATCHED_MB)
+    ens.step(dt)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    reps = ens.step(dt)
+    ev1.record()
+    ev1.synchronize()
+    batch_ms = ev0.elapsed_time(ev1)
+    ep = es = 0.0
+    for i in sample:
+        st = ens.state(i)
+        ep = max(ep, float(np.max(np.abs(st["pressure"] - fp64_states[i]["pressure"]) /
+                                  np.maximum(np.abs(fp64_states[i]["pressure"]), 1.0))))
+        es = max(es, float(np.max(np.abs(st["sat_water"] - fp64_states[i]["sat_water"]))))
+    ens.close()
+    cells = sum(d.n_cells for d in ds)
+    v_batch = cells / (batch_ms / 1e3)
+    v_seq = seq_cells / (seq_ms / 1e3)
+    return {"profile": "matched: reference controller, Newton accepted at CNV 1e-9 / MB 1e-11 on both paths",
+            "batched_mixed": v_batch, "plain_fp64_one_at_a_time": v_seq, "ratio": v_batch / v_seq,
+            "plain_sample_variants": list(sample), "report_step": "the second report step (one untimed before it)",
+            "newton_iterations_batched": sum(r["newton_iterations"] for r in reps),
+            "field_error_mixed_vs_fp64": {"pressure_rel": ep, "sat_water_abs": es, "variants": list(sample)}}
+
+
 def run_ensemble(args, rank, world):
     """`--workload ensemble`: every rank steps its own `--variants` variants (weak scaling, no
     collective on the data path); value = all ranks' cells x K / the slowest rank's device time."""
     cpu_job = None
+    flags = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import multiprocessing as mp
 
+        flags = use_native_oracle()
         pool = mp.get_context("spawn").Pool(1)
         cpu_job = (pool, pool.apply_async(cpu_leg, ("ensemble", args.dt, args.warmup, 1, args.cpu_sample_s)))
     import ctypes as C
@@ -374,7 +497,7 @@ def run_ensemble(args, rank, world):
 
     import numpy as np
 
-    from ressim_b200 import Ensemble, _abi, _lib, decks
+    from ressim_b200 import Ensemble, _lib, decks
 
     if not torch.cuda.is_available():
         print(json.dumps({"error": "no CUDA device"}))
@@ -404,16 +527,22 @@ def run_ensemble(args, rank, world):
         autotune.tune([ds[i] for i in pick], dt, args.precision, path=args.cluster_table)
     if pg:
         pg.barrier()
-    ens = Ensemble(ds, precision=args.precision)
-    if args.cluster_table and os.path.exists(args.cluster_table):
-        from ressim_b200 import autotune
 
-        table = autotune.load(args.cluster_table)
-        sizes = autotune.apply(ens, table, args.precision,
-                               autotune.plan(table, ds, args.precision, host_threads=32,
-                                             sms=torch.cuda.get_device_properties(0).multi_processor_count))
-        tuned = {"table": os.path.basename(args.cluster_table),
-                 "sizes": {str(k): sizes.count(k) for k in sorted(set(sizes))}}
+    def make_ensemble():
+        e = Ensemble(ds, precision=args.precision)
+        nonlocal tuned
+        if args.cluster_table and os.path.exists(args.cluster_table):
+            from ressim_b200 import autotune
+
+            table = autotune.load(args.cluster_table)
+            sizes = autotune.apply(e, table, args.precision,
+                                   autotune.plan(table, ds, args.precision, host_threads=32,
+                                                 sms=torch.cuda.get_device_properties(0).multi_processor_count))
+            tuned = {"table": os.path.basename(args.cluster_table),
+                     "sizes": {str(k): sizes.count(k) for k in sorted(set(sizes))}}
+        return e
+
+    ens = make_ensemble()
     L = _lib.load()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -425,6 +554,9 @@ def run_ensemble(args, rank, world):
         ens.step(dt)
     for i in range(nv):
         ens.profile(i, enable=True, reset=True)
+    batch_prof = hasattr(ens, "batch_profile")
+    if batch_prof:
+        ens.batch_profile(enable=True, reset=True)
     launches0 = ens.kernel_launches()
     l2_flush()
     if pg:
@@ -435,22 +567,32 @@ def run_ensemble(args, rank, world):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dev_ms = 0.0
     newton = 0
-    for _ in range(args.steps):
+    first_state = None
+    for k in range(args.steps):
         ev0.record()
         reps = ens.step(dt)  # returns once every variant's stream has finished the report step
         ev1.record()
         ev1.synchronize()
         dev_ms += ev0.elapsed_time(ev1)
         newton += sum(r["newton_iterations"] for r in reps)
+        if k == 0 and rank == 0:
+            first_state = ens.state(0)  # outside the timed region: variant 0 after report step W
         l2_flush()
     clk = clocks.stop()
     launches = ens.kernel_launches() - launches0
     profs = [ens.profile(i, enable=False, reset=True) for i in range(nv)]
+    batch = ens.batch_profile(enable=False, reset=True) if batch_prof else None
     dev_ms_max = max_over_ranks(dev_ms, pg, "cuda")
     value = world * cells * args.steps / (dev_ms_max / 1e3)
+    ens.close()
 
-    # e2e: the next K report steps with every variant's state uploaded from pinned host memory
-    # before the step and read back after it
+    # e2e: a second ensemble takes the same warm-up (the path is deterministic), then the same K
+    # report steps are timed on the host clock with every variant's state uploaded from pinned host
+    # memory before each step and read back after it
+    ens = make_ensemble()
+    for _ in range(args.warmup):
+        reps = ens.step(dt)
+    times = [r["time_days"] for r in reps] if args.warmup else [0.0] * nv
     hosts = []
     for i, d in enumerate(ds):
         st = ens.state(i)
@@ -464,7 +606,6 @@ def run_ensemble(args, rank, world):
         pg.barrier()
     torch.cuda.synchronize()
     e2e_s = 0.0
-    times = [r["time_days"] for r in reps]
     for _ in range(args.steps):
         t0 = time.perf_counter()
         for i in range(nv):
@@ -479,30 +620,31 @@ def run_ensemble(args, rank, world):
         l2_flush()
     e2e_s = max_over_ranks(e2e_s, pg, "cuda")
     e2e_value = world * cells * args.steps / e2e_s
+    ens.close()
 
     peak, peak_kind = measured_hbm_peak()
-    it = sum(p["bicgstab_iterations"] for p in profs)
-    nl = sum(p["bicgstab_launches"] for p in profs)
-    kms = sum(p["bicgstab_kernel"] for p in profs)
-    byts = sum(bicgstab_bytes_per_iteration(d.n_cells, p["nnzb"]) * p["bicgstab_iterations"] for d, p in zip(ds, profs))
-    roof = None
-    if nl > 0 and kms > 0:
-        achieved_one = byts / (kms / 1e3) / 1e9  # per kernel, launches of all variants pooled
-        achieved_all = byts / (dev_ms / 1e3) / 1e9  # all variants' kernels over the step time
-        roof = {"kernel": "k_bicgstab_dsmem (all variants)", "bound": "hbm", "achieved": achieved_all, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved_all / peak, "traffic": None,
-                "achieved_per_kernel": achieved_one, "iterations_per_launch": it / nl,
-                "share_of_kernel_time": kms / max(sum(sum(p[k] for k in _lib.PHASES if k != "bicgstab_kernel")
-                                                      for p in profs), 1e-9)}
+    roof = ensemble_roofline(ds, profs, peak, peak_kind, batch)
+    matched = None
+    if rank == 0 and world == 1 and not args.no_matched:
+        sample = spread_sample([d.n_cells for d in ds], 16)
+        matched = matched_comparison(ds, dt, sample)
     cpu = None
+    field_err = None
     if cpu_job is not None:
         pool, job = cpu_job
         try:
-            v, k, el, cnewton, _ = job.get(timeout=900)
+            v, k, el, cnewton, cstates = job.get(timeout=900)
             cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                    "sample": f"variant 0 ({ds[0].n_cells} cells), report step(s) {args.warmup}..{args.warmup + k - 1} "
                              f"after {args.warmup} untimed ones ({cnewton} Newton iterations, {el:.1f} s), C++ "
-                             f"restatement of the reference FIM, 1 thread"}
+                             f"restatement of the reference FIM, 1 thread, {flags}"}
+            if first_state is not None and cstates:
+                cp_, cs_ = cstates[0][0], cstates[0][1]
+                field_err = {"variant": 0, "report_step": args.warmup,
+                             "pressure_rel": float(np.max(np.abs(first_state["pressure"] - cp_) /
+                                                          np.maximum(np.abs(cp_), 1.0))),
+                             "sat_water_abs": float(np.max(np.abs(first_state["sat_water"] - cs_))),
+                             "against": "FP64 oracle (C++ restatement of the reference), the reference's tolerances"}
         except Exception as e:  # noqa: BLE001 - reported in the line
             cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
         pool.terminate()
@@ -517,15 +659,15 @@ def run_ensemble(args, rank, world):
                        "dt_days": dt, "parallelism": f"variants sharded over {world} GPU(s)",
                        "l2": "flushed (256 MB write) between timed report steps; state alone exceeds L2",
                        "newton_iterations": newton,
-                       "e2e_steps": "the K report steps after the timed ones",
-                       "cluster_sizes": tuned or "automatic (smallest that fits the shared-memory form)"},
+                       "e2e_steps": "the same K report steps, on a second ensemble after the same warm-up",
+                       "cluster_sizes": tuned or "automatic"},
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * cells,
                     "d2h_bytes_per_step": 2 * 8 * cells},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
-            "precision": args.precision,
+            "precision": args.precision, "field_error_vs_oracle": field_err, "matched_comparison": matched,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
-    ens.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -685,9 +827,11 @@ def main():
     if args.workload == "adjoint":
         return run_adjoint(args, rank, world)
     cpu_job = None
+    flags = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "2m":
         import multiprocessing as mp
 
+        flags = use_native_oracle()
         pool = mp.get_context("spawn").Pool(1)
         cpu_job = (pool, pool.apply_async(cpu_leg, (args.workload, args.dt, args.warmup, 2, args.cpu_sample_s)))
 
@@ -841,7 +985,7 @@ def main():
             cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                    "sample": f"report steps {args.warmup}..{args.warmup + k - 1} of the same deck after "
                              f"{args.warmup} untimed ones ({cnewton} Newton iterations, {el:.1f} s), C++ "
-                             f"restatement of the reference FIM, 1 thread, run beside the GPU legs"}
+                             f"restatement of the reference FIM, 1 thread, {flags}, run beside the GPU legs"}
         except Exception as e:  # noqa: BLE001 - reported in the line
             cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
         pool.terminate()
