@@ -313,7 +313,7 @@ int32_t rf_dense_solve_noalloc(int32_t n, const double* a, const double* b, doub
  * simulator object steps one deck.  Each variant gets its own context (the rf_* calls above work on
  * rf_batch_context(b, i)); rf_batch_step advances every variant by one report step, driving the
  * variants from `host_threads` host threads (<= 0: max(32, hardware threads), at most n) so their
- * kernels run concurrently on the device from separate streams.  Set the environment variable
+ * kernels run concurrently on the device (see rf_batch_set_mode).  Set the environment variable
  * CUDA_DEVICE_MAX_CONNECTIONS=32 before CUDA initialises in the process: with the default of 8
  * hardware queues the variants' streams alias and short kernels wait behind long pressure solves
  * (the Python package sets it on import).  Returns the first negative
@@ -324,6 +324,24 @@ int32_t rf_batch_destroy(RfBatch* batch);
 int32_t rf_batch_size(const RfBatch* batch);
 RfCtx* rf_batch_context(RfBatch* batch, int32_t index);
 int32_t rf_batch_step(RfBatch* batch, double target_dt_days, RfStepReport* reports);
+
+/* How rf_batch_step drives the variants.  RF_BATCH_GROUPS (the default after rf_batch_create): the
+ * variants are split into `host_threads` groups with one host thread and one CUDA stream each;
+ * every variant's report step runs as a fiber on its group's thread, suspended instead of blocked
+ * while its stream works, and the group's pressure BiCGStab solves and block-ILU0 sweeps are issued
+ * as one batched launch per kind (thread block b runs variant b's solve), so far more solves run at
+ * once than there are hardware queues.  RF_BATCH_THREADS: one stream per variant and a pool of
+ * host threads stepping one variant at a time.  A variant's results do not depend on the mode.
+ * No counterpart in the reference. */
+#define RF_BATCH_GROUPS 0
+#define RF_BATCH_THREADS 1
+int32_t rf_batch_set_mode(RfBatch* batch, int32_t mode);
+/* Batched-launch statistics of RF_BATCH_GROUPS (CUDA events on the groups' streams while enabled):
+ * out (may be NULL) receives up to n values, read before enable/reset take effect: the group
+ * count, then per kind (pressure BiCGStab, block-ILU0 sweep) the launches, the solves they
+ * carried and their device ms.  enable > 0 switches the timing on, 0 off, < 0 leaves it; reset
+ * != 0 zeroes the totals. */
+int32_t rf_batch_profile(RfBatch* batch, int32_t enable, int32_t reset, double* out, int32_t n);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,8 @@ def load():
     L.rf_batch_context.argtypes = [C.c_void_p, C.c_int32]
     L.rf_batch_context.restype = C.c_void_p
     L.rf_batch_step.argtypes = [C.c_void_p, C.c_double, C.POINTER(_abi.RfStepReport)]
+    L.rf_batch_set_mode.argtypes = [C.c_void_p, C.c_int32]
+    L.rf_batch_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32]
     L.rf_dense_solve_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
                                          C.c_size_t]
     L.rf_set_controller_options.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double]
@@ -68,7 +70,7 @@ EXPORTED_SYMBOLS = (
     "rf_step", "rf_rate_history_len", "rf_rate_history_get", "rf_linear_solve_bsr", "rf_linear_solve_csr", "rf_kernel_launches",
     "rf_profile", "rf_set_linear_precision", "rf_set_cluster_size", "rf_batch_create", "rf_batch_destroy", "rf_batch_size",
     "rf_batch_context", "rf_batch_step", "rf_dense_solve_noalloc", "rf_set_controller_options", "rf_adjoint_record",
-    "rf_backward", "rf_well_count", "rf_set_pressure_solver",
+    "rf_backward", "rf_well_count", "rf_set_pressure_solver", "rf_batch_set_mode", "rf_batch_profile",
 )
 
 PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",

@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libressim_fim.so")
 SOURCES = ["rf_assembly.cu", "rf_linear.cu", "rf_direct.cu", "rf_state.cu", "rf_api.cu", "rf_noalloc.cu",
-           "rf_blackoil.cu", "rf_adjoint.cu", "rf_level.cu"]
+           "rf_blackoil.cu", "rf_adjoint.cu", "rf_level.cu", "rf_fiber.cu"]
 COMPILE_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
     "-Xcompiler", "-fPIC", "--fmad=false", "-Xptxas", "-O3",

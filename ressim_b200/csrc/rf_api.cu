@@ -25,6 +25,7 @@
 #include <tuple>
 
 #include "rf_blackoil.cuh"
+#include "rf_fiber.hpp"
 #include "rf_fluid.hpp"
 #include "rf_ops.hpp"
 #include "rf_state.hpp"
@@ -342,7 +343,7 @@ static void upload_controls(Ctx& c) {
   std::vector<WellControlH> k(W);
   for (int w = 0; w < W; ++w) k[w] = well_control(c, w);
   RF_CUDA(cudaMemcpyAsync(c.d_ctrl.p, k.data(), sizeof(WellControlH) * W, cudaMemcpyHostToDevice, c.stream));
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  stream_wait(c);
 }
 
 static void swap_state(Ctx& c) {
@@ -734,7 +735,7 @@ static void refresh_head_offsets(Ctx& c) {
     for (int k = 0; k < t.n_perfs; ++k) head[k] = c.head_offset[t.perf_entry[k]];
     RF_CUDA(cudaMemcpyAsync(c.d_perf_head.p, head.data(), sizeof(double) * head.size(), cudaMemcpyHostToDevice,
                             c.stream));
-    RF_CUDA(cudaStreamSynchronize(c.stream));
+    stream_wait(c);
   }
 }
 
@@ -851,6 +852,7 @@ static int step(Ctx& c, double target, RfStepReport* out) {
   if (!warning && substeps == max_sub && stepped < target) warning = 3;
   prof_resolve(c);
   RF_CUDA(cudaEventRecord(c.ev1, c.stream));
+  if (fiber_active()) fiber_wait_event(c.ev1);
   RF_CUDA(cudaEventSynchronize(c.ev1));
   float ms = 0.f;
   RF_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
@@ -1084,6 +1086,7 @@ static void setup_device(Ctx& c) {
   c.pin_pending.reserve(64);
   RF_CUDA(cudaEventCreate(&c.ev0));
   RF_CUDA(cudaEventCreate(&c.ev1));
+  RF_CUDA(cudaEventCreateWithFlags(&c.ev_wait, cudaEventDisableTiming));
   const int n = c.n, nx = c.nx, ny = c.ny, nz = c.nz, nxy = nx * ny;
   std::vector<double> tx(n, 0.0), ty(n, 0.0), tz(n, 0.0);
   for (int i = 0; i < n; ++i) {
@@ -1192,9 +1195,11 @@ static void free_ctx(Ctx& c) {
   c.d_bicg_iters = nullptr;
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
+  if (c.ev_wait) cudaEventDestroy(c.ev_wait);
   if (c.h_pin) cudaFreeHost(c.h_pin);
   c.h_pin = nullptr;
-  if (c.stream) cudaStreamDestroy(c.stream);
+  if (c.stream && c.stream_owned) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
 }
 
 #include "rf_adjoint.inc"
@@ -1617,17 +1622,82 @@ int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32
 }
 
 // ---------------------------------------------------------------------------------------------
-// Ensemble batch: independent decks stepped concurrently.  Every variant keeps its own context
-// (device buffers, CUDA stream, one-cluster level-scheduled launches), and a pool of host threads
-// drives the variants' controllers, largest first, so the device runs many variants' kernels at
-// once from separate streams.  The variants never exchange data.
+// Ensemble batch: independent decks stepped together.  Every variant keeps its own context
+// (device buffers, controller state).  Two ways of driving them:
+//  - RF_BATCH_GROUPS (default): the variants are split into groups of about equal size mix, one
+//    host thread and one CUDA stream per group; each variant's report step runs as a fiber on its
+//    group's thread, and the group's pressure solves and block-ILU0 sweeps go out as one batched
+//    launch per kind (rf_fiber.cu);
+//  - RF_BATCH_THREADS: one stream per variant and a pool of host threads, each stepping one
+//    variant at a time with its own launches.
+// The variants never exchange data, and a variant's results are the same either way.
 // ---------------------------------------------------------------------------------------------
 struct RfBatch {
   std::vector<RfCtx*> ctx;
   std::vector<int> order;  // variant indices by descending cell count
   int threads = 1;
   int device = 0;
+  int mode = RF_BATCH_GROUPS;
+  std::vector<std::unique_ptr<rf::BatchGroup>> groups;
 };
+
+namespace {
+
+// Hand the variants to `groups` groups (round robin in size order, so every group gets a similar
+// mix) on one stream each, or give every variant its own stream again (groups = 0).
+int32_t regroup(RfBatch* b, int mode) {
+  for (auto& g : b->groups) cudaStreamSynchronize(g->stream);
+  for (RfCtx* x : b->ctx) {
+    rf::Ctx& c = x->c;
+    if (!c.stream_owned) {
+      c.stream = nullptr;
+      if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return RF_ERR_CUDA;
+      c.stream_owned = 1;
+    }
+    c.batched = 0;
+  }
+  for (auto& g : b->groups)
+    if (g->stream) cudaStreamDestroy(g->stream);
+  b->groups.clear();
+  b->mode = mode;
+  if (mode != RF_BATCH_GROUPS) return RF_OK;
+  const int n = int(b->ctx.size());
+  const int G = std::max(1, std::min(b->threads, n));
+  for (int k = 0; k < G; ++k) {
+    auto g = std::make_unique<rf::BatchGroup>();
+    if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) return RF_ERR_CUDA;
+    b->groups.push_back(std::move(g));
+  }
+  for (int k = 0; k < n; ++k) {
+    const int i = b->order[k];
+    rf::BatchGroup& g = *b->groups[k % G];
+    rf::Ctx& c = b->ctx[i]->c;
+    cudaStreamSynchronize(c.stream);
+    cudaStreamDestroy(c.stream);
+    c.stream = g.stream;
+    c.stream_owned = 0;
+    c.batched = 1;
+    g.members.push_back(i);
+  }
+  return RF_OK;
+}
+
+struct StepJob {
+  RfCtx* ctx;
+  double dt;
+  RfStepReport* rep;
+  int32_t rc;
+};
+
+void step_job(void* p) {
+  StepJob* j = static_cast<StepJob*>(p);
+  j->rc = rf_step(j->ctx, j->dt, j->rep);
+}
+
+// Fiber stack per variant: the controller's frames hold a few KB; vectors live on the heap.
+constexpr size_t kFiberStack = 256 * 1024;
+
+}  // namespace
 
 int32_t rf_batch_create(const RfDeck* const* decks, int32_t n, int32_t host_threads, RfBatch** out) {
   if (!out || !decks || n <= 0) return RF_ERR_INVALID;
@@ -1652,19 +1722,34 @@ int32_t rf_batch_create(const RfDeck* const* decks, int32_t n, int32_t host_thre
   for (int32_t i = 0; i < n; ++i) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(),
                    [&](int x, int y) { return b->ctx[x]->c.n > b->ctx[y]->c.n; });
-  // the host threads mostly wait on their variant's stream: up to 32 (the most hardware queues
+  // the host threads mostly wait on the device: up to 32 (the most hardware queues
   // CUDA_DEVICE_MAX_CONNECTIONS can give the streams) even on fewer cores
   const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
   b->threads = host_threads > 0 ? host_threads : std::min<int>(n, std::max(hw, 32));
+  const int32_t rc = regroup(b, RF_BATCH_GROUPS);
+  if (rc != RF_OK) {
+    rf_batch_destroy(b);
+    return rc;
+  }
   *out = b;
   return RF_OK;
 }
 
 int32_t rf_batch_destroy(RfBatch* b) {
   if (!b) return RF_OK;
-  for (RfCtx* c : b->ctx) rf_destroy(c);
+  for (auto& g : b->groups) cudaStreamSynchronize(g->stream);
+  for (RfCtx* c : b->ctx) rf_destroy(c);  // group streams are not the contexts' to destroy
+  for (auto& g : b->groups)
+    if (g->stream) cudaStreamDestroy(g->stream);
+  b->groups.clear();
   delete b;
   return RF_OK;
+}
+
+int32_t rf_batch_set_mode(RfBatch* b, int32_t mode) {
+  if (!b || (mode != RF_BATCH_GROUPS && mode != RF_BATCH_THREADS)) return RF_ERR_INVALID;
+  if (mode == b->mode) return RF_OK;
+  return regroup(b, mode);
 }
 
 int32_t rf_batch_size(const RfBatch* b) { return b ? int32_t(b->ctx.size()) : 0; }
@@ -1674,23 +1759,65 @@ RfCtx* rf_batch_context(RfBatch* b, int32_t i) {
   return b->ctx[i];
 }
 
+int32_t rf_batch_profile(RfBatch* b, int32_t enable, int32_t reset, double* out, int32_t n) {
+  if (!b) return RF_ERR_INVALID;
+  double v[1 + 3 * rf::kBatchKinds] = {double(b->groups.size())};
+  for (auto& g : b->groups) {
+    g->resolve_timing();
+    for (int k = 0; k < rf::kBatchKinds; ++k) {
+      v[1 + 3 * k] += double(g->launches[k]);
+      v[2 + 3 * k] += double(g->items[k]);
+      v[3 + 3 * k] += g->ms_by_kind[k];
+    }
+  }
+  if (out)
+    for (int32_t i = 0; i < n && i < int32_t(sizeof(v) / sizeof(v[0])); ++i) out[i] = v[i];
+  for (auto& g : b->groups) {
+    if (reset) g->reset_stats();
+    if (enable >= 0) g->profiling = enable > 0;
+  }
+  return RF_OK;
+}
+
 int32_t rf_batch_step(RfBatch* b, double target_dt_days, RfStepReport* reports) {
   if (!b || !reports || !(target_dt_days > 0.0) || !std::isfinite(target_dt_days)) return RF_ERR_INVALID;
   const int n = int(b->ctx.size());
   std::vector<int32_t> rcs(n, RF_OK);
-  std::atomic<int> next{0};
-  auto work = [&]() {
-    cudaSetDevice(b->device);
-    for (int k = next.fetch_add(1); k < n; k = next.fetch_add(1)) {
-      const int i = b->order[k];
-      rcs[i] = rf_step(b->ctx[i], target_dt_days, &reports[i]);
-    }
-  };
-  std::vector<std::thread> pool;
-  const int extra = std::min(b->threads, n) - 1;
-  for (int t = 0; t < extra; ++t) pool.emplace_back(work);
-  work();
-  for (auto& t : pool) t.join();
+  if (b->mode == RF_BATCH_GROUPS) {
+    std::vector<StepJob> jobs(n);
+    for (int i = 0; i < n; ++i) jobs[i] = {b->ctx[i], target_dt_days, &reports[i], RF_OK};
+    auto run_group = [&](rf::BatchGroup* g) {
+      cudaSetDevice(b->device);
+      std::vector<void*> args;
+      for (int i : g->members) args.push_back(&jobs[i]);
+      g->failed = false;
+      rf::run_fibers(*g, step_job, args.data(), int(args.size()), kFiberStack);
+      if (g->failed)
+        for (int i : g->members) {
+          jobs[i].rc = RF_ERR_CUDA;
+          b->ctx[i]->c.err = "a batched launch of the variant's group failed";
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < b->groups.size(); ++k) pool.emplace_back(run_group, b->groups[k].get());
+    if (!b->groups.empty()) run_group(b->groups[0].get());
+    for (auto& t : pool) t.join();
+    for (int i = 0; i < n; ++i) rcs[i] = jobs[i].rc;
+  } else {
+    std::atomic<int> next{0};
+    auto work = [&]() {
+      cudaSetDevice(b->device);
+      for (int k = next.fetch_add(1); k < n; k = next.fetch_add(1)) {
+        const int i = b->order[k];
+        rcs[i] = rf_step(b->ctx[i], target_dt_days, &reports[i]);
+      }
+    };
+    std::vector<std::thread> pool;
+    const int extra = std::min(b->threads, n) - 1;
+    for (int t = 0; t < extra; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+  }
   int32_t worst = RF_OK;
   for (int i = 0; i < n; ++i) {
     if (rcs[i] < 0) return rcs[i];

@@ -89,9 +89,19 @@ struct LevelPlan {
   size_t blk_smem[2] = {0, 0};
 };
 
+// Cooperative scheduling of an ensemble's variants on shared host threads (rf_fiber.cu).  Inside a
+// batch step each variant's controller runs as a fiber on its group's thread: a wait on the
+// stream suspends the fiber instead of blocking the thread, and the level-scheduled kernels of the
+// group's variants are collected into one launch per kind.
+bool fiber_active();
+void fiber_wait_event(cudaEvent_t ev);
+
 struct Ctx {
   std::string err;
   cudaStream_t stream = nullptr;
+  int stream_owned = 1;  // 0: the stream belongs to an ensemble group (rf_batch_create)
+  int batched = 0;       // the context's level-scheduled kernels join its group's batched launches
+  cudaEvent_t ev_wait = nullptr;  // stream waits of a fiber
   long long launches = 0;
   int device = 0, num_sms = 0;
 
@@ -234,9 +244,20 @@ inline void d2h(Ctx& c, void* dst, const void* src, size_t bytes) {
   c.pin_pending.push_back({dst, off, bytes});
   c.h_pin_used = off + bytes;
 }
+// Wait until the context's stream has finished its queued work: a host block, or inside an
+// ensemble fiber a suspension of the fiber until an event recorded now has completed.
+inline void stream_wait(Ctx& c) {
+  if (fiber_active() && c.ev_wait) {
+    RF_CUDA(cudaEventRecord(c.ev_wait, c.stream));
+    fiber_wait_event(c.ev_wait);
+    RF_CUDA(cudaEventSynchronize(c.ev_wait));  // complete by now; reports a device error, if any
+  } else {
+    RF_CUDA(cudaStreamSynchronize(c.stream));
+  }
+}
 // Synchronise the context's stream and deliver the queued readbacks.
 inline void d2h_wait(Ctx& c) {
-  RF_CUDA(cudaStreamSynchronize(c.stream));
+  stream_wait(c);
   for (const auto& q : c.pin_pending) std::memcpy(q.dst, c.h_pin + q.off, q.bytes);
   c.pin_pending.clear();
   c.h_pin_used = 0;
@@ -285,7 +306,7 @@ struct PhaseScope {
 };
 inline void prof_resolve(Ctx& c) {
   if (!c.profiling) return;
-  cudaStreamSynchronize(c.stream);
+  stream_wait(c);
   for (auto& pe : c.ev_pending) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {

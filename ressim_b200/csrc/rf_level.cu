@@ -24,6 +24,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "rf_fiber.hpp"
 #include "rf_ops.hpp"
 
 namespace rf {
@@ -66,6 +67,8 @@ __device__ __forceinline__ void cp_wait_dyn(int pending) {
 template <class T>
 struct LvlArgs {
   int n, L, width, stages;
+  int threads;  // threads that work on this solve (a batched launch may have more; they only
+                // take part in the barriers, so the solve is the same as its own launch's)
   const int* lstart;   // [L + 1] first position of each level
   const int* pos_row;  // [n] natural row of each position
   const unsigned long long* fcode;  // [n] forward (lower part) code words
@@ -142,7 +145,8 @@ template <class T, int MODE>
 __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* win, T* far, T* out, double& acc,
                           double beta, double omega, double alpha, bool first) {
   constexpr bool FWD = MODE != 2;
-  const int t = threadIdx.x, NT = blockDim.x, L = a.L, W = a.width, D = a.stages, n = a.n;
+  const int NT = a.threads, L = a.L, W = a.width, D = a.stages, n = a.n;
+  const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   const unsigned long long* codes = FWD ? a.fcode : a.bcode;
   const T* vals = FWD ? a.fval : a.bval;
   const int* lptr = FWD ? a.flong_ptr : a.blong_ptr;
@@ -252,7 +256,8 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* win, T* 
 // MODE 0: acc0 += rh . out;  MODE 1: acc0 += out . out, acc1 += out . s
 template <class T, int MODE>
 __device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0, double& acc1) {
-  for (int q = threadIdx.x; q < a.n; q += blockDim.x) {
+  const int t0 = int(threadIdx.x) < a.threads ? int(threadIdx.x) : (1 << 30);
+  for (int q = t0; q < a.n; q += a.threads) {
     T s = T(0);
     const int k1 = a.sp_ptr[q + 1];
     for (int k = a.sp_ptr[q]; k < k1; ++k) s += a.spval[k] * in[a.sp_col[k]];
@@ -272,7 +277,8 @@ __device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0,
 // storage type T, as in the cluster kernels.
 template <class T>
 __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem, double* red) {
-  const int W = a.width, n = a.n, t = threadIdx.x, NT = blockDim.x;
+  const int W = a.width, n = a.n, NT = a.threads;
+  const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   unsigned char* stage = lvl_smem;
   T* win = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * W * (8 + 6 * sizeof(T)));
   T* far = win + 2 * size_t(W);
@@ -339,7 +345,7 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
   }
   __syncthreads();
   for (int q = t; q < n; q += NT) a.x[a.pos_row[q]] = a.xq[q];
-  if (t == 0 && a.iter_counter) atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
+  if (threadIdx.x == 0 && a.iter_counter) atomicAdd((unsigned long long*)a.iter_counter, (unsigned long long)started);
 }
 
 template <class T>
@@ -347,6 +353,20 @@ __global__ void __launch_bounds__(kLvlMaxThreads, 1) k_bicgstab_level(const __gr
   extern __shared__ __align__(16) unsigned char lvl_smem[];
   __shared__ double red[72];
   bicgstab_level_body(a, lvl_smem, red);
+}
+
+// Many independent pressure solves in one launch: thread block b solves item b (every item lays
+// out its own shared memory inside the launch's allocation, the largest item's size).
+template <class T>
+struct LvlBatch {
+  int count;
+  LvlArgs<T> item[kBatchItems];
+};
+template <class T>
+__global__ void __launch_bounds__(kLvlMaxThreads, 1) k_bicgstab_level_batch(const __grid_constant__ LvlBatch<T> b) {
+  extern __shared__ __align__(16) unsigned char lvl_smem[];
+  __shared__ double red[72];
+  if (blockIdx.x < unsigned(b.count)) bicgstab_level_body(b.item[blockIdx.x], lvl_smem, red);
 }
 
 // ============================================================================================
@@ -361,6 +381,7 @@ __global__ void __launch_bounds__(kLvlMaxThreads, 1) k_bicgstab_level(const __gr
 template <class T>
 struct BlkArgs {
   int n, L, width;
+  int threads;  // working threads (see LvlArgs::threads)
   const int* lstart;
   const int* pos_row;
   const int* f0;  // [n] CSR index of each position's first lower block
@@ -393,7 +414,8 @@ __device__ __forceinline__ void blk_sub(T& b0, T& b1, T& b2, const T* B, const T
 
 template <class T>
 __device__ void block_sweep_level_body(const BlkArgs<T>& a, unsigned char* blk_smem) {
-  const int W = a.width, L = a.L, t = threadIdx.x, NT = blockDim.x;
+  const int W = a.width, L = a.L, NT = a.threads;
+  const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   T* win = reinterpret_cast<T*>(blk_smem);  // [2][3 W]
   T* far = win + 6 * size_t(W);
   // forward: y = L^-1 cr
@@ -479,6 +501,17 @@ __global__ void __launch_bounds__(kLvlMaxThreads, 1) k_block_sweep_level(const _
 }
 
 template <class T>
+struct BlkBatch {
+  int count;
+  BlkArgs<T> item[kBatchItems];
+};
+template <class T>
+__global__ void __launch_bounds__(kLvlMaxThreads, 1) k_block_sweep_level_batch(const __grid_constant__ BlkBatch<T> b) {
+  extern __shared__ __align__(16) unsigned char blk_smem[];
+  if (blockIdx.x < unsigned(b.count)) block_sweep_level_body(b.item[blockIdx.x], blk_smem);
+}
+
+template <class T>
 size_t blk_smem_bytes(int W, int nfar) {
   return (6 * size_t(W) + 3 * size_t(std::max(nfar, 1))) * sizeof(T);
 }
@@ -532,6 +565,7 @@ void choose_block_shape(Ctx& c, int f) {
   P.blk_smem[f] = bytes;
   P.blk_threads[f] = auto_threads(c);
   raise_dynamic_smem((const void*)k_block_sweep_level<T>, bytes);
+  raise_dynamic_smem((const void*)k_block_sweep_level_batch<T>, bytes);
   P.blk_fits[f] = 1;
 }
 
@@ -553,6 +587,7 @@ void choose_shape(Ctx& c, int f) {
   P.smem[f] = lvl_smem_bytes<T>(P.width, st, nfar);
   P.threads[f] = auto_threads(c);
   raise_dynamic_smem((const void*)k_bicgstab_level<T>, P.smem[f]);
+  raise_dynamic_smem((const void*)k_bicgstab_level_batch<T>, P.smem[f]);
   P.fits[f] = 1;
 }
 
@@ -757,6 +792,52 @@ void level_pack(Ctx& c) {
   c.launches += 3;
 }
 
+static_assert(sizeof(LvlArgs<double>) <= kBatchArgBytes && sizeof(BlkArgs<double>) <= kBatchArgBytes,
+              "batched launch arguments must fit a batch item");
+
+// File a launch with the calling fiber's group (batched stepping); false when not in a fiber.
+static bool submit_item(int kind, int type, const void* args, size_t bytes, int threads, size_t smem) {
+  if (!fiber_active()) return false;
+  BatchItem it;
+  it.kind = kind;
+  it.type = type;
+  it.threads = threads;
+  it.smem = smem;
+  std::memcpy(it.args, args, bytes);
+  return fiber_submit(it);
+}
+
+template <class A, class B>
+static bool launch_batch(const BatchItem* const* items, int count, cudaStream_t stream, const void* fn) {
+  B b;
+  b.count = count;
+  int threads = 32;
+  size_t smem = 0;
+  for (int i = 0; i < count; ++i) {
+    std::memcpy(&b.item[i], items[i]->args, sizeof(A));
+    threads = std::max(threads, items[i]->threads);
+    smem = std::max(smem, items[i]->smem);
+  }
+  void* args[] = {&b};
+  return cudaLaunchKernel(fn, dim3(count), dim3(threads), args, smem, stream) == cudaSuccess;
+}
+
+bool launch_batch_items(int kind, int type, const BatchItem* const* items, int count, cudaStream_t stream) {
+  if (count <= 0) return true;
+  if (kind == kBatchPressure) {
+    if (type == 1)
+      return launch_batch<LvlArgs<float>, LvlBatch<float>>(items, count, stream,
+                                                           (const void*)k_bicgstab_level_batch<float>);
+    return launch_batch<LvlArgs<double>, LvlBatch<double>>(items, count, stream,
+                                                           (const void*)k_bicgstab_level_batch<double>);
+  }
+  if (type == 1)
+    return launch_batch<BlkArgs<float>, BlkBatch<float>>(items, count, stream,
+                                                         (const void*)k_block_sweep_level_batch<float>);
+  return launch_batch<BlkArgs<double>, BlkBatch<double>>(items, count, stream,
+                                                         (const void*)k_block_sweep_level_batch<double>);
+}
+
 template <class T>
 static void launch_level(Ctx& c, const double* rhs, double* x) {
   LevelPlan& P = c.lvl;
@@ -806,6 +887,8 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.sh = vb + 8 * size_t(n);
   a.max_iters = 50;
   a.iter_counter = c.d_bicg_iters;
+  a.threads = P.threads[f];
+  if (c.batched && submit_item(kBatchPressure, f, &a, sizeof(a), P.threads[f], P.smem[f])) return;
   c.launches++;
   k_bicgstab_level<T><<<1, P.threads[f], P.smem[f], c.stream>>>(a);
   RF_CUDA(cudaGetLastError());
@@ -838,14 +921,16 @@ void launch_block_sweep_level(Ctx& c, const double* cr, double* x, const void* l
     a.blong_code = P.d_blong_code.p;
     a.cr = cr;
     a.x = x;
+    a.threads = P.blk_threads[f];
   };
-  c.launches++;
   if (f == 1) {
     BlkArgs<float> a;
     fill(a);
     a.lu = static_cast<const float*>(lu);
     a.dinv = static_cast<const float*>(dinv);
     a.y = reinterpret_cast<float*>(P.d_blk_y.p);
+    if (c.batched && submit_item(kBatchBlockSweep, 1, &a, sizeof(a), P.blk_threads[1], P.blk_smem[1])) return;
+    c.launches++;
     k_block_sweep_level<float><<<1, P.blk_threads[1], P.blk_smem[1], c.stream>>>(a);
   } else {
     BlkArgs<double> a;
@@ -853,6 +938,8 @@ void launch_block_sweep_level(Ctx& c, const double* cr, double* x, const void* l
     a.lu = static_cast<const double*>(lu);
     a.dinv = static_cast<const double*>(dinv);
     a.y = reinterpret_cast<double*>(P.d_blk_y.p);
+    if (c.batched && submit_item(kBatchBlockSweep, 0, &a, sizeof(a), P.blk_threads[0], P.blk_smem[0])) return;
+    c.launches++;
     k_block_sweep_level<double><<<1, P.blk_threads[0], P.blk_smem[0], c.stream>>>(a);
   }
   RF_CUDA(cudaGetLastError());

@@ -81,6 +81,26 @@ class Ensemble:
         d["nnzb"] = int(out[k + 2])
         return d
 
+    def set_mode(self, mode: str) -> None:
+        """"groups" (default: fibers on per-group threads, one batched launch per group for the
+        pressure solves and block-ILU0 sweeps) or "threads" (a stream and a host-thread turn per
+        variant)."""
+        codes = {"groups": 0, "threads": 1}
+        if mode not in codes:
+            raise ValueError(f"batch mode must be one of {sorted(codes)}")
+        rc = _lib.load().rf_batch_set_mode(self._h, codes[mode])
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_batch_set_mode failed ({rc})")
+
+    def batch_profile(self, enable=None, reset=False) -> dict:
+        """Batched-launch statistics: groups, then launches / solves / device ms per kind."""
+        out = np.zeros(7)
+        en = -1 if enable is None else int(bool(enable))
+        _lib.load().rf_batch_profile(self._h, en, int(reset), _ptr(out), len(out))
+        return {"groups": int(out[0]), "pressure_launches": int(out[1]), "pressure_items": int(out[2]),
+                "pressure_ms": float(out[3]), "block_sweep_launches": int(out[4]),
+                "block_sweep_items": int(out[5]), "block_sweep_ms": float(out[6])}
+
     def set_controller_options(self, one_substep_per_report_step: bool = False, cnv_tol: float = 0.0,
                                mb_tol: float = 0.0) -> None:
         """rf_set_controller_options on every variant (see ReservoirSimulator.set_controller_options)."""
