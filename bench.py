@@ -583,7 +583,7 @@ def run_ensemble(args, rank, world):
     profs = [ens.profile(i, enable=False, reset=True) for i in range(nv)]
     batch = ens.batch_profile(enable=False, reset=True) if batch_prof else None
     if batch:  # the batched launches carry the filed solves; the contexts count their own launches
-        launches += batch["pressure_launches"] + batch["block_sweep_launches"]
+        launches += batch["pressure_launches"] + batch["block_sweep_launches"] + batch["factor_launches"]
     dev_ms_max = max_over_ranks(dev_ms, pg, "cuda")
     value = world * cells * args.steps / (dev_ms_max / 1e3)
     ens.close()

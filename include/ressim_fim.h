@@ -328,8 +328,8 @@ int32_t rf_batch_step(RfBatch* batch, double target_dt_days, RfStepReport* repor
 /* How rf_batch_step drives the variants.  RF_BATCH_GROUPS (the default after rf_batch_create): the
  * variants are split into `host_threads` groups with one host thread and one CUDA stream each;
  * every variant's report step runs as a fiber on its group's thread, suspended instead of blocked
- * while its stream works, and the group's pressure BiCGStab solves and block-ILU0 sweeps are issued
- * as one batched launch per kind (thread block b runs variant b's solve), so far more solves run at
+ * while its stream works, and the group's ILU0 factorisations, pressure BiCGStab solves and
+ * block-ILU0 sweeps are issued as one batched launch per kind (thread block b runs variant b's solve), so far more solves run at
  * once than there are hardware queues.  RF_BATCH_THREADS: one stream per variant and a pool of
  * host threads stepping one variant at a time.  A variant's results do not depend on the mode.
  * No counterpart in the reference. */
@@ -338,8 +338,8 @@ int32_t rf_batch_step(RfBatch* batch, double target_dt_days, RfStepReport* repor
 int32_t rf_batch_set_mode(RfBatch* batch, int32_t mode);
 /* Batched-launch statistics of RF_BATCH_GROUPS (CUDA events on the groups' streams while enabled):
  * out (may be NULL) receives up to n values, read before enable/reset take effect: the group
- * count, then per kind (pressure BiCGStab, block-ILU0 sweep) the launches, the solves they
- * carried and their device ms.  enable > 0 switches the timing on, 0 off, < 0 leaves it; reset
+ * count, then per kind (pressure BiCGStab, block-ILU0 sweep, ILU0 factorisation) the launches,
+ * the solves they carried and their device ms.  enable > 0 switches the timing on, 0 off, < 0 leaves it; reset
  * != 0 zeroes the totals. */
 int32_t rf_batch_profile(RfBatch* batch, int32_t enable, int32_t reset, double* out, int32_t n);
 

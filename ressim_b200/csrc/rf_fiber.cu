@@ -8,8 +8,8 @@
 // ucontext switches) on the group's thread:
 //   - a wait on the stream (stream_wait / d2h_wait) records an event and suspends the fiber; the
 //     thread resumes other fibers and picks the fiber up once the event has completed;
-//   - a level-scheduled kernel (the pressure BiCGStab, the block-ILU0 sweep) is not launched
-//     directly: the fiber files its arguments with the group and suspends.  When every unfinished
+//   - a level-scheduled kernel (the ILU0 factorisation, the pressure BiCGStab, the block-ILU0
+//     sweep) is not launched directly: the fiber files its arguments with the group and suspends.  When every unfinished
 //     fiber of the group is waiting for such a launch, the thread launches one kernel per kind
 //     whose thread block b runs item b, and resumes the fibers.
 // So the device runs the pressure solves of a whole group as one launch, and the groups' launches
@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "rf_fiber.hpp"
@@ -104,6 +105,17 @@ bool fiber_submit(const BatchItem& item) {
   tl_run->g->pending.push_back(item);
   suspend(2);
   return true;
+}
+
+bool fiber_file(int kind, int type, const void* args, size_t bytes, int threads, size_t smem) {
+  if (!fiber_active() || bytes > kBatchArgBytes) return false;
+  BatchItem it;
+  it.kind = kind;
+  it.type = type;
+  it.threads = threads;
+  it.smem = smem;
+  std::memcpy(it.args, args, bytes);
+  return fiber_submit(it);
 }
 
 cudaEvent_t BatchGroup::timing_event() {

@@ -9,10 +9,12 @@
 
 namespace rf {
 
-// Kinds of batched launches: the pressure BiCGStab and the block-ILU0 sweep (rf_level.cu).
+// Kinds of batched launches: the pressure BiCGStab and the block-ILU0 sweep (rf_level.cu), the
+// block-ILU0 and pressure-ILU0 factorisation (rf_linear.cu).
 constexpr int kBatchPressure = 0;
 constexpr int kBatchBlockSweep = 1;
-constexpr int kBatchKinds = 2;
+constexpr int kBatchFactor = 2;
+constexpr int kBatchKinds = 3;
 // Items per launch: the kernel parameter carries their arguments by value.
 constexpr int kBatchItems = 24;
 constexpr size_t kBatchArgBytes = 320;
@@ -50,10 +52,14 @@ struct BatchGroup {
 // File an item with the calling fiber's group and suspend until the group launches it; false
 // (nothing filed) when the caller is not a batch fiber.
 bool fiber_submit(const BatchItem& item);
+// The same for launch arguments `args` (bytes <= kBatchArgBytes) of a kernel kind.
+bool fiber_file(int kind, int type, const void* args, size_t bytes, int threads, size_t smem);
 // Run fn(args[i]) for i < count as fibers on the calling thread until all have returned.
 void run_fibers(BatchGroup& g, void (*fn)(void*), void* const* args, int count, size_t stack_bytes);
 // One launch of `count` items of one kind and value type on `stream` (rf_level.cu); false when
 // the launch failed.
 bool launch_batch_items(int kind, int type, const BatchItem* const* items, int count, cudaStream_t stream);
+// The factorisation's batched launch (rf_linear.cu).
+bool launch_factor_batch(const BatchItem* const* items, int count, cudaStream_t stream);
 
 }  // namespace rf

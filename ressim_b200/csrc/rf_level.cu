@@ -797,14 +797,7 @@ static_assert(sizeof(LvlArgs<double>) <= kBatchArgBytes && sizeof(BlkArgs<double
 
 // File a launch with the calling fiber's group (batched stepping); false when not in a fiber.
 static bool submit_item(int kind, int type, const void* args, size_t bytes, int threads, size_t smem) {
-  if (!fiber_active()) return false;
-  BatchItem it;
-  it.kind = kind;
-  it.type = type;
-  it.threads = threads;
-  it.smem = smem;
-  std::memcpy(it.args, args, bytes);
-  return fiber_submit(it);
+  return fiber_file(kind, type, args, bytes, threads, smem);
 }
 
 template <class A, class B>
@@ -824,6 +817,7 @@ static bool launch_batch(const BatchItem* const* items, int count, cudaStream_t 
 
 bool launch_batch_items(int kind, int type, const BatchItem* const* items, int count, cudaStream_t stream) {
   if (count <= 0) return true;
+  if (kind == kBatchFactor) return launch_factor_batch(items, count, stream);
   if (kind == kBatchPressure) {
     if (type == 1)
       return launch_batch<LvlArgs<float>, LvlBatch<float>>(items, count, stream,

@@ -20,9 +20,11 @@
 // fill.  Pressure-matrix entries with |v| <= 1e-14 are dropped, as the reference does.
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <cstdio>
 
+#include "rf_fiber.hpp"
 #include "rf_ops.hpp"
 
 namespace rf {
@@ -774,6 +776,54 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(LevelSched L, con
       ilu_rows_warp(L.long_rows[q], L.rp, L.col, L.diag, val, mask, lu, dinv, pval, plu, pdiag);
     cluster_barrier();
   }
+}
+
+// The same factorisation for many contexts in one launch (the ensemble's batched stepping):
+// thread block b factors item b's matrices alone, level by level, with block barriers.  Every row
+// gets the operations of k_factor_cluster, so the factors do not depend on the launch.
+struct FacArgs {
+  LevelSched L;
+  const double* val;
+  const unsigned char* mask;
+  double* lu;
+  double* dinv;
+  const double* pval;
+  double* plu;
+  double* pdiag;
+};
+struct FacBatch {
+  int count;
+  FacArgs item[kBatchItems];
+};
+__global__ void __launch_bounds__(kFBlock, 1) k_factor_batch(const __grid_constant__ FacBatch b) {
+  if (blockIdx.x >= unsigned(b.count)) return;  // uniform over the block
+  const FacArgs& a = b.item[blockIdx.x];
+  const LevelSched& L = a.L;
+  __shared__ int s_ptr[kSmemLevels];
+  const int* lp = stage_levels(L, s_ptr);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int warp = tid >> 5, nwarps = nth >> 5;
+  for (int l = 0; l < L.n_levels; ++l) {
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) {
+      const int r = L.lvl_rows[q];
+      if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
+      block_ilu_row(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv);
+      pressure_ilu_row(r, L.rp, L.col, L.diag, a.pval, a.plu, a.pdiag);
+    }
+    __syncwarp();
+    for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps)
+      ilu_rows_warp(L.long_rows[q], L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv, a.pval, a.plu, a.pdiag);
+    __syncthreads();
+  }
+}
+static_assert(sizeof(FacArgs) <= kBatchArgBytes, "factorisation arguments must fit a batch item");
+
+bool launch_factor_batch(const BatchItem* const* items, int count, cudaStream_t stream) {
+  FacBatch b;
+  b.count = count;
+  for (int i = 0; i < count; ++i) std::memcpy(&b.item[i], items[i]->args, sizeof(FacArgs));
+  void* args[] = {&b};
+  return cudaLaunchKernel((const void*)k_factor_batch, dim3(count), dim3(kFBlock), args, 0, stream) == cudaSuccess;
 }
 
 // ============================================================================================
@@ -1819,8 +1869,11 @@ static void cpr_build(Ctx& c) {
   const double* pval = c.d_pval.p;
   double* plu = c.d_plu.p;
   double* pdiag = c.d_pdiag.p;
-  void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
-  cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
+  const FacArgs fa{L, val, mask, lu, dinv, pval, plu, pdiag};
+  if (!(c.batched && fiber_file(kBatchFactor, 0, &fa, sizeof(fa), kFBlock, 0))) {
+    void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
+    cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
+  }
   c.lvl.packed = -1;
   const bool level = level_solver_active(c);
   if (level) level_pack(c);

@@ -94,12 +94,15 @@ class Ensemble:
 
     def batch_profile(self, enable=None, reset=False) -> dict:
         """Batched-launch statistics: groups, then launches / solves / device ms per kind."""
-        out = np.zeros(7)
+        out = np.zeros(10)
         en = -1 if enable is None else int(bool(enable))
         _lib.load().rf_batch_profile(self._h, en, int(reset), _ptr(out), len(out))
-        return {"groups": int(out[0]), "pressure_launches": int(out[1]), "pressure_items": int(out[2]),
-                "pressure_ms": float(out[3]), "block_sweep_launches": int(out[4]),
-                "block_sweep_items": int(out[5]), "block_sweep_ms": float(out[6])}
+        d = {"groups": int(out[0])}
+        for k, name in enumerate(("pressure", "block_sweep", "factor")):
+            d[f"{name}_launches"] = int(out[1 + 3 * k])
+            d[f"{name}_items"] = int(out[2 + 3 * k])
+            d[f"{name}_ms"] = float(out[3 + 3 * k])
+        return d
 
     def set_controller_options(self, one_substep_per_report_step: bool = False, cnv_tol: float = 0.0,
                                mb_tol: float = 0.0) -> None:
