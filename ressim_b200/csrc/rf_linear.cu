@@ -1691,52 +1691,61 @@ __global__ void k_dense_build(int nb, const int* __restrict__ rp, const int* __r
   for (int k = rp[r]; k < rp[r + 1]; ++k) a[size_t(r) * nb + col[k]] = pval[k];
 }
 // Dense inverse by LU with partial pivoting in nalgebra's operation order (linalg/lu.rs
-// `try_invert_to` and `gauss_step`, linalg/solve.rs triangular solves), one CTA, matrices in
-// global memory.  Every step updates each element once, so spreading a step over threads keeps
-// the sequential rounding: the first largest |pivot| of the column wins, multipliers are scaled by
-// the pivot's reciprocal, updates are y = (-p) * c + y, the forward solve has a unit diagonal and
-// the back substitution applies the columns from the last one down.  ok[0] = 0 when a pivot is
-// exactly zero.  `a` is overwritten by the factors; `perm` holds n ints.
-__global__ void __launch_bounds__(1024) k_dense_invert(int n, double* a, double* inv, int* perm, int* ok) {
-  __shared__ int s_piv[1];
-  __shared__ int s_fail;
-  const int t = threadIdx.x, nt = blockDim.x, lane = t & 31;
-  for (int r = t; r < n; r += nt) perm[r] = r;
-  if (t == 0) s_fail = 0;
+// `try_invert_to` and `gauss_step`, linalg/solve.rs triangular solves).  Every step updates each
+// element once, so spreading a step over threads keeps the sequential rounding: the first largest
+// |pivot| of the column wins, multipliers are scaled by the pivot's reciprocal, updates are
+// y = (-p) * c + y, the forward solve has a unit diagonal and the back substitution applies the
+// columns from the last one down.  Two kernels:
+//   k_dense_lu: one 1024-thread block factors `a` in place (row-major).  A warp owns a row of the
+//     trailing matrix at each step, its lanes the columns; while updating, lane 0 of each warp
+//     also tracks the largest |a_r,c+1| of its rows, so the next pivot is a reduction over 32
+//     partials (value descending, row ascending: the sequential scan's first maximum) instead of
+//     a pass over the column.  ok[0] = 0 when a pivot is exactly zero, else 1.
+//   k_dense_inv_cols: thread block b solves for the 32 columns 32b.. of the inverse with them held
+//     in shared memory (lane = column, warp = row), the factors read from global memory.
+// `perm` holds n ints.
+constexpr int kDenseColsPerBlock = 32;
+
+__device__ __forceinline__ void piv_better(double v, int r, double& bv, int& br) {
+  if (br < 0 || v > bv || (v == bv && r < br)) {
+    bv = v;
+    br = r;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_dense_lu(int n, double* a, int* perm, int* ok) {
+  __shared__ double s_val[32];
+  __shared__ int s_row[32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5;
+  for (int r = t; r < n; r += blockDim.x) perm[r] = r;
+  // partial pivots of column 0
+  {
+    double bv = 0.0;
+    int br = -1;
+    for (int r = t; r < n; r += blockDim.x) piv_better(fabs(a[size_t(r) * n]), r, bv, br);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+      const int orr = __shfl_down_sync(0xffffffffu, br, o);
+      if (orr >= 0) piv_better(ov, orr, bv, br);
+    }
+    if (lane == 0) {
+      s_val[warp] = bv;
+      s_row[warp] = br;
+    }
+  }
   __syncthreads();
   for (int c = 0; c < n; ++c) {
-    if (t < 32) {
-      // first maximum of |a[r][c]| over r >= c (strictly larger replaces)
-      int piv = -1;
-      double best = 0.0;
-      for (int r = c + lane; r < n; r += 32) {
-        const double v = fabs(a[size_t(r) * n + c]);
-        if (piv < 0 || v > best) {
-          best = v;
-          piv = r;
-        }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, o);
-        const int op = __shfl_down_sync(0xffffffffu, piv, o);
-        if (op >= 0 && (piv < 0 || ob > best || (ob == best && op < piv))) {
-          best = ob;
-          piv = op;
-        }
-      }
-      if (lane == 0) {
-        s_piv[0] = piv;
-        if (a[size_t(piv) * n + c] == 0.0) s_fail = 1;
-      }
-    }
-    __syncthreads();
-    if (s_fail) {
+    // every thread reduces the warps' partials in warp order: the same pivot everywhere
+    double bv = 0.0;
+    int piv = -1;
+    for (int w = 0; w < nwarps; ++w)
+      if (s_row[w] >= 0) piv_better(s_val[w], s_row[w], bv, piv);
+    if (piv < 0 || bv == 0.0) {  // |a_piv,c| of the partials: an exactly zero pivot
       if (t == 0) ok[0] = 0;
-      return;
+      return;  // uniform: every thread saw the same partials
     }
-    const int piv = s_piv[0];
     if (piv != c) {
-      for (int k = t; k < n; k += nt) {
+      for (int k = t; k < n; k += blockDim.x) {
         const double x = a[size_t(c) * n + k];
         a[size_t(c) * n + k] = a[size_t(piv) * n + k];
         a[size_t(piv) * n + k] = x;
@@ -1747,45 +1756,65 @@ __global__ void __launch_bounds__(1024) k_dense_invert(int n, double* a, double*
         perm[piv] = q;
       }
     }
-    __syncthreads();
+    __syncthreads();  // swapped rows visible; every thread is done reading this step's partials
     const double inv_pivot = 1.0 / a[size_t(c) * n + c];
-    for (int r = c + 1 + t; r < n; r += nt) a[size_t(r) * n + c] = a[size_t(r) * n + c] * inv_pivot;
-    __syncthreads();
-    const int m = n - c - 1;
-    for (long long idx = t; idx < (long long)m * m; idx += nt) {
-      const int r = c + 1 + int(idx / m), k = c + 1 + int(idx % m);
-      const double p = -a[size_t(c) * n + k];
-      a[size_t(r) * n + k] = p * a[size_t(r) * n + c] + a[size_t(r) * n + k];
+    double wv = 0.0;
+    int wr = -1;
+    for (int r = c + 1 + warp; r < n; r += nwarps) {
+      double* row = a + size_t(r) * n;
+      const double m = row[c] * inv_pivot;
+      __syncwarp();
+      if (lane == 0) row[c] = m;
+      for (int k = c + 1 + lane; k < n; k += 32) {
+        const double p = -a[size_t(c) * n + k];
+        row[k] = p * m + row[k];
+      }
+      if (lane == 0 && c + 1 < n) piv_better(fabs(row[c + 1]), r, wv, wr);
     }
-    __syncthreads();
-  }
-  // inv = P I, then the unit-lower and upper solves on all columns at once
-  for (long long idx = t; idx < (long long)n * n; idx += nt) {
-    const int r = int(idx / n), j = int(idx % n);
-    inv[idx] = (perm[r] == j) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  for (int i = 0; i + 1 < n; ++i) {
-    const int m = n - i - 1;
-    for (long long idx = t; idx < (long long)m * n; idx += nt) {
-      const int r = i + 1 + int(idx / n), j = int(idx % n);
-      const double coeff = -inv[size_t(i) * n + j];
-      inv[size_t(r) * n + j] = coeff * a[size_t(r) * n + i] + inv[size_t(r) * n + j];
-    }
-    __syncthreads();
-  }
-  for (int i = n - 1; i >= 0; --i) {
-    const double d = a[size_t(i) * n + i];
-    for (int j = t; j < n; j += nt) inv[size_t(i) * n + j] = inv[size_t(i) * n + j] / d;
-    __syncthreads();
-    for (long long idx = t; idx < (long long)i * n; idx += nt) {
-      const int r = int(idx / n), j = int(idx % n);
-      const double coeff = inv[size_t(i) * n + j];
-      inv[size_t(r) * n + j] = (-coeff) * a[size_t(r) * n + i] + inv[size_t(r) * n + j];
+    if (lane == 0) {
+      s_val[warp] = wv;
+      s_row[warp] = wr;
     }
     __syncthreads();
   }
   if (t == 0) ok[0] = 1;
+}
+
+__global__ void __launch_bounds__(1024) k_dense_inv_cols(int n, const double* __restrict__ lu,
+                                                         const int* __restrict__ perm, const int* __restrict__ ok,
+                                                         double* __restrict__ inv) {
+  extern __shared__ double X[];  // [n][32]
+  if (*ok == 0) return;          // the factorisation failed: leave the inverse untouched
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int j = blockIdx.x * kDenseColsPerBlock + lane;
+  const bool active = j < n;
+  for (int r = warp; r < n; r += nwarps) X[r * 32 + lane] = (active && perm[r] == j) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int i = 0; i + 1 < n; ++i) {  // unit-lower forward solve
+    const double coeff = -X[i * 32 + lane];
+    for (int r = i + 1 + warp; r < n; r += nwarps) X[r * 32 + lane] = coeff * lu[size_t(r) * n + i] + X[r * 32 + lane];
+    __syncthreads();
+  }
+  for (int i = n - 1; i >= 0; --i) {  // back substitution, columns from the last one down
+    if (warp == 0) X[i * 32 + lane] = X[i * 32 + lane] / lu[size_t(i) * n + i];
+    __syncthreads();
+    const double coeff = X[i * 32 + lane];
+    for (int r = warp; r < i; r += nwarps) X[r * 32 + lane] = (-coeff) * lu[size_t(r) * n + i] + X[r * 32 + lane];
+    __syncthreads();
+  }
+  if (active)
+    for (int r = warp; r < n; r += nwarps) inv[size_t(r) * n + j] = X[r * 32 + lane];
+}
+
+void dense_invert_launch(int n, double* a, double* inv, int* perm, int* ok, cudaStream_t stream) {
+  const size_t smem = sizeof(double) * size_t(n) * kDenseColsPerBlock;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute((const void*)k_dense_inv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(sizeof(double) * 299 * kDenseColsPerBlock));
+  });
+  k_dense_lu<<<1, 1024, 0, stream>>>(n, a, perm, ok);
+  k_dense_inv_cols<<<(n + kDenseColsPerBlock - 1) / kDenseColsPerBlock, 1024, smem, stream>>>(n, a, perm, ok, inv);
 }
 
 // ============================================================================================
@@ -1897,7 +1926,7 @@ static void cpr_build(Ctx& c) {
   c.dense_ok = 0;
   if (n <= 299) {
     k_dense_build<<<blocks_for(n), kBlock, 0, c.stream>>>(n, c.d_row_ptr.p, c.d_col.p, c.d_pval.p, c.d_tmp2.p);
-    k_dense_invert<<<1, 1024, 0, c.stream>>>(n, c.d_tmp2.p, c.d_dense.p, c.d_dense_perm.p, c.d_flag_dense.p);
+    dense_invert_launch(n, c.d_tmp2.p, c.d_dense.p, c.d_dense_perm.p, c.d_flag_dense.p, c.stream);
     c.launches += 2;
     int ok = 0;
     d2h(c, &ok, c.d_flag_dense.p, sizeof(int));

@@ -5,10 +5,11 @@
 // allocator owns the GPU, or a time-critical loop that must not block, since cudaMalloc and
 // cudaFree can synchronise the device.  For them this file offers x = A^{-1} b for a dense
 // row-major n x n pressure matrix, n <= RF_NOALLOC_MAX_ROWS (299, the size up to which the
-// reference's CPR inverts its pressure block densely, gmres_block_jacobi.rs:903-917).  It runs the same
-// two kernels as a context's CPR coarse stage (k_dense_invert, LU with partial pivoting in
-// nalgebra's order, then k_dense_matvec), with all scratch (the LU work copy, the inverse, the row
-// permutation and a status word) in one file-scope static device array.  The caller passes A, b
+// reference's CPR inverts its pressure block densely, gmres_block_jacobi.rs:903-917).  It runs
+// the same kernels as a context's CPR coarse stage (k_dense_lu and k_dense_inv_cols, the inverse
+// by LU with partial pivoting in nalgebra's order, then k_dense_matvec), with all scratch (the LU
+// work copy, the inverse, the row permutation and a status word) in one file-scope static device
+// array.  The caller passes A, b
 // and x in device memory; the call itself allocates nothing, on the device or the host.
 //
 // The array is part of the loaded library, so every GPU that loads it keeps about 1.4 MB for it
@@ -28,7 +29,7 @@
 #include "../../include/ressim_fim.h"
 
 namespace rf {
-__global__ void __launch_bounds__(1024) k_dense_invert(int n, double* a, double* inv, int* perm, int* ok);
+void dense_invert_launch(int n, double* a, double* inv, int* perm, int* ok, cudaStream_t stream);
 __global__ void k_dense_matvec(int n, const double* __restrict__ a, const double* __restrict__ x,
                                double* __restrict__ y, const int* __restrict__ ok);
 }  // namespace rf
@@ -89,7 +90,7 @@ extern "C" int32_t rf_dense_solve_noalloc(int32_t n, const double* a, const doub
   if ((e = cudaMemcpyAsync(lu, a, sizeof(double) * size_t(n) * n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
       (e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess)
     return report(err, err_len, RF_ERR_CUDA, cudaGetErrorString(e));
-  rf::k_dense_invert<<<1, 1024, 0, s>>>(n, lu, inv, perm, status);
+  rf::dense_invert_launch(n, lu, inv, perm, status, s);
   // the product skips its writes when the factorisation failed, so x keeps the caller's values
   rf::k_dense_matvec<<<(n + 63) / 64, 64, 0, s>>>(n, inv, b, x, status);
   if ((e = cudaGetLastError()) != cudaSuccess) return report(err, err_len, RF_ERR_CUDA, cudaGetErrorString(e));
