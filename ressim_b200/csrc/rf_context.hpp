@@ -68,11 +68,14 @@ struct LevelPlan {
   DBuf<unsigned long long> d_fcode, d_bcode;
   DBuf<int> d_flong_ptr, d_blong_ptr;                  // long rows: entry ranges
   DBuf<unsigned short> d_flong_code, d_blong_code;     // long rows: dependency codes
-  DBuf<int> d_sp_ptr, d_sp_col;                        // pressure matrix in position space
+  // pressure matrix in position space: [7][n] fixed-width columns, longer rows separately
+  DBuf<int> d_sp_col, d_splong_row, d_splong_ptr, d_splong_col;
+  int n_splong = 0, n_splong_entries = 0;
   // gather maps of the value packing: packed value i = T(src[map[i]]) (0 when map[i] < 0)
-  //   factor map over plu: [fwd 3n | bwd 3n | fwd long | bwd long]; matrix map over pval: [nnz]
+  //   factor map over plu: [fwd 3n | bwd 3n | fwd long | bwd long]; matrix map over pval:
+  //   [fixed width 7n | longer rows]
   DBuf<int> d_fmap, d_smap;
-  DBuf<double> d_vals64;  // [fwd 3n | bwd 3n | fwd long | bwd long | piv n | spmv nnz]
+  DBuf<double> d_vals64;  // [fwd 3n | bwd 3n | fwd long | bwd long | piv n | matrix 7n | longer rows]
   DBuf<float> d_vals32;
   DBuf<unsigned char> d_work;  // BiCGStab vectors in position order (9 x T) and x (double)
   size_t work_bytes = 0;

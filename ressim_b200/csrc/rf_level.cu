@@ -36,6 +36,7 @@ constexpr int kLvlMaxThreads = 512;
 constexpr int kLvlMaxStages = 4;
 constexpr unsigned kFarBit = 0x8000u;
 constexpr unsigned kLongCnt = 7u;
+constexpr int kSpK = 7;  // pressure-matrix entries per row held in the fixed-width layout
 
 __device__ __forceinline__ unsigned smem_u32a(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -77,14 +78,20 @@ struct LvlArgs {
   const unsigned short* flong_code;
   const int* blong_ptr;
   const unsigned short* blong_code;
-  const int* sp_ptr;  // [n + 1] pressure matrix rows in position space
-  const int* sp_col;  // positions of the columns, in the rows' column order
+  // pressure matrix in position space: rows of at most kSpK entries as [kSpK][n] column positions
+  // (-1: no entry; -2 in slot 0: a longer row, listed separately) and values, in column order
+  const int* sp_col;
+  int n_splong;
+  const int* splong_row;  // [n_splong] positions of the longer rows
+  const int* splong_ptr;  // [n_splong + 1]
+  const int* splong_col;
   const T* fval;      // [3][n] lower factor entries of short rows
   const T* bval;      // [3][n] upper factor entries of short rows
   const T* flong_val;
   const T* blong_val;
   const T* piv;    // [n] pressure ILU pivots
-  const T* spval;  // pressure matrix values in sp order
+  const T* spval;    // [kSpK][n]
+  const T* splongval;
   const double* rhs;  // natural order
   double* x;          // natural order
   double* xq;         // the iterate in position order
@@ -253,22 +260,45 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* win, T* 
 }
 
 // out = A in (pressure matrix, position space), with the dot products the solve needs next:
-// MODE 0: acc0 += rh . out;  MODE 1: acc0 += out . out, acc1 += out . s
+// MODE 0: acc0 += rh . out;  MODE 1: acc0 += out . out, acc1 += out . s.  A row's entries are
+// loaded together (fixed-width layout, coalesced across the warp) and summed in column order.
+template <class T, int MODE>
+__device__ __forceinline__ void spmv_row_done(const LvlArgs<T>& a, int q, T s, T* out, double& acc0, double& acc1) {
+  out[q] = s;
+  if (MODE == 0) {
+    acc0 += double(a.rh[q]) * double(s);
+  } else {
+    const double ti = double(s);
+    acc0 += ti * ti;
+    acc1 += ti * double(a.s[q]);
+  }
+}
 template <class T, int MODE>
 __device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0, double& acc1) {
-  const int t0 = int(threadIdx.x) < a.threads ? int(threadIdx.x) : (1 << 30);
-  for (int q = t0; q < a.n; q += a.threads) {
-    T s = T(0);
-    const int k1 = a.sp_ptr[q + 1];
-    for (int k = a.sp_ptr[q]; k < k1; ++k) s += a.spval[k] * in[a.sp_col[k]];
-    out[q] = s;
-    if (MODE == 0) {
-      acc0 += double(a.rh[q]) * double(s);
-    } else {
-      const double ti = double(s);
-      acc0 += ti * ti;
-      acc1 += ti * double(a.s[q]);
+  const int NT = a.threads, n = a.n;
+  const int t0 = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);
+  for (int q = t0; q < n; q += NT) {
+    int c[kSpK];
+    T v[kSpK], x[kSpK];
+#pragma unroll
+    for (int j = 0; j < kSpK; ++j) {
+      c[j] = a.sp_col[size_t(j) * n + q];
+      v[j] = a.spval[size_t(j) * n + q];
     }
+    if (c[0] == -2) continue;  // a longer row: below
+#pragma unroll
+    for (int j = 0; j < kSpK; ++j) x[j] = c[j] >= 0 ? in[c[j]] : T(0);
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < kSpK; ++j)
+      if (c[j] >= 0) s += v[j] * x[j];
+    spmv_row_done<T, MODE>(a, q, s, out, acc0, acc1);
+  }
+  for (int e = t0; e < a.n_splong; e += NT) {
+    const int q = a.splong_row[e];
+    T s = T(0);
+    for (int k = a.splong_ptr[e]; k < a.splong_ptr[e + 1]; ++k) s += a.splongval[k] * in[a.splong_col[k]];
+    spmv_row_done<T, MODE>(a, q, s, out, acc0, acc1);
   }
 }
 
@@ -534,7 +564,7 @@ size_t lvl_smem_bytes(int W, int stages, int nfar) {
 
 // offsets of the packed value segments (elements)
 struct LvlSeg {
-  size_t fval, bval, flong, blong, piv, sp, total;
+  size_t fval, bval, flong, blong, piv, sp, splong, total;
 };
 LvlSeg lvl_segments(const LevelPlan& P, int n) {
   LvlSeg s;
@@ -544,7 +574,8 @@ LvlSeg lvl_segments(const LevelPlan& P, int n) {
   s.blong = s.flong + size_t(P.n_flong);
   s.piv = s.blong + size_t(P.n_blong);
   s.sp = s.piv + size_t(n);
-  s.total = s.sp + size_t(P.nnz);
+  s.splong = s.sp + size_t(kSpK) * n;
+  s.total = s.splong + size_t(P.n_splong_entries);
   return s;
 }
 
@@ -677,18 +708,33 @@ void build_level_plan(Ctx& c) {
   P.nnz = c.h_row_ptr[n];
   fmap.insert(fmap.end(), flong_map.begin(), flong_map.end());
   fmap.insert(fmap.end(), blong_map.begin(), blong_map.end());
-  std::vector<int> sp_ptr(n + 1, 0), sp_col(P.nnz), smap(P.nnz), f0(n), b0(n);
+  // pressure matrix in position space: fixed-width rows, longer rows separately; smap gathers the
+  // values: [kSpK][n] fixed-width slots, then the longer rows' entries
+  std::vector<int> sp_col(size_t(kSpK) * n, -1), smap(size_t(kSpK) * n, -1), splong_row, splong_ptr{0},
+      splong_col, splong_map, f0(n), b0(n);
   for (int q = 0; q < n; ++q) {
     const int r = rows[q];
-    int e = sp_ptr[q];
-    for (int k = c.h_row_ptr[r]; k < c.h_row_ptr[r + 1]; ++k, ++e) {
-      sp_col[e] = pos[c.h_col[k]];
-      smap[e] = k;
+    const int k0 = c.h_row_ptr[r], k1 = c.h_row_ptr[r + 1];
+    if (k1 - k0 <= kSpK) {
+      for (int k = k0; k < k1; ++k) {
+        sp_col[size_t(k - k0) * n + q] = pos[c.h_col[k]];
+        smap[size_t(k - k0) * n + q] = k;
+      }
+    } else {
+      sp_col[q] = -2;
+      splong_row.push_back(q);
+      for (int k = k0; k < k1; ++k) {
+        splong_col.push_back(pos[c.h_col[k]]);
+        splong_map.push_back(k);
+      }
+      splong_ptr.push_back(int(splong_col.size()));
     }
-    sp_ptr[q + 1] = e;
     f0[q] = c.h_row_ptr[r];
     b0[q] = c.h_diag[r] + 1;
   }
+  P.n_splong = int(splong_row.size());
+  P.n_splong_entries = int(splong_col.size());
+  smap.insert(smap.end(), splong_map.begin(), splong_map.end());
   auto up_i = [](DBuf<int>& b, const std::vector<int>& h) {
     b.free();
     b.alloc(h.size());
@@ -712,8 +758,10 @@ void build_level_plan(Ctx& c) {
   up_i(P.d_blong_ptr, blong_ptr);
   up_u16(P.d_flong_code, flong_code);
   up_u16(P.d_blong_code, blong_code);
-  up_i(P.d_sp_ptr, sp_ptr);
   up_i(P.d_sp_col, sp_col);
+  up_i(P.d_splong_row, splong_row);
+  up_i(P.d_splong_ptr, splong_ptr);
+  up_i(P.d_splong_col, splong_col);
   up_i(P.d_fmap, fmap);
   up_i(P.d_smap, smap);
   up_i(P.d_blk_f0, f0);
@@ -735,8 +783,8 @@ void build_level_plan(Ctx& c) {
 
 void free_level_plan(Ctx& c) {
   LevelPlan& P = c.lvl;
-  for (auto* b : {&P.d_lstart, &P.d_pos_row, &P.d_flong_ptr, &P.d_blong_ptr, &P.d_sp_ptr, &P.d_sp_col, &P.d_fmap,
-                  &P.d_smap, &P.d_blk_f0, &P.d_blk_b0})
+  for (auto* b : {&P.d_lstart, &P.d_pos_row, &P.d_flong_ptr, &P.d_blong_ptr, &P.d_sp_col, &P.d_splong_row,
+                  &P.d_splong_ptr, &P.d_splong_col, &P.d_fmap, &P.d_smap, &P.d_blk_f0, &P.d_blk_b0})
     b->free();
   P.d_fcode.free();
   P.d_bcode.free();
@@ -773,20 +821,21 @@ void level_pack(Ctx& c) {
   LevelPlan& P = c.lvl;
   const int n = c.n;
   const LvlSeg g = lvl_segments(P, n);
-  const long long mf = (long long)g.piv;  // factor entries: fval, bval, long rows
+  const long long mf = (long long)g.piv;                    // factor entries: fval, bval, long rows
+  const long long ms = (long long)(g.total - g.sp);           // matrix entries: fixed width, longer rows
   if (c.precision == 1) {
     if (!P.d_vals32.p) P.d_vals32.alloc(g.total);
     float* v = P.d_vals32.p;
     k_lvl_gather<float><<<blocks_for(mf), kBlock, 0, c.stream>>>(mf, P.d_fmap.p, c.d_plu.p, v);
     k_lvl_gather<float><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_pos_row.p, c.d_pdiag.p, v + g.piv);
-    k_lvl_gather<float><<<blocks_for(P.nnz), kBlock, 0, c.stream>>>(P.nnz, P.d_smap.p, c.d_pval.p, v + g.sp);
+    k_lvl_gather<float><<<blocks_for(ms), kBlock, 0, c.stream>>>(ms, P.d_smap.p, c.d_pval.p, v + g.sp);
     P.packed = 1;
   } else {
     if (!P.d_vals64.p) P.d_vals64.alloc(g.total);
     double* v = P.d_vals64.p;
     k_lvl_gather<double><<<blocks_for(mf), kBlock, 0, c.stream>>>(mf, P.d_fmap.p, c.d_plu.p, v);
     k_lvl_gather<double><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_pos_row.p, c.d_pdiag.p, v + g.piv);
-    k_lvl_gather<double><<<blocks_for(P.nnz), kBlock, 0, c.stream>>>(P.nnz, P.d_smap.p, c.d_pval.p, v + g.sp);
+    k_lvl_gather<double><<<blocks_for(ms), kBlock, 0, c.stream>>>(ms, P.d_smap.p, c.d_pval.p, v + g.sp);
     P.packed = 0;
   }
   c.launches += 3;
@@ -857,14 +906,18 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.flong_code = P.d_flong_code.p;
   a.blong_ptr = P.d_blong_ptr.p;
   a.blong_code = P.d_blong_code.p;
-  a.sp_ptr = P.d_sp_ptr.p;
   a.sp_col = P.d_sp_col.p;
+  a.n_splong = P.n_splong;
+  a.splong_row = P.d_splong_row.p;
+  a.splong_ptr = P.d_splong_ptr.p;
+  a.splong_col = P.d_splong_col.p;
   a.fval = vals + g.fval;
   a.bval = vals + g.bval;
   a.flong_val = vals + g.flong;
   a.blong_val = vals + g.blong;
   a.piv = vals + g.piv;
   a.spval = vals + g.sp;
+  a.splongval = vals + g.splong;
   a.rhs = rhs;
   a.x = x;
   double* xq = reinterpret_cast<double*>(P.d_work.p);
