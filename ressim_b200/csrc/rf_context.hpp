@@ -68,6 +68,11 @@ struct LevelPlan {
   DBuf<unsigned long long> d_fcode, d_bcode;
   DBuf<int> d_flong_ptr, d_blong_ptr;                  // long rows: entry ranges
   DBuf<unsigned short> d_flong_code, d_blong_code;     // long rows: dependency codes
+  // the pressure sweeps: words with shared-memory dependency indices (static) and the per-position
+  // records built from them and the factors after each factorisation; long rows' indices
+  DBuf<unsigned long long> d_fword, d_bword;
+  DBuf<unsigned short> d_flong_abs, d_blong_abs;
+  DBuf<unsigned char> d_frec, d_brec;
   // pressure matrix in position space: [7][n] fixed-width columns, longer rows separately
   DBuf<int> d_sp_col, d_splong_row, d_splong_ptr, d_splong_col;
   int n_splong = 0, n_splong_entries = 0;

@@ -11,9 +11,10 @@
 //   - a row of level l reads its dependencies from a shared-memory window holding the values of
 //     the level processed just before (l-1 forward, l+1 backward); the few rows a dependency
 //     reaches from further away (the wells' fill) are kept in a shared-memory cache;
-//   - the pressure solve copies the per-row data of the levels ahead (factor values, dependency
-//     codes, pivots and the input vectors) into shared memory with cp.async, `stages - 1` levels
-//     ahead of use, so a level step is a block barrier, shared-memory reads and the row arithmetic;
+//   - the pressure solve copies the per-row data of the levels ahead (16-byte records of factor
+//     values, pivot and the dependencies' shared-memory indices, plus the input vectors) into
+//     shared memory with cp.async, `stages - 1` levels ahead of use, so a level step is a block
+//     barrier, shared-memory reads and the row arithmetic, with no branch per dependency;
 //   - the BiCGStab updates are fused into the sweeps that read them (the search direction p into
 //     the first forward sweep, s = r - alpha v and its norm into the second).
 // Every row is computed with the same operations in the same order as the natural-order
@@ -44,9 +45,6 @@ __device__ __forceinline__ unsigned smem_u32a(const void* p) {
 __device__ __forceinline__ void cp_async(void* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async(void* dst, const unsigned long long* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
-}
 __device__ __forceinline__ void cp_async(void* dst, const float* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
 }
@@ -65,9 +63,27 @@ __device__ __forceinline__ void cp_wait_dyn(int pending) {
   }
 }
 
+// Per-position records of the pressure sweeps (rebuilt after each factorisation), copied into
+// shared memory with 16-byte cp.async: a 64-bit word with three dependency indices into the
+// shared-memory array S (the two level windows, the far cache and a zero slot that absent entries
+// point at, their factor value being 0) and a meta field (bits 0-2 entry count, 7 = long row whose
+// index is the word's low 16 bits; bits 3-15 own far slot + 1), then the factor values in column
+// order (and the pivot for the backward sweep).
+template <class T>
+struct alignas(16) FRec {
+  unsigned long long word;
+  T v[3];
+};
+template <class T>
+struct alignas(16) BRec {
+  unsigned long long word;
+  T v[3];
+  T piv;
+};
+
 template <class T>
 struct LvlArgs {
-  int n, L, width, stages;
+  int n, L, width, stages, nfar;
   int threads;  // threads that work on this solve (a batched launch may have more; they only
                 // take part in the barriers, so the solve is the same as its own launch's)
   const int* lstart;   // [L + 1] first position of each level
@@ -85,11 +101,12 @@ struct LvlArgs {
   const int* splong_row;  // [n_splong] positions of the longer rows
   const int* splong_ptr;  // [n_splong + 1]
   const int* splong_col;
-  const T* fval;      // [3][n] lower factor entries of short rows
-  const T* bval;      // [3][n] upper factor entries of short rows
+  const FRec<T>* frec;  // [n] forward records
+  const BRec<T>* brec;  // [n] backward records
+  const unsigned short* flong_abs;  // long rows' dependency indices into S
+  const unsigned short* blong_abs;
   const T* flong_val;
   const T* blong_val;
-  const T* piv;    // [n] pressure ILU pivots
   const T* spval;    // [kSpK][n]
   const T* splongval;
   const double* rhs;  // natural order
@@ -138,115 +155,120 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* red) {
   b = red[65];
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
+}
+
+// Bytes of one staging slot: the level's records (the larger record type) and up to three input
+// vectors, rounded to 16 bytes.
 template <class T>
-__device__ __forceinline__ T dep_value(unsigned c, const T* nb, const T* far) {
-  return (c & kFarBit) ? far[c & 0x7fffu] : nb[c];
+__host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
+  return (size_t(W) * (sizeof(BRec<T>) + 3 * sizeof(T)) + 15) / 16 * 16;
 }
 
 // One triangular sweep over all levels.  MODE 0: forward sweep of p = r + beta (p - omega v)
 // (p = r on the first iteration), p stored; MODE 1: forward sweep of s = r - alpha v, s stored and
 // its squares summed into acc; MODE 2: backward sweep of y.  The result goes to `out` (position
 // order).  Each thread handles the offsets t, t + NT, ... of every level and stages exactly those
-// offsets' data, so the staging needs no barrier of its own.
+// offsets' data, so the staging needs no barrier of its own.  S holds the window of level l at
+// S[(l & 1) W ..], the far cache at S[2W ..] and the zero slot after it; sl is the level pointers.
 template <class T, int MODE>
-__device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* win, T* far, T* out, double& acc,
+__device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const int* sl, T* out, double& acc,
                           double beta, double omega, double alpha, bool first) {
   constexpr bool FWD = MODE != 2;
-  const int NT = a.threads, L = a.L, W = a.width, D = a.stages, n = a.n;
+  constexpr size_t RB = FWD ? sizeof(FRec<T>) : sizeof(BRec<T>);
+  constexpr size_t RMAX = sizeof(BRec<T>);
+  const int NT = a.threads, L = a.L, W = a.width, D = a.stages;
   const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
-  const unsigned long long* codes = FWD ? a.fcode : a.bcode;
-  const T* vals = FWD ? a.fval : a.bval;
+  const unsigned char* recs = FWD ? reinterpret_cast<const unsigned char*>(a.frec)
+                                  : reinterpret_cast<const unsigned char*>(a.brec);
   const int* lptr = FWD ? a.flong_ptr : a.blong_ptr;
-  const unsigned short* lcode = FWD ? a.flong_code : a.blong_code;
+  const unsigned short* lidx = FWD ? a.flong_abs : a.blong_abs;
   const T* lval = FWD ? a.flong_val : a.blong_val;
-  const T* in0 = MODE == 2 ? a.piv : a.r;
-  const T* in1 = MODE == 2 ? a.y : a.v;
-  const T* in2 = a.p;  // MODE 0 only
-  const size_t slot_bytes = size_t(W) * (8 + 6 * sizeof(T));
+  const T* in0 = MODE == 2 ? a.y : a.r;
+  const T* in1 = a.v;
+  const T* in2 = a.p;
+  const size_t slot_bytes = lvl_slot_bytes<T>(W);
   auto level_at = [&](int k) { return FWD ? k : L - 1 - k; };
-  auto issue = [&](int k) {
+  auto issue = [&](int k, int slot) {
     if (k >= L) return;
-    const int l = level_at(k), lst = a.lstart[l], w = a.lstart[l + 1] - lst;
-    unsigned char* base = stage + size_t(k % D) * slot_bytes;
-    unsigned long long* sc = reinterpret_cast<unsigned long long*>(base);
-    T* tp = reinterpret_cast<T*>(base + size_t(W) * 8);
+    const int l = level_at(k), lst = sl[l], w = sl[l + 1] - lst;
+    unsigned char* base = stage + size_t(slot) * slot_bytes;
+    T* inp = reinterpret_cast<T*>(base + size_t(W) * RMAX);
     for (int off = t; off < w; off += NT) {
       const int q = lst + off;
-      cp_async(sc + off, codes + q);
-      cp_async(tp + off, vals + q);
-      cp_async(tp + W + off, vals + n + q);
-      cp_async(tp + 2 * W + off, vals + 2 * n + q);
-      cp_async(tp + 3 * W + off, in0 + q);
-      cp_async(tp + 4 * W + off, in1 + q);
-      if (MODE == 0) cp_async(tp + 5 * W + off, in2 + q);
+      const unsigned char* src = recs + size_t(q) * RB;
+      unsigned char* dst = base + size_t(off) * RMAX;
+#pragma unroll
+      for (int b = 0; b < int(RB / 16); ++b) cp_async16(dst + 16 * b, src + 16 * b);
+      cp_async(inp + off, in0 + q);
+      if (MODE != 2) cp_async(inp + W + off, in1 + q);
+      if (MODE == 0) cp_async(inp + 2 * W + off, in2 + q);
     }
   };
-  if (D > 0)
+  int s_iss = 0, s_cur = 0;
+  if (D > 0) {
     for (int k = 0; k < D - 1; ++k) {
-      issue(k);
+      issue(k, k);
       cp_commit();
     }
+    s_iss = D - 1;
+  }
+  T* far = S + 2 * size_t(W);
   for (int k = 0; k < L; ++k) {
-    const int l = level_at(k), lst = a.lstart[l], w = a.lstart[l + 1] - lst;
-    const unsigned long long* sc;
-    const T *v0, *v1, *v2, *i0, *i1, *i2;
+    const int l = level_at(k), lst = sl[l], w = sl[l + 1] - lst;
+    const unsigned char* rbase;
+    const T* inp;
+    size_t rstride;
     if (D > 0) {
-      issue(k + D - 1);
+      issue(k + D - 1, s_iss);
       cp_commit();
       cp_wait_dyn(D - 1);
-      const unsigned char* base = stage + size_t(k % D) * slot_bytes;
-      sc = reinterpret_cast<const unsigned long long*>(base);
-      const T* tp = reinterpret_cast<const T*>(base + size_t(W) * 8);
-      v0 = tp;
-      v1 = tp + W;
-      v2 = tp + 2 * W;
-      i0 = tp + 3 * W;
-      i1 = tp + 4 * W;
-      i2 = tp + 5 * W;
+      s_iss = s_iss + 1 == D ? 0 : s_iss + 1;
+      rbase = stage + size_t(s_cur) * slot_bytes;
+      inp = reinterpret_cast<const T*>(rbase + size_t(W) * RMAX);
+      rstride = RMAX;
+      s_cur = s_cur + 1 == D ? 0 : s_cur + 1;
     } else {
-      sc = codes + lst;
-      v0 = vals + lst;
-      v1 = vals + n + lst;
-      v2 = vals + 2 * n + lst;
-      i0 = in0 + lst;
-      i1 = in1 + lst;
-      i2 = in2 + lst;
+      rbase = recs + size_t(lst) * RB;
+      inp = nullptr;
+      rstride = RB;
     }
-    const T* nb = win + size_t((k + 1) & 1) * W;  // the level processed before this one
-    T* cur = win + size_t(k & 1) * W;
+    T* cur = S + size_t(l & 1) * W;
     for (int off = t; off < w; off += NT) {
       const int q = lst + off;
-      const unsigned long long code = sc[off];
-      const unsigned meta = unsigned(code >> 48);
-      const unsigned cnt = meta & 7u;
+      const unsigned char* rp = rbase + size_t(off) * rstride;
+      const unsigned long long word = *reinterpret_cast<const unsigned long long*>(rp);
+      const T* v = reinterpret_cast<const T*>(rp + 8);
+      const T x0 = inp ? inp[off] : in0[q];
       T s;
       if (MODE == 0) {
-        const T rr = i0[off];
-        s = first ? rr : T(double(rr) + beta * (double(i2[off]) - omega * double(i1[off])));
+        const T x1 = inp ? inp[W + off] : in1[q];
+        const T x2 = inp ? inp[2 * W + off] : in2[q];
+        s = first ? x0 : T(double(x0) + beta * (double(x2) - omega * double(x1)));
         a.p[q] = s;
       } else if (MODE == 1) {
-        s = T(double(i0[off]) - alpha * double(i1[off]));
+        const T x1 = inp ? inp[W + off] : in1[q];
+        s = T(double(x0) - alpha * double(x1));
         a.s[q] = s;
         acc += double(s) * double(s);
       } else {
-        s = i1[off];
+        s = x0;
       }
-      if (cnt != kLongCnt) {
-        const unsigned c0 = unsigned(code) & 0xffffu, c1 = unsigned(code >> 16) & 0xffffu,
-                       c2 = unsigned(code >> 32) & 0xffffu;
-        T d0 = T(0), d1 = T(0), d2 = T(0);
-        if (cnt > 0u) d0 = dep_value(c0, nb, far);
-        if (cnt > 1u) d1 = dep_value(c1, nb, far);
-        if (cnt > 2u) d2 = dep_value(c2, nb, far);
-        if (cnt > 0u) s -= v0[off] * d0;
-        if (cnt > 1u) s -= v1[off] * d1;
-        if (cnt > 2u) s -= v2[off] * d2;
+      const unsigned meta = unsigned(word >> 48);
+      if ((meta & 7u) != kLongCnt) {
+        // absent entries point at the zero slot with a zero value: exact no-ops
+        const T d0 = S[unsigned(word) & 0xffffu], d1 = S[unsigned(word >> 16) & 0xffffu],
+                d2 = S[unsigned(word >> 32) & 0xffffu];
+        s -= v[0] * d0;
+        s -= v[1] * d1;
+        s -= v[2] * d2;
       } else {
-        const int li = int(code & 0xffffu);
-        for (int e = lptr[li]; e < lptr[li + 1]; ++e) s -= lval[e] * dep_value(unsigned(lcode[e]), nb, far);
+        const int li = int(word & 0xffffu);
+        for (int e = lptr[li]; e < lptr[li + 1]; ++e) s -= lval[e] * S[lidx[e]];
       }
       if (MODE == 2) {
-        const T d = i0[off];
+        const T d = v[3];
         s = fabs(double(d)) > kEpsL ? s / d : s;
       }
       cur[off] = s;
@@ -310,8 +332,10 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
   const int W = a.width, n = a.n, NT = a.threads;
   const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   unsigned char* stage = lvl_smem;
-  T* win = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * W * (8 + 6 * sizeof(T)));
-  T* far = win + 2 * size_t(W);
+  T* S = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * lvl_slot_bytes<T>(W));
+  int* sl = reinterpret_cast<int*>(S + 2 * size_t(W) + a.nfar + 1);
+  for (int l = threadIdx.x; l <= a.L; l += blockDim.x) sl[l] = a.lstart[l];
+  if (threadIdx.x == 0) S[2 * size_t(W) + a.nfar] = T(0);  // the zero slot
   double d0 = 0.0, d1 = 0.0;
   for (int q = t; q < n; q += NT) {
     const double ri = a.rhs[a.pos_row[q]] - 0.0;
@@ -335,8 +359,8 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     const double beta = it == 0 ? 0.0 : (rho / rho_prev) * (alpha / omega);
     d0 = 0.0;
     d1 = 0.0;
-    lvl_sweep<T, 0>(a, stage, win, far, a.y, d0, beta, omega, 0.0, it == 0);
-    lvl_sweep<T, 2>(a, stage, win, far, a.ph, d0, 0.0, 0.0, 0.0, false);
+    lvl_sweep<T, 0>(a, stage, S, sl, a.y, d0, beta, omega, 0.0, it == 0);
+    lvl_sweep<T, 2>(a, stage, S, sl, a.ph, d0, 0.0, 0.0, 0.0, false);
     lvl_spmv<T, 0>(a, a.ph, a.v, d0, d1);
     block_sum2(d0, d1, red);
     const double vd = d0;
@@ -344,13 +368,13 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     alpha = rho / vd;
     d0 = 0.0;
     d1 = 0.0;
-    lvl_sweep<T, 1>(a, stage, win, far, a.y, d0, 0.0, 0.0, alpha, false);
+    lvl_sweep<T, 1>(a, stage, S, sl, a.y, d0, 0.0, 0.0, alpha, false);
     block_sum2(d0, d1, red);
     if (sqrt(d0) <= tol) {
       for (int q = t; q < n; q += NT) a.xq[q] += alpha * double(a.ph[q]);
       break;
     }
-    lvl_sweep<T, 2>(a, stage, win, far, a.sh, d0, 0.0, 0.0, 0.0, false);
+    lvl_sweep<T, 2>(a, stage, S, sl, a.sh, d0, 0.0, 0.0, 0.0, false);
     d0 = 0.0;
     d1 = 0.0;
     lvl_spmv<T, 1>(a, a.sh, a.t, d0, d1);
@@ -557,9 +581,32 @@ __global__ void k_lvl_gather(long long m, const int* __restrict__ map, const dou
   }
 }
 
+// The sweep records from the gathered factor values (position order) and the static words.
 template <class T>
-size_t lvl_smem_bytes(int W, int stages, int nfar) {
-  return size_t(stages) * W * (8 + 6 * sizeof(T)) + (2 * size_t(W) + size_t(std::max(nfar, 1))) * sizeof(T);
+__global__ void k_lvl_pack_rec(int n, const unsigned long long* __restrict__ fword,
+                               const unsigned long long* __restrict__ bword, const T* __restrict__ fval,
+                               const T* __restrict__ bval, const T* __restrict__ piv, FRec<T>* __restrict__ frec,
+                               BRec<T>* __restrict__ brec) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  FRec<T> f;
+  BRec<T> b;
+  f.word = fword[q];
+  b.word = bword[q];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    f.v[j] = fval[size_t(j) * n + q];
+    b.v[j] = bval[size_t(j) * n + q];
+  }
+  b.piv = piv[q];
+  frec[q] = f;
+  brec[q] = b;
+}
+
+template <class T>
+size_t lvl_smem_bytes(int W, int stages, int nfar, int L) {
+  const size_t win = ((2 * size_t(W) + size_t(nfar) + 1) * sizeof(T) + 15) / 16 * 16;
+  return size_t(stages) * lvl_slot_bytes<T>(W) + win + sizeof(int) * (size_t(L) + 1);
 }
 
 // offsets of the packed value segments (elements)
@@ -610,12 +657,12 @@ void choose_shape(Ctx& c, int f) {
   const size_t budget = size_t(optin) > fa.sharedSizeBytes + 1024 ? size_t(optin) - fa.sharedSizeBytes - 1024 : 0;
   const int nfar = std::max(P.nfar_f, P.nfar_b);
   P.fits[f] = 0;
-  if (lvl_smem_bytes<T>(P.width, 0, nfar) > budget) return;
+  if (lvl_smem_bytes<T>(P.width, 0, nfar, P.n_levels) > budget) return;
   int st = kLvlMaxStages;
-  while (st > 0 && lvl_smem_bytes<T>(P.width, st, nfar) > budget) --st;
+  while (st > 0 && lvl_smem_bytes<T>(P.width, st, nfar, P.n_levels) > budget) --st;
   if (st == 1) st = 0;  // one stage only re-reads what it just copied: direct loads do the same
   P.stages[f] = st;
-  P.smem[f] = lvl_smem_bytes<T>(P.width, st, nfar);
+  P.smem[f] = lvl_smem_bytes<T>(P.width, st, nfar, P.n_levels);
   P.threads[f] = auto_threads(c);
   raise_dynamic_smem((const void*)k_bicgstab_level<T>, P.smem[f]);
   raise_dynamic_smem((const void*)k_bicgstab_level_batch<T>, P.smem[f]);
@@ -699,6 +746,40 @@ void build_level_plan(Ctx& c) {
     pack_row(false, q, rows[q]);
   }
   if (flong_ptr.size() > 65536 || blong_ptr.size() > 65536) return;
+  // the pressure sweeps' words: dependency indices into S (window of level lc at (lc & 1) W, far
+  // cache at 2W, zero slot at 2W + nfar)
+  const int nfar = std::max(nff, nfb);
+  const unsigned zero_slot = unsigned(2 * W + nfar);
+  if (zero_slot >= 65535u) return;
+  std::vector<unsigned long long> fword(n), bword(n);
+  std::vector<unsigned short> flong_abs, blong_abs;
+  for (int q = 0; q < n; ++q) {
+    const int r = rows[q], l = lvl[r];
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool fwd = dir == 0;
+      const int k0 = fwd ? c.h_row_ptr[r] : c.h_diag[r] + 1;
+      const int k1 = fwd ? c.h_diag[r] : c.h_row_ptr[r + 1];
+      auto abs_of = [&](int col) -> unsigned {
+        const int lc = lvl[col];
+        if (lc == (fwd ? l - 1 : l + 1)) return unsigned((lc & 1) * W + pos[col] - lp[lc]);
+        return unsigned(2 * W + (fwd ? ffar[col] : bfar[col]));
+      };
+      const unsigned long long code = (fwd ? fcode : bcode)[q];
+      const unsigned meta = unsigned(code >> 48);
+      unsigned long long word;
+      if ((meta & 7u) != kLongCnt) {
+        word = 0;
+        for (int j = 0; j < 3; ++j)
+          word |= (unsigned long long)(j < k1 - k0 ? abs_of(c.h_col[k0 + j]) : zero_slot) << (16 * j);
+      } else {
+        word = code & 0xffffull;  // the long-row index
+        std::vector<unsigned short>& out = fwd ? flong_abs : blong_abs;
+        for (int k = k0; k < k1; ++k) out.push_back(static_cast<unsigned short>(abs_of(c.h_col[k])));
+      }
+      word |= (unsigned long long)meta << 48;
+      (fwd ? fword : bword)[q] = word;
+    }
+  }
   P.n_levels = L;
   P.width = W;
   P.nfar_f = nff;
@@ -758,6 +839,14 @@ void build_level_plan(Ctx& c) {
   up_i(P.d_blong_ptr, blong_ptr);
   up_u16(P.d_flong_code, flong_code);
   up_u16(P.d_blong_code, blong_code);
+  up_u64(P.d_fword, fword);
+  up_u64(P.d_bword, bword);
+  up_u16(P.d_flong_abs, flong_abs);
+  up_u16(P.d_blong_abs, blong_abs);
+  P.d_frec.free();
+  P.d_brec.free();
+  P.d_frec.alloc(size_t(n) * sizeof(FRec<double>));
+  P.d_brec.alloc(size_t(n) * sizeof(BRec<double>));
   up_i(P.d_sp_col, sp_col);
   up_i(P.d_splong_row, splong_row);
   up_i(P.d_splong_ptr, splong_ptr);
@@ -790,6 +879,12 @@ void free_level_plan(Ctx& c) {
   P.d_bcode.free();
   P.d_flong_code.free();
   P.d_blong_code.free();
+  P.d_fword.free();
+  P.d_bword.free();
+  P.d_flong_abs.free();
+  P.d_blong_abs.free();
+  P.d_frec.free();
+  P.d_brec.free();
   P.d_vals64.free();
   P.d_vals32.free();
   P.d_work.free();
@@ -829,6 +924,9 @@ void level_pack(Ctx& c) {
     k_lvl_gather<float><<<blocks_for(mf), kBlock, 0, c.stream>>>(mf, P.d_fmap.p, c.d_plu.p, v);
     k_lvl_gather<float><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_pos_row.p, c.d_pdiag.p, v + g.piv);
     k_lvl_gather<float><<<blocks_for(ms), kBlock, 0, c.stream>>>(ms, P.d_smap.p, c.d_pval.p, v + g.sp);
+    k_lvl_pack_rec<float><<<blocks_for(n), kBlock, 0, c.stream>>>(
+        n, P.d_fword.p, P.d_bword.p, v + g.fval, v + g.bval, v + g.piv, reinterpret_cast<FRec<float>*>(P.d_frec.p),
+        reinterpret_cast<BRec<float>*>(P.d_brec.p));
     P.packed = 1;
   } else {
     if (!P.d_vals64.p) P.d_vals64.alloc(g.total);
@@ -836,9 +934,12 @@ void level_pack(Ctx& c) {
     k_lvl_gather<double><<<blocks_for(mf), kBlock, 0, c.stream>>>(mf, P.d_fmap.p, c.d_plu.p, v);
     k_lvl_gather<double><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_pos_row.p, c.d_pdiag.p, v + g.piv);
     k_lvl_gather<double><<<blocks_for(ms), kBlock, 0, c.stream>>>(ms, P.d_smap.p, c.d_pval.p, v + g.sp);
+    k_lvl_pack_rec<double><<<blocks_for(n), kBlock, 0, c.stream>>>(
+        n, P.d_fword.p, P.d_bword.p, v + g.fval, v + g.bval, v + g.piv, reinterpret_cast<FRec<double>*>(P.d_frec.p),
+        reinterpret_cast<BRec<double>*>(P.d_brec.p));
     P.packed = 0;
   }
-  c.launches += 3;
+  c.launches += 4;
 }
 
 static_assert(sizeof(LvlArgs<double>) <= kBatchArgBytes && sizeof(BlkArgs<double>) <= kBatchArgBytes,
@@ -911,11 +1012,13 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.splong_row = P.d_splong_row.p;
   a.splong_ptr = P.d_splong_ptr.p;
   a.splong_col = P.d_splong_col.p;
-  a.fval = vals + g.fval;
-  a.bval = vals + g.bval;
+  a.frec = reinterpret_cast<const FRec<T>*>(P.d_frec.p);
+  a.brec = reinterpret_cast<const BRec<T>*>(P.d_brec.p);
+  a.flong_abs = P.d_flong_abs.p;
+  a.blong_abs = P.d_blong_abs.p;
+  a.nfar = std::max(P.nfar_f, P.nfar_b);
   a.flong_val = vals + g.flong;
   a.blong_val = vals + g.blong;
-  a.piv = vals + g.piv;
   a.spval = vals + g.sp;
   a.splongval = vals + g.splong;
   a.rhs = rhs;
