@@ -101,6 +101,8 @@ def parse():
                     help="ensemble: JSON table of tuned cluster sizes (ressim_b200.autotune) applied per variant")
     ap.add_argument("--tune-variants", type=int, default=0,
                     help="ensemble: first tune this many variants spread over the size range into --cluster-table")
+    ap.add_argument("--batch-mode", choices=["groups", "threads"], default="groups",
+                    help="ensemble: fiber groups with batched level-scheduled launches, or a thread per variant")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-matched", action="store_true",
                     help="ensemble: skip the matched-profile comparison (batched mixed vs plain FP64)")
@@ -530,6 +532,7 @@ def run_ensemble(args, rank, world):
 
     def make_ensemble():
         e = Ensemble(ds, precision=args.precision)
+        e.set_mode(args.batch_mode)
         nonlocal tuned
         if args.cluster_table and os.path.exists(args.cluster_table):
             from ressim_b200 import autotune
@@ -662,7 +665,7 @@ def run_ensemble(args, rank, world):
                        "l2": "flushed (256 MB write) between timed report steps; state alone exceeds L2",
                        "newton_iterations": newton,
                        "e2e_steps": "the same K report steps, on a second ensemble after the same warm-up",
-                       "cluster_sizes": tuned or "automatic"},
+                       "cluster_sizes": tuned or "automatic", "batch_mode": args.batch_mode},
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * 8 * cells,
                     "d2h_bytes_per_step": 2 * 8 * cells},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
