@@ -1643,8 +1643,11 @@ struct RfBatch {
 
 namespace {
 
-// Hand the variants to `groups` groups (round robin in size order, so every group gets a similar
-// mix) on one stream each, or give every variant its own stream again (groups = 0).
+// Hand the variants to groups of neighbours in size order (largest first), one stream each, or give
+// every variant its own stream again.  A group advances from one batched launch to the next
+// together, so a launch lasts as long as its largest solve: groups of similar sizes keep the
+// small variants from waiting on large ones, and the groups of small variants finish early and
+// leave the device to the large ones.
 int32_t regroup(RfBatch* b, int mode) {
   for (auto& g : b->groups) cudaStreamSynchronize(g->stream);
   for (RfCtx* x : b->ctx) {
@@ -1670,7 +1673,7 @@ int32_t regroup(RfBatch* b, int mode) {
   }
   for (int k = 0; k < n; ++k) {
     const int i = b->order[k];
-    rf::BatchGroup& g = *b->groups[k % G];
+    rf::BatchGroup& g = *b->groups[int((long long)k * G / n)];
     rf::Ctx& c = b->ctx[i]->c;
     cudaStreamSynchronize(c.stream);
     cudaStreamDestroy(c.stream);
