@@ -1185,6 +1185,7 @@ static void free_ctx(Ctx& c) {
   c.d_dir_perm.free();
   c.dir_rows = 0;
   free_level_plan(c);
+  for (auto* b : {&c.d_tri_ptr, &c.d_tri_up, &c.d_tri_ip, &c.d_pt_ptr, &c.d_pt_lp, &c.d_pt_ue}) b->free();
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
   if (c.levels.d_long_rows) cudaFree(c.levels.d_long_rows);

@@ -221,6 +221,8 @@ struct Ctx {
   int precision = 0;
   DBuf<float> d_lu32, d_dinv32, d_plu32, d_pval32, d_pdiag32, d_pvec32, d_sweep32;
   DBuf<int> d_flag_dense;
+  // update lists of the factorisation (rf_linear.cu, FacRecipes)
+  DBuf<int> d_tri_ptr, d_tri_up, d_tri_ip, d_pt_ptr, d_pt_lp, d_pt_ue;
   // pressure-stage solver: 0 automatic, 1 the cluster kernels, 2 the single-CTA level-order kernels
   int pressure_solver = 0;
   int level_threads = 0;  // threads of the level-order kernels (0: automatic)

@@ -781,6 +781,20 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(LevelSched L, con
 // The same factorisation for many contexts in one launch (the ensemble's batched stepping):
 // thread block b factors item b's matrices alone, level by level, with block barriers.  Every row
 // gets the operations of k_factor_cluster, so the factors do not depend on the launch.
+// Precomputed update lists of the factorisation (built once per pattern): for each lower entry kp
+// of a row, the pairs (up, ip) of the U-row of col[kp] whose column the row also holds (the
+// merge block_ilu_row performs); for each entry k of a row, the terms (lp, ue) of the pressure ILU
+// (pressure_ilu_row's lower entries lp before it whose row holds the column of k above its
+// diagonal, at entry ue).  Present-entry checks on the values stay at run time.
+struct FacRecipes {
+  const int* tri_ptr;  // [nnzb + 1]
+  const int* tri_up;
+  const int* tri_ip;
+  const int* pt_ptr;   // [nnzb + 1]
+  const int* pt_lp;
+  const int* pt_ue;
+};
+
 struct FacArgs {
   LevelSched L;
   const double* val;
@@ -790,7 +804,66 @@ struct FacArgs {
   const double* pval;
   double* plu;
   double* pdiag;
+  FacRecipes R;  // tri_ptr == nullptr: search as block_ilu_row / pressure_ilu_row do
 };
+
+// Both ILU0 rows of row i from the update lists: the same operations in the same order as
+// block_ilu_row and pressure_ilu_row.
+__device__ void ilu_row_recipe(int i, const FacArgs& a) {
+  const int* rp = a.L.rp;
+  const int* col = a.L.col;
+  const int b0 = rp[i], dp = a.L.diag[i], b1 = rp[i + 1];
+  const FacRecipes& R = a.R;
+  for (int k = b0; k < b1; ++k) {
+    const bool m = a.mask[k];
+    for (int e = 0; e < 9; ++e) a.lu[size_t(k) * 9 + e] = m ? a.val[size_t(k) * 9 + e] : 0.0;
+  }
+  for (int kp = b0; kp < dp; ++kp) {
+    if (!a.mask[kp]) continue;
+    double lik[9];
+    mat3_mul(a.lu + size_t(kp) * 9, a.dinv + size_t(col[kp]) * 9, lik);
+    for (int e = R.tri_ptr[kp]; e < R.tri_ptr[kp + 1]; ++e) {
+      const int up = R.tri_up[e], ip = R.tri_ip[e];
+      if (!a.mask[up] || !a.mask[ip]) continue;
+      double prod[9];
+      mat3_mul(lik, a.lu + size_t(up) * 9, prod);
+      double* t = a.lu + size_t(ip) * 9;
+      for (int q = 0; q < 9; ++q) t[q] -= prod[q];
+    }
+    for (int q = 0; q < 9; ++q) a.lu[size_t(kp) * 9 + q] = lik[q];
+  }
+  mat3_inverse_or_diag(a.lu + size_t(dp) * 9, a.dinv + size_t(i) * 9);
+  // pressure ILU0
+  auto terms = [&](int k, double s) {
+    for (int e = R.pt_ptr[k]; e < R.pt_ptr[k + 1]; ++e) {
+      const int lp = R.pt_lp[e];
+      if (a.pval[lp] == 0.0) continue;
+      s -= a.plu[lp] * a.plu[R.pt_ue[e]];
+    }
+    return s;
+  };
+  for (int kp = b0; kp < dp; ++kp) {
+    if (a.pval[kp] == 0.0) {
+      a.plu[kp] = 0.0;
+      continue;
+    }
+    const double s = terms(kp, a.pval[kp]);
+    const double d = a.pdiag[col[kp]];
+    a.plu[kp] = fabs(d) > kEps ? s / d : 0.0;
+  }
+  const double de = a.pval[dp];
+  double ud = terms(dp, de);
+  if (fabs(ud) <= kEps) ud = fabs(de) > kEps ? de : 1.0;
+  a.pdiag[i] = ud;
+  a.plu[dp] = 0.0;
+  for (int up = dp + 1; up < b1; ++up) {
+    if (a.pval[up] == 0.0) {
+      a.plu[up] = 0.0;
+      continue;
+    }
+    a.plu[up] = terms(up, a.pval[up]);
+  }
+}
 struct FacBatch {
   int count;
   FacArgs item[kBatchItems];
@@ -807,8 +880,12 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_batch(const __grid_consta
     for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) {
       const int r = L.lvl_rows[q];
       if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
-      block_ilu_row(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv);
-      pressure_ilu_row(r, L.rp, L.col, L.diag, a.pval, a.plu, a.pdiag);
+      if (a.R.tri_ptr) {
+        ilu_row_recipe(r, a);
+      } else {
+        block_ilu_row(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv);
+        pressure_ilu_row(r, L.rp, L.col, L.diag, a.pval, a.plu, a.pdiag);
+      }
     }
     __syncwarp();
     for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps)
@@ -1898,8 +1975,18 @@ static void cpr_build(Ctx& c) {
   const double* pval = c.d_pval.p;
   double* plu = c.d_plu.p;
   double* pdiag = c.d_pdiag.p;
-  const FacArgs fa{L, val, mask, lu, dinv, pval, plu, pdiag};
-  if (!(c.batched && fiber_file(kBatchFactor, 0, &fa, sizeof(fa), kFBlock, 0))) {
+  FacRecipes rec{c.d_tri_ptr.p, c.d_tri_up.p, c.d_tri_ip.p, c.d_pt_ptr.p, c.d_pt_lp.p, c.d_pt_ue.p};
+  const FacArgs fa{L, val, mask, lu, dinv, pval, plu, pdiag, rec};
+  if (c.batched && fiber_file(kBatchFactor, 0, &fa, sizeof(fa), kFBlock, 0)) {
+    // filed with the group's batched launch
+  } else if (level_solver_active(c)) {
+    // the level-order path: one thread block with the update lists
+    FacBatch fb;
+    fb.count = 1;
+    fb.item[0] = fa;
+    k_factor_batch<<<1, kFBlock, 0, c.stream>>>(fb);
+    c.launches++;
+  } else {
     void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
     cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
   }
@@ -2377,6 +2464,56 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
 }
 
 // ---- one-time setup ----
+// Update lists of the factorisation (FacRecipes) for the current pattern.
+void build_factor_recipes(Ctx& c) {
+  const int n = c.n, nnzb = c.nnzb;
+  std::vector<int> tri_ptr(nnzb + 1, 0), tri_up, tri_ip, pt_ptr(nnzb + 1, 0), pt_lp, pt_ue;
+  auto find_in_row_upper = [&](int row, int colj) -> int {
+    const int lo = c.h_diag[row] + 1, hi = c.h_row_ptr[row + 1];
+    auto b = c.h_col.begin() + lo, e = c.h_col.begin() + hi;
+    auto it = std::lower_bound(b, e, colj);
+    return (it != e && *it == colj) ? int(it - c.h_col.begin()) : -1;
+  };
+  for (int i = 0; i < n; ++i) {
+    const int b0 = c.h_row_ptr[i], dp = c.h_diag[i], b1 = c.h_row_ptr[i + 1];
+    for (int k = b0; k < b1; ++k) {
+      if (k < dp) {  // block ILU: U-row of col[k] against row i's later entries
+        const int kr = c.h_col[k];
+        int ip = k + 1;
+        for (int up = c.h_diag[kr] + 1; up < c.h_row_ptr[kr + 1]; ++up) {
+          const int j = c.h_col[up];
+          while (ip < b1 && c.h_col[ip] < j) ++ip;
+          if (ip >= b1) break;
+          if (c.h_col[ip] != j) continue;
+          tri_up.push_back(up);
+          tri_ip.push_back(ip);
+        }
+      }
+      tri_ptr[k + 1] = int(tri_up.size());
+      // pressure ILU: earlier lower entries lp whose row holds col[k] above its diagonal
+      const int lp_end = k < dp ? k : dp;
+      for (int lp = b0; lp < lp_end; ++lp) {
+        const int ue = find_in_row_upper(c.h_col[lp], c.h_col[k]);
+        if (ue < 0) continue;
+        pt_lp.push_back(lp);
+        pt_ue.push_back(ue);
+      }
+      pt_ptr[k + 1] = int(pt_lp.size());
+    }
+  }
+  auto up = [](DBuf<int>& b, const std::vector<int>& h) {
+    b.free();
+    b.alloc(h.size());
+    if (!h.empty()) RF_CUDA(cudaMemcpy(b.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  };
+  up(c.d_tri_ptr, tri_ptr);
+  up(c.d_tri_up, tri_up);
+  up(c.d_tri_ip, tri_ip);
+  up(c.d_pt_ptr, pt_ptr);
+  up(c.d_pt_lp, pt_lp);
+  up(c.d_pt_ue, pt_ue);
+}
+
 void build_levels(Ctx& c) {
   const int n = c.n;
   std::vector<int> lvl(n, 0);
@@ -2661,6 +2798,7 @@ void setup_linear_workspace(Ctx& c) {
   // the largest cluster (16 CTAs, non-portable; else 8) that every level-scheduled kernel can run
   set_cluster_size(c, auto_cluster_size(c));
   build_level_plan(c);
+  build_factor_recipes(c);
   const int nt = 1 + c.topo.max_perfs_per_well;
   const size_t smem = sizeof(double) * (2 * size_t(nt) * nt + 2 * nt);
   if (smem > 48 * 1024) raise_dynamic_smem((const void*)k_schur, smem);
