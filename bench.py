@@ -101,6 +101,8 @@ def parse():
                     help="ensemble: JSON table of tuned cluster sizes (ressim_b200.autotune) applied per variant")
     ap.add_argument("--tune-variants", type=int, default=0,
                     help="ensemble: first tune this many variants spread over the size range into --cluster-table")
+    ap.add_argument("--host-threads", type=int, default=0,
+                    help="ensemble: host threads, one per group of variants (0: the library's default)")
     ap.add_argument("--batch-mode", choices=["groups", "threads"], default="groups",
                     help="ensemble: fiber groups with batched level-scheduled launches, or a thread per variant")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -531,7 +533,7 @@ def run_ensemble(args, rank, world):
         pg.barrier()
 
     def make_ensemble():
-        e = Ensemble(ds, precision=args.precision)
+        e = Ensemble(ds, precision=args.precision, host_threads=args.host_threads)
         e.set_mode(args.batch_mode)
         nonlocal tuned
         if args.cluster_table and os.path.exists(args.cluster_table):
