@@ -968,7 +968,9 @@ def main():
         bytes_launch = bicgstab_bytes_per_iteration(n, nnzb) * iters / launches_b
         ms_launch = kernel_ms / launches_b
         achieved = bytes_launch / (ms_launch / 1e3) / 1e9
-        roof = {"kernel": "k_bicgstab_cluster", "bound": "hbm", "achieved": achieved, "peak": peak,
+        kname = ("k_bicgstab_level (one thread block, level order)" if prof.get("level_kernels")
+                 else "k_bicgstab_dsmem / k_bicgstab_cluster (one thread-block cluster)")
+        roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                 "bytes_per_launch": bytes_launch, "ms_per_launch": ms_launch,
                 "iterations_per_launch": iters / launches_b,

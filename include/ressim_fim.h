@@ -260,7 +260,8 @@ int64_t rf_kernel_launches(const RfCtx* ctx);
  * out (may be NULL) receives up to n values, read before the enable/reset below take effect:
  * ms for assembly, well elimination, CPR build, pressure stage, block-ILU0 smoother, Krylov,
  * update, the BiCGStab kernel alone, the direct LU route; then the BiCGStab iteration total, the number of BiCGStab
- * launches timed, and the block count of the reduced matrix.
+ * launches timed, the block count of the reduced matrix, and 1 when the level-order kernels serve
+ * the pressure stage (0: the cluster kernels).
  * enable > 0 switches the profiler on, 0 off, < 0 leaves it as is; reset != 0 zeroes the totals. */
 int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32_t n);
 

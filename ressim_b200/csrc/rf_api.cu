@@ -1608,6 +1608,7 @@ int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32
       if (n > rf::kPhCount) out[rf::kPhCount] = double(it);
       if (n > rf::kPhCount + 1) out[rf::kPhCount + 1] = double(c.phase_count[rf::kPhBicgKernel]);
       if (n > rf::kPhCount + 2) out[rf::kPhCount + 2] = double(c.nnzb);
+      if (n > rf::kPhCount + 3) out[rf::kPhCount + 3] = rf::level_solver_active(c) ? 1.0 : 0.0;
     }
     if (enable >= 0) c.profiling = enable > 0;
     if (reset) {

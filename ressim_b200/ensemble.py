@@ -71,7 +71,7 @@ class Ensemble:
         return sum(int(L.rf_kernel_launches(c)) for c in self._ctx)
 
     def profile(self, i: int, enable=None, reset=False) -> dict:
-        out = np.zeros(len(_lib.PHASES) + 3)
+        out = np.zeros(len(_lib.PHASES) + 4)
         en = -1 if enable is None else int(bool(enable))
         _lib.load().rf_profile(self._ctx[i], en, int(reset), _ptr(out), len(out))
         d = {k: float(v) for k, v in zip(_lib.PHASES, out)}
@@ -79,6 +79,7 @@ class Ensemble:
         d["bicgstab_iterations"] = int(out[k])
         d["bicgstab_launches"] = int(out[k + 1])
         d["nnzb"] = int(out[k + 2])
+        d["level_kernels"] = bool(out[k + 3])
         return d
 
     def set_mode(self, mode: str) -> None:

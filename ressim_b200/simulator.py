@@ -135,7 +135,7 @@ class ReservoirSimulator(Deck):
     def profile(self, enable=None, reset=False) -> dict:
         """Phase timings (ms, CUDA events) and the BiCGStab iteration total; `enable` switches the
         profiler on/off."""
-        out = np.zeros(len(_lib.PHASES) + 3)
+        out = np.zeros(len(_lib.PHASES) + 4)
         en = -1 if enable is None else int(bool(enable))
         rc = _lib.load().rf_profile(self._context(), en, int(reset), _ptr(out), len(out))
         if rc != _abi.RF_OK:
@@ -145,6 +145,7 @@ class ReservoirSimulator(Deck):
         d["bicgstab_iterations"] = int(out[k])
         d["bicgstab_launches"] = int(out[k + 1])
         d["nnzb"] = int(out[k + 2])
+        d["level_kernels"] = bool(out[k + 3])
         return d
 
     def set_linear_precision(self, mode: str) -> None:
