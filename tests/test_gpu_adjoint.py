@@ -105,7 +105,9 @@ def test_adjoint_gradient_matches_finite_differences(kind):
         h = 1e-4
         fo = (oracle_objective(perturbed(deck, h * e), steps, dt) -
               oracle_objective(perturbed(deck, -h * e), steps, dt)) / (2 * h)
-        print(f"cell {i}: oracle fd {fo:.8e}, adjoint rel {abs(g[i] - fo) / max(abs(fo), 1e-3 * gscale):.2e}")
+        ref_err = abs(g[i] - fo) / max(abs(fo), 1e-3 * gscale)
+        print(f"cell {i}: oracle fd {fo:.8e}, adjoint rel {ref_err:.2e}")
+        assert ref_err < 1e-4, (int(i), g[i], fo)
     v = rng.standard_normal(n)
     fd = fd_lnk(deck, v, steps, dt)
     dd = float(g @ v)
