@@ -185,8 +185,9 @@ __host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
 // level l + 2 while it sweeps level l (levels l+1..l+3 are final then), with the dot products of
 // SP (0: acc0 += rh . spout; 1: acc0 += spout . spout, acc1 += spout . s).
 template <class T, int SP>
-__device__ __forceinline__ void fused_spmv_compute(const LvlArgs<T>& a, const T* S, int q, const SRec<T>& r, T dotw,
-                                                   T* spout, double& acc0, double& acc1) {
+__device__ __forceinline__ void fused_spmv_row(const LvlArgs<T>& a, const T* S, int q, T* spout, double& acc0,
+                                               double& acc1) {
+  const SRec<T>& r = a.srec[q];
   if (r.idx[7]) return;  // after the sweep
   T x[kSpK];
 #pragma unroll
@@ -196,22 +197,12 @@ __device__ __forceinline__ void fused_spmv_compute(const LvlArgs<T>& a, const T*
   for (int j = 0; j < kSpK; ++j) s += r.v[j] * x[j];  // absent entries: 0 * 0, exact no-ops
   spout[q] = s;
   if (SP == 0) {
-    acc0 += double(dotw) * double(s);
+    acc0 += double(a.rh[q]) * double(s);
   } else {
     const double ti = double(s);
     acc0 += ti * ti;
-    acc1 += ti * double(dotw);
+    acc1 += ti * double(a.s[q]);
   }
-}
-// the weight of the row's dot product: rh (SP 0) or s (SP 1)
-template <class T, int SP>
-__device__ __forceinline__ T spmv_dotw(const LvlArgs<T>& a, int q) {
-  return SP == 0 ? a.rh[q] : a.s[q];
-}
-template <class T, int SP>
-__device__ __forceinline__ void fused_spmv_row(const LvlArgs<T>& a, const T* S, int q, T* spout, double& acc0,
-                                               double& acc1) {
-  fused_spmv_compute<T, SP>(a, S, q, a.srec[q], spmv_dotw<T, SP>(a, q), spout, acc0, acc1);
 }
 
 template <class T, int MODE, int SP = 0>
@@ -279,18 +270,9 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
       rstride = RB;
     }
     T* cur = S + size_t(l & 3) * W;
-    // the backward sweep's product rows of level l + 2: the first one's loads are issued before
-    // the sweep rows, so their latency overlaps the sweep's arithmetic
-    int sq = 1 << 30, sq_end = 0;
-    SRec<T> sr;
-    T sw = T(0);
-    if (MODE == 2 && l + 2 < L) {
-      sq = sl[l + 2] + t;
-      sq_end = sl[l + 3];
-      if (sq < sq_end) {
-        sr = a.srec[sq];
-        sw = spmv_dotw<T, SP>(a, sq);
-      }
+    if (MODE == 2 && l + 2 < L) {  // the product rows of level l + 2
+      const int m0 = sl[l + 2], m1 = sl[l + 3];
+      for (int q = m0 + t; q < m1; q += NT) fused_spmv_row<T, SP>(a, S, q, spout, sa0, sa1);
     }
     for (int off = t; off < w; off += NT) {
       const int q = lst + off;
@@ -332,10 +314,6 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
       out[q] = s;
       const unsigned fs = meta >> 3;
       if (fs) far[fs - 1] = s;
-    }
-    if (MODE == 2 && sq < sq_end) {
-      fused_spmv_compute<T, SP>(a, S, sq, sr, sw, spout, sa0, sa1);
-      for (int q = sq + NT; q < sq_end; q += NT) fused_spmv_row<T, SP>(a, S, q, spout, sa0, sa1);
     }
     __syncthreads();
   }
