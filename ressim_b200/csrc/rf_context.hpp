@@ -73,17 +73,14 @@ struct LevelPlan {
   DBuf<unsigned long long> d_fword, d_bword;
   DBuf<unsigned short> d_flong_abs, d_blong_abs;
   DBuf<unsigned char> d_frec, d_brec;
-  // pressure matrix in position space: window indices of the rows fused into the backward sweep
-  // (two 64-bit words per position), their records after packing, and the other rows as CSR
-  DBuf<unsigned long long> d_sidx;
-  DBuf<unsigned char> d_srec;
-  DBuf<int> d_sptail, d_sptail_ptr, d_sptail_col;
-  int n_sptail = 0, n_sptail_entries = 0;
+  // pressure matrix in position space: [7][n] fixed-width columns, longer rows separately
+  DBuf<int> d_sp_col, d_splong_row, d_splong_ptr, d_splong_col;
+  int n_splong = 0, n_splong_entries = 0;
   // gather maps of the value packing: packed value i = T(src[map[i]]) (0 when map[i] < 0)
   //   factor map over plu: [fwd 3n | bwd 3n | fwd long | bwd long]; matrix map over pval:
-  //   [fused rows 7n | tail rows]
+  //   [fixed width 7n | longer rows]
   DBuf<int> d_fmap, d_smap;
-  DBuf<double> d_vals64;  // [fwd 3n | bwd 3n | fwd long | bwd long | piv n | matrix 7n | tail rows]
+  DBuf<double> d_vals64;  // [fwd 3n | bwd 3n | fwd long | bwd long | piv n | matrix 7n | longer rows]
   DBuf<float> d_vals32;
   DBuf<unsigned char> d_work;  // BiCGStab vectors in position order (9 x T) and x (double)
   size_t work_bytes = 0;

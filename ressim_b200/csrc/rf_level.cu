@@ -38,7 +38,6 @@ constexpr int kLvlMaxStages = 4;
 constexpr unsigned kFarBit = 0x8000u;
 constexpr unsigned kLongCnt = 7u;
 constexpr int kSpK = 7;  // pressure-matrix entries per row held in the fixed-width layout
-constexpr int kWin = 4;  // level windows in shared memory (the fused SpMV reads three levels)
 
 __device__ __forceinline__ unsigned smem_u32a(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -82,15 +81,6 @@ struct alignas(16) BRec {
   T piv;
 };
 
-// Pressure-matrix row fused into the backward sweep: shared-memory indices of its (at most 7)
-// entries' columns in column order (absent: the zero slot; idx[7] != 0: the row is done after the
-// sweep from global memory instead), and the values.
-template <class T>
-struct alignas(16) SRec {
-  unsigned short idx[8];
-  T v[kSpK];
-};
-
 template <class T>
 struct LvlArgs {
   int n, L, width, stages, nfar;
@@ -104,20 +94,21 @@ struct LvlArgs {
   const unsigned short* flong_code;
   const int* blong_ptr;
   const unsigned short* blong_code;
-  // pressure-matrix rows that are not fused into the backward sweep (they read rows beyond the
-  // level window: the wells' fill): positions, CSR of column positions and values
-  int n_sptail;
-  const int* sptail;
-  const int* sptail_ptr;
-  const int* sptail_col;
+  // pressure matrix in position space: rows of at most kSpK entries as [kSpK][n] column positions
+  // (-1: no entry; -2 in slot 0: a longer row, listed separately) and values, in column order
+  const int* sp_col;
+  int n_splong;
+  const int* splong_row;  // [n_splong] positions of the longer rows
+  const int* splong_ptr;  // [n_splong + 1]
+  const int* splong_col;
   const FRec<T>* frec;  // [n] forward records
   const BRec<T>* brec;  // [n] backward records
   const unsigned short* flong_abs;  // long rows' dependency indices into S
   const unsigned short* blong_abs;
   const T* flong_val;
   const T* blong_val;
-  const T* sptail_val;
-  const SRec<T>* srec;  // [n] fused SpMV rows
+  const T* spval;    // [kSpK][n]
+  const T* splongval;
   const double* rhs;  // natural order
   double* x;          // natural order
   double* xq;         // the iterate in position order
@@ -180,35 +171,10 @@ __host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
 // its squares summed into acc; MODE 2: backward sweep of y.  The result goes to `out` (position
 // order).  Each thread handles the offsets t, t + NT, ... of every level and stages exactly those
 // offsets' data, so the staging needs no barrier of its own.  S holds the window of level l at
-// S[(l & 3) W ..], the far cache at S[4W ..] and the zero slot after it; sl is the level pointers.
-// The backward sweep also computes the pressure-matrix product of its output, spout = A out, for
-// level l + 2 while it sweeps level l (levels l+1..l+3 are final then), with the dot products of
-// SP (0: acc0 += rh . spout; 1: acc0 += spout . spout, acc1 += spout . s).
-template <class T, int SP>
-__device__ __forceinline__ void fused_spmv_row(const LvlArgs<T>& a, const T* S, int q, T* spout, double& acc0,
-                                               double& acc1) {
-  const SRec<T>& r = a.srec[q];
-  if (r.idx[7]) return;  // after the sweep
-  T x[kSpK];
-#pragma unroll
-  for (int j = 0; j < kSpK; ++j) x[j] = S[r.idx[j]];
-  T s = T(0);
-#pragma unroll
-  for (int j = 0; j < kSpK; ++j) s += r.v[j] * x[j];  // absent entries: 0 * 0, exact no-ops
-  spout[q] = s;
-  if (SP == 0) {
-    acc0 += double(a.rh[q]) * double(s);
-  } else {
-    const double ti = double(s);
-    acc0 += ti * ti;
-    acc1 += ti * double(a.s[q]);
-  }
-}
-
-template <class T, int MODE, int SP = 0>
+// S[(l & 1) W ..], the far cache at S[2W ..] and the zero slot after it; sl is the level pointers.
+template <class T, int MODE>
 __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const int* sl, T* out, double& acc,
-                          double beta, double omega, double alpha, bool first, T* spout = nullptr,
-                          double* sacc = nullptr) {
+                          double beta, double omega, double alpha, bool first) {
   constexpr bool FWD = MODE != 2;
   constexpr size_t RB = FWD ? sizeof(FRec<T>) : sizeof(BRec<T>);
   constexpr size_t RMAX = sizeof(BRec<T>);
@@ -248,8 +214,7 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
     }
     s_iss = D - 1;
   }
-  T* far = S + size_t(kWin) * W;
-  double sa0 = 0.0, sa1 = 0.0;
+  T* far = S + 2 * size_t(W);
   for (int k = 0; k < L; ++k) {
     const int l = level_at(k), lst = sl[l], w = sl[l + 1] - lst;
     const unsigned char* rbase;
@@ -269,11 +234,7 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
       inp = nullptr;
       rstride = RB;
     }
-    T* cur = S + size_t(l & 3) * W;
-    if (MODE == 2 && l + 2 < L) {  // the product rows of level l + 2
-      const int m0 = sl[l + 2], m1 = sl[l + 3];
-      for (int q = m0 + t; q < m1; q += NT) fused_spmv_row<T, SP>(a, S, q, spout, sa0, sa1);
-    }
+    T* cur = S + size_t(l & 1) * W;
     for (int off = t; off < w; off += NT) {
       const int q = lst + off;
       const unsigned char* rp = rbase + size_t(off) * rstride;
@@ -318,26 +279,48 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
     __syncthreads();
   }
   if (D > 0) cp_wait<0>();
-  if (MODE == 2) {
-    // the product rows of levels 1 and 0, then the rows that read beyond the window (well fill,
-    // longer rows) from global memory; the sweep's last barrier made its output visible
-    for (int m = L < 2 ? L - 1 : 1; m >= 0; --m)
-      for (int q = sl[m] + t; q < sl[m + 1]; q += NT) fused_spmv_row<T, SP>(a, S, q, spout, sa0, sa1);
-    for (int e = t; e < a.n_sptail; e += NT) {
-      const int q = a.sptail[e];
-      T s = T(0);
-      for (int k = a.sptail_ptr[e]; k < a.sptail_ptr[e + 1]; ++k) s += a.sptail_val[k] * out[a.sptail_col[k]];
-      spout[q] = s;
-      if (SP == 0) {
-        sa0 += double(a.rh[q]) * double(s);
-      } else {
-        const double ti = double(s);
-        sa0 += ti * ti;
-        sa1 += ti * double(a.s[q]);
-      }
+}
+
+// out = A in (pressure matrix, position space), with the dot products the solve needs next:
+// MODE 0: acc0 += rh . out;  MODE 1: acc0 += out . out, acc1 += out . s.  A row's entries are
+// loaded together (fixed-width layout, coalesced across the warp) and summed in column order.
+template <class T, int MODE>
+__device__ __forceinline__ void spmv_row_done(const LvlArgs<T>& a, int q, T s, T* out, double& acc0, double& acc1) {
+  out[q] = s;
+  if (MODE == 0) {
+    acc0 += double(a.rh[q]) * double(s);
+  } else {
+    const double ti = double(s);
+    acc0 += ti * ti;
+    acc1 += ti * double(a.s[q]);
+  }
+}
+template <class T, int MODE>
+__device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0, double& acc1) {
+  const int NT = a.threads, n = a.n;
+  const int t0 = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);
+  for (int q = t0; q < n; q += NT) {
+    int c[kSpK];
+    T v[kSpK], x[kSpK];
+#pragma unroll
+    for (int j = 0; j < kSpK; ++j) {
+      c[j] = a.sp_col[size_t(j) * n + q];
+      v[j] = a.spval[size_t(j) * n + q];
     }
-    sacc[0] += sa0;
-    sacc[1] += sa1;
+    if (c[0] == -2) continue;  // a longer row: below
+#pragma unroll
+    for (int j = 0; j < kSpK; ++j) x[j] = c[j] >= 0 ? in[c[j]] : T(0);
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < kSpK; ++j)
+      if (c[j] >= 0) s += v[j] * x[j];
+    spmv_row_done<T, MODE>(a, q, s, out, acc0, acc1);
+  }
+  for (int e = t0; e < a.n_splong; e += NT) {
+    const int q = a.splong_row[e];
+    T s = T(0);
+    for (int k = a.splong_ptr[e]; k < a.splong_ptr[e + 1]; ++k) s += a.splongval[k] * in[a.splong_col[k]];
+    spmv_row_done<T, MODE>(a, q, s, out, acc0, acc1);
   }
 }
 
@@ -350,9 +333,9 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
   const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   unsigned char* stage = lvl_smem;
   T* S = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * lvl_slot_bytes<T>(W));
-  int* sl = reinterpret_cast<int*>(S + size_t(kWin) * W + a.nfar + 1);
+  int* sl = reinterpret_cast<int*>(S + 2 * size_t(W) + a.nfar + 1);
   for (int l = threadIdx.x; l <= a.L; l += blockDim.x) sl[l] = a.lstart[l];
-  if (threadIdx.x == 0) S[size_t(kWin) * W + a.nfar] = T(0);  // the zero slot
+  if (threadIdx.x == 0) S[2 * size_t(W) + a.nfar] = T(0);  // the zero slot
   double d0 = 0.0, d1 = 0.0;
   for (int q = t; q < n; q += NT) {
     const double ri = a.rhs[a.pos_row[q]] - 0.0;
@@ -376,11 +359,9 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     const double beta = it == 0 ? 0.0 : (rho / rho_prev) * (alpha / omega);
     d0 = 0.0;
     d1 = 0.0;
-    double sp[2] = {0.0, 0.0};
     lvl_sweep<T, 0>(a, stage, S, sl, a.y, d0, beta, omega, 0.0, it == 0);
-    lvl_sweep<T, 2, 0>(a, stage, S, sl, a.ph, d0, 0.0, 0.0, 0.0, false, a.v, sp);  // and v = A ph
-    d0 = sp[0];
-    d1 = sp[1];
+    lvl_sweep<T, 2>(a, stage, S, sl, a.ph, d0, 0.0, 0.0, 0.0, false);
+    lvl_spmv<T, 0>(a, a.ph, a.v, d0, d1);
     block_sum2(d0, d1, red);
     const double vd = d0;
     if (!isfinite(vd) || fabs(vd) < kEpsL) break;
@@ -393,10 +374,10 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
       for (int q = t; q < n; q += NT) a.xq[q] += alpha * double(a.ph[q]);
       break;
     }
-    sp[0] = sp[1] = 0.0;
-    lvl_sweep<T, 2, 1>(a, stage, S, sl, a.sh, d0, 0.0, 0.0, 0.0, false, a.t, sp);  // and t = A sh
-    d0 = sp[0];
-    d1 = sp[1];
+    lvl_sweep<T, 2>(a, stage, S, sl, a.sh, d0, 0.0, 0.0, 0.0, false);
+    d0 = 0.0;
+    d1 = 0.0;
+    lvl_spmv<T, 1>(a, a.sh, a.t, d0, d1);
     block_sum2(d0, d1, red);
     const double tt = d0;
     if (!isfinite(tt) || tt <= kEpsL) break;
@@ -622,33 +603,15 @@ __global__ void k_lvl_pack_rec(int n, const unsigned long long* __restrict__ fwo
   brec[q] = b;
 }
 
-// The fused product rows: static window indices and the gathered matrix values.
-template <class T>
-__global__ void k_lvl_pack_srec(int n, const unsigned long long* __restrict__ sidx, const T* __restrict__ sp,
-                                SRec<T>* __restrict__ srec) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  SRec<T> r;
-  const unsigned long long w0 = sidx[2 * size_t(q)], w1 = sidx[2 * size_t(q) + 1];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    r.idx[j] = static_cast<unsigned short>(w0 >> (16 * j));
-    r.idx[4 + j] = static_cast<unsigned short>(w1 >> (16 * j));
-  }
-#pragma unroll
-  for (int j = 0; j < kSpK; ++j) r.v[j] = sp[size_t(j) * n + q];
-  srec[q] = r;
-}
-
 template <class T>
 size_t lvl_smem_bytes(int W, int stages, int nfar, int L) {
-  const size_t win = ((size_t(kWin) * W + size_t(nfar) + 1) * sizeof(T) + 15) / 16 * 16;
+  const size_t win = ((2 * size_t(W) + size_t(nfar) + 1) * sizeof(T) + 15) / 16 * 16;
   return size_t(stages) * lvl_slot_bytes<T>(W) + win + sizeof(int) * (size_t(L) + 1);
 }
 
 // offsets of the packed value segments (elements)
 struct LvlSeg {
-  size_t fval, bval, flong, blong, piv, sp, sptail, total;
+  size_t fval, bval, flong, blong, piv, sp, splong, total;
 };
 LvlSeg lvl_segments(const LevelPlan& P, int n) {
   LvlSeg s;
@@ -658,8 +621,8 @@ LvlSeg lvl_segments(const LevelPlan& P, int n) {
   s.blong = s.flong + size_t(P.n_flong);
   s.piv = s.blong + size_t(P.n_blong);
   s.sp = s.piv + size_t(n);
-  s.sptail = s.sp + size_t(kSpK) * n;
-  s.total = s.sptail + size_t(P.n_sptail_entries);
+  s.splong = s.sp + size_t(kSpK) * n;
+  s.total = s.splong + size_t(P.n_splong_entries);
   return s;
 }
 
@@ -783,10 +746,10 @@ void build_level_plan(Ctx& c) {
     pack_row(false, q, rows[q]);
   }
   if (flong_ptr.size() > 65536 || blong_ptr.size() > 65536) return;
-  // the pressure sweeps' words: dependency indices into S (window of level lc at (lc & 3) W, far
-  // cache at 4W, zero slot at 4W + nfar)
+  // the pressure sweeps' words: dependency indices into S (window of level lc at (lc & 1) W, far
+  // cache at 2W, zero slot at 2W + nfar)
   const int nfar = std::max(nff, nfb);
-  const unsigned zero_slot = unsigned(kWin * W + nfar);
+  const unsigned zero_slot = unsigned(2 * W + nfar);
   if (zero_slot >= 65535u) return;
   std::vector<unsigned long long> fword(n), bword(n);
   std::vector<unsigned short> flong_abs, blong_abs;
@@ -798,8 +761,8 @@ void build_level_plan(Ctx& c) {
       const int k1 = fwd ? c.h_diag[r] : c.h_row_ptr[r + 1];
       auto abs_of = [&](int col) -> unsigned {
         const int lc = lvl[col];
-        if (lc == (fwd ? l - 1 : l + 1)) return unsigned((lc & 3) * W + pos[col] - lp[lc]);
-        return unsigned(kWin * W + (fwd ? ffar[col] : bfar[col]));
+        if (lc == (fwd ? l - 1 : l + 1)) return unsigned((lc & 1) * W + pos[col] - lp[lc]);
+        return unsigned(2 * W + (fwd ? ffar[col] : bfar[col]));
       };
       const unsigned long long code = (fwd ? fcode : bcode)[q];
       const unsigned meta = unsigned(code >> 48);
@@ -826,51 +789,33 @@ void build_level_plan(Ctx& c) {
   P.nnz = c.h_row_ptr[n];
   fmap.insert(fmap.end(), flong_map.begin(), flong_map.end());
   fmap.insert(fmap.end(), blong_map.begin(), blong_map.end());
-  // the pressure matrix for the product fused into the backward sweep: per position the window
-  // indices of its entries (rows of at most kSpK entries whose neighbours all lie in the adjacent
-  // levels) or a flag sending the row to the tail list, computed from global memory after the
-  // sweep; smap gathers the values: [kSpK][n] fused slots, then the tail rows' entries
-  std::vector<unsigned long long> sidx(2 * size_t(n), 0);
-  std::vector<int> smap(size_t(kSpK) * n, -1), sptail, sptail_ptr{0}, sptail_col, sptail_map, f0(n), b0(n);
+  // pressure matrix in position space: fixed-width rows, longer rows separately; smap gathers the
+  // values: [kSpK][n] fixed-width slots, then the longer rows' entries
+  std::vector<int> sp_col(size_t(kSpK) * n, -1), smap(size_t(kSpK) * n, -1), splong_row, splong_ptr{0},
+      splong_col, splong_map, f0(n), b0(n);
   for (int q = 0; q < n; ++q) {
-    const int r = rows[q], l = lvl[r];
+    const int r = rows[q];
     const int k0 = c.h_row_ptr[r], k1 = c.h_row_ptr[r + 1];
-    bool fused = k1 - k0 <= kSpK;
-    unsigned short idx[8];
-    for (int j = 0; j < 8; ++j) idx[j] = static_cast<unsigned short>(zero_slot);
-    idx[7] = 0;
-    for (int k = k0; k < k1 && fused; ++k) {
-      const int col = c.h_col[k], lc = lvl[col];
-      if (lc < l - 1 || lc > l + 1 || (lc == l && col != r)) {
-        fused = false;
-        break;
-      }
-      idx[k - k0] = static_cast<unsigned short>((lc & 3) * W + pos[col] - lp[lc]);
-    }
-    if (fused) {
-      for (int k = k0; k < k1; ++k) smap[size_t(k - k0) * n + q] = k;
-    } else {
-      idx[7] = 1;
-      sptail.push_back(q);
+    if (k1 - k0 <= kSpK) {
       for (int k = k0; k < k1; ++k) {
-        sptail_col.push_back(pos[c.h_col[k]]);
-        sptail_map.push_back(k);
+        sp_col[size_t(k - k0) * n + q] = pos[c.h_col[k]];
+        smap[size_t(k - k0) * n + q] = k;
       }
-      sptail_ptr.push_back(int(sptail_col.size()));
+    } else {
+      sp_col[q] = -2;
+      splong_row.push_back(q);
+      for (int k = k0; k < k1; ++k) {
+        splong_col.push_back(pos[c.h_col[k]]);
+        splong_map.push_back(k);
+      }
+      splong_ptr.push_back(int(splong_col.size()));
     }
-    unsigned long long w0 = 0, w1 = 0;
-    for (int j = 0; j < 4; ++j) {
-      w0 |= (unsigned long long)idx[j] << (16 * j);
-      w1 |= (unsigned long long)idx[4 + j] << (16 * j);
-    }
-    sidx[2 * size_t(q)] = w0;
-    sidx[2 * size_t(q) + 1] = w1;
     f0[q] = c.h_row_ptr[r];
     b0[q] = c.h_diag[r] + 1;
   }
-  P.n_sptail = int(sptail.size());
-  P.n_sptail_entries = int(sptail_col.size());
-  smap.insert(smap.end(), sptail_map.begin(), sptail_map.end());
+  P.n_splong = int(splong_row.size());
+  P.n_splong_entries = int(splong_col.size());
+  smap.insert(smap.end(), splong_map.begin(), splong_map.end());
   auto up_i = [](DBuf<int>& b, const std::vector<int>& h) {
     b.free();
     b.alloc(h.size());
@@ -902,12 +847,10 @@ void build_level_plan(Ctx& c) {
   P.d_brec.free();
   P.d_frec.alloc(size_t(n) * sizeof(FRec<double>));
   P.d_brec.alloc(size_t(n) * sizeof(BRec<double>));
-  up_u64(P.d_sidx, sidx);
-  up_i(P.d_sptail, sptail);
-  up_i(P.d_sptail_ptr, sptail_ptr);
-  up_i(P.d_sptail_col, sptail_col);
-  P.d_srec.free();
-  P.d_srec.alloc(size_t(n) * sizeof(SRec<double>));
+  up_i(P.d_sp_col, sp_col);
+  up_i(P.d_splong_row, splong_row);
+  up_i(P.d_splong_ptr, splong_ptr);
+  up_i(P.d_splong_col, splong_col);
   up_i(P.d_fmap, fmap);
   up_i(P.d_smap, smap);
   up_i(P.d_blk_f0, f0);
@@ -929,8 +872,8 @@ void build_level_plan(Ctx& c) {
 
 void free_level_plan(Ctx& c) {
   LevelPlan& P = c.lvl;
-  for (auto* b : {&P.d_lstart, &P.d_pos_row, &P.d_flong_ptr, &P.d_blong_ptr, &P.d_sptail, &P.d_sptail_ptr,
-                  &P.d_sptail_col, &P.d_fmap, &P.d_smap, &P.d_blk_f0, &P.d_blk_b0})
+  for (auto* b : {&P.d_lstart, &P.d_pos_row, &P.d_flong_ptr, &P.d_blong_ptr, &P.d_sp_col, &P.d_splong_row,
+                  &P.d_splong_ptr, &P.d_splong_col, &P.d_fmap, &P.d_smap, &P.d_blk_f0, &P.d_blk_b0})
     b->free();
   P.d_fcode.free();
   P.d_bcode.free();
@@ -942,8 +885,6 @@ void free_level_plan(Ctx& c) {
   P.d_blong_abs.free();
   P.d_frec.free();
   P.d_brec.free();
-  P.d_sidx.free();
-  P.d_srec.free();
   P.d_vals64.free();
   P.d_vals32.free();
   P.d_work.free();
@@ -976,7 +917,7 @@ void level_pack(Ctx& c) {
   const int n = c.n;
   const LvlSeg g = lvl_segments(P, n);
   const long long mf = (long long)g.piv;                    // factor entries: fval, bval, long rows
-  const long long ms = (long long)(g.total - g.sp);           // matrix entries: fused slots, tail rows
+  const long long ms = (long long)(g.total - g.sp);           // matrix entries: fixed width, longer rows
   if (c.precision == 1) {
     if (!P.d_vals32.p) P.d_vals32.alloc(g.total);
     float* v = P.d_vals32.p;
@@ -986,8 +927,6 @@ void level_pack(Ctx& c) {
     k_lvl_pack_rec<float><<<blocks_for(n), kBlock, 0, c.stream>>>(
         n, P.d_fword.p, P.d_bword.p, v + g.fval, v + g.bval, v + g.piv, reinterpret_cast<FRec<float>*>(P.d_frec.p),
         reinterpret_cast<BRec<float>*>(P.d_brec.p));
-    k_lvl_pack_srec<float><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_sidx.p, v + g.sp,
-                                                                     reinterpret_cast<SRec<float>*>(P.d_srec.p));
     P.packed = 1;
   } else {
     if (!P.d_vals64.p) P.d_vals64.alloc(g.total);
@@ -998,11 +937,9 @@ void level_pack(Ctx& c) {
     k_lvl_pack_rec<double><<<blocks_for(n), kBlock, 0, c.stream>>>(
         n, P.d_fword.p, P.d_bword.p, v + g.fval, v + g.bval, v + g.piv, reinterpret_cast<FRec<double>*>(P.d_frec.p),
         reinterpret_cast<BRec<double>*>(P.d_brec.p));
-    k_lvl_pack_srec<double><<<blocks_for(n), kBlock, 0, c.stream>>>(n, P.d_sidx.p, v + g.sp,
-                                                                      reinterpret_cast<SRec<double>*>(P.d_srec.p));
     P.packed = 0;
   }
-  c.launches += 5;
+  c.launches += 4;
 }
 
 static_assert(sizeof(LvlArgs<double>) <= kBatchArgBytes && sizeof(BlkArgs<double>) <= kBatchArgBytes,
@@ -1070,10 +1007,11 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.flong_code = P.d_flong_code.p;
   a.blong_ptr = P.d_blong_ptr.p;
   a.blong_code = P.d_blong_code.p;
-  a.n_sptail = P.n_sptail;
-  a.sptail = P.d_sptail.p;
-  a.sptail_ptr = P.d_sptail_ptr.p;
-  a.sptail_col = P.d_sptail_col.p;
+  a.sp_col = P.d_sp_col.p;
+  a.n_splong = P.n_splong;
+  a.splong_row = P.d_splong_row.p;
+  a.splong_ptr = P.d_splong_ptr.p;
+  a.splong_col = P.d_splong_col.p;
   a.frec = reinterpret_cast<const FRec<T>*>(P.d_frec.p);
   a.brec = reinterpret_cast<const BRec<T>*>(P.d_brec.p);
   a.flong_abs = P.d_flong_abs.p;
@@ -1081,8 +1019,8 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.nfar = std::max(P.nfar_f, P.nfar_b);
   a.flong_val = vals + g.flong;
   a.blong_val = vals + g.blong;
-  a.sptail_val = vals + g.sptail;
-  a.srec = reinterpret_cast<const SRec<T>*>(P.d_srec.p);
+  a.spval = vals + g.sp;
+  a.splongval = vals + g.splong;
   a.rhs = rhs;
   a.x = x;
   double* xq = reinterpret_cast<double*>(P.d_work.p);
