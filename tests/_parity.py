@@ -45,15 +45,19 @@ NEWTON_TOL_P, NEWTON_TOL_SW = 1e-4, 2e-3
 def check_within_floor(step, p, sw, newton, runs, rtol=1e-6, state=None):
     """Device fields within three times the rounding floor plus `rtol` while every report step so
     far took the oracle's Newton count; within the Newton tolerance after a step that did not.
-    Newton count within one.  `state` (a dict carried across steps) records the divergence."""
+    Newton count within one of the range the oracle itself takes under the reordered summations
+    (where the pressure BiCGStab stops at its cap, a changed summation order alone can move a
+    report step's count by more than one).  `state` (a dict carried across steps) records the
+    divergence."""
     state = {} if state is None else state
     p0, sw0, n0 = runs[0][step]
     fp = max(rel_err(runs[m][step][0], p0) for m in runs if m != 0)
     fs = max(rel_err(runs[m][step][1], sw0) for m in runs if m != 0)
     ep, es = rel_err(p, p0), rel_err(sw, sw0)
+    counts = [runs[m][step][2] for m in runs]
     print(f"step {step}: pressure {ep:.2e} (floor {fp:.2e}), sw {es:.2e} (floor {fs:.2e}), "
-          f"newton {newton} vs {n0}")
-    assert abs(newton - n0) <= 1, (step, newton, n0)
+          f"newton {newton} vs {n0} (oracle range {min(counts)}..{max(counts)})")
+    assert min(counts) - 1 <= newton <= max(counts) + 1, (step, newton, counts)
     if newton != n0:
         state["diverged"] = True
     if state.get("diverged"):

@@ -28,6 +28,35 @@ def test_batch_equals_sequential_runs():
     ens.close()
 
 
+@pytest.mark.parametrize("mode,threads", [("groups", 1), ("groups", 2), ("threads", 4)])
+def test_batched_launches_equal_sequential_runs(mode, threads):
+    """Several variants per group: their factorisations, pressure solves and block-ILU0 sweeps run
+    as batched launches (a thread block per variant, the launch sized for the largest); the states
+    equal the variants stepped alone, bit for bit, as do the variants of the thread mode."""
+    ids = (142, 215, 226, 206, 7)  # 3,300 to 6,578 cells
+    ds = [decks.ensemble_variant(i) for i in ids]
+    ens = Ensemble(ds, host_threads=threads)
+    ens.set_mode(mode)
+    ens.batch_profile(enable=True, reset=True)
+    singles = [ReservoirSimulator.from_deck(d) for d in ds]
+    for _ in range(2):
+        reps = ens.step(10.0)
+        for i, s in enumerate(singles):
+            r = s.step(10.0)
+            assert reps[i]["newton_iterations"] == r["newton_iterations"], (mode, i)
+    for i, s in enumerate(singles):
+        a, b = ens.state(i), s.state()
+        assert np.array_equal(a["pressure"], b["pressure"]), (mode, i)
+        assert np.array_equal(a["sat_water"], b["sat_water"]), (mode, i)
+    prof = ens.batch_profile(enable=False, reset=True)
+    print(mode, threads, prof)
+    if mode == "groups":
+        assert prof["pressure_items"] > prof["pressure_launches"] > 0  # launches carried several solves
+    else:
+        assert prof["pressure_launches"] == 0
+    ens.close()
+
+
 def test_batch_variant_matches_oracle():
     """A variant stepped inside a batch against the oracle, within the oracle's rounding floor."""
     d = decks.ensemble_variant(SMALL_VARIANTS[0])
