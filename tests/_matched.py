@@ -35,7 +35,7 @@ def make_deck(spec):
     raise ValueError(spec)
 
 
-def oracle_run(spec, dt, steps, matched=True):
+def oracle_run(spec, dt, steps, matched=True, sum_order=0):
     """The oracle on deck `spec` for `steps` report steps of `dt` days.  Returns (per-step list of
     (state dict, well BHPs, Newton iterations, substeps, rc), rate history)."""
     if ROOT not in sys.path:
@@ -44,12 +44,13 @@ def oracle_run(spec, dt, steps, matched=True):
 
     if matched:
         lib().orc_set_controller_options(0, MATCHED_CNV, MATCHED_MB)
+    lib().orc_set_sum_order(sum_order)
     deck = make_deck(spec)
     o = OracleSimulator(deck)
     out = []
     for _ in range(steps):
         rc, r = o.step(dt)
-        out.append((o.state(), o.well_bhp().copy(), r.newton_iterations, r.substeps, rc))
+        out.append((o.state(), o.well_bhp().copy(), r.newton_iterations, r.substeps, rc, r.retries))
     hist = o.rate_history()
     o.close()
     return out, hist
@@ -59,3 +60,23 @@ def oracle_runs_parallel(jobs):
     """oracle_run over several (spec, dt, steps[, matched]) jobs in spawned processes, in job order."""
     with mp.get_context("spawn").Pool(min(len(jobs), os.cpu_count() or 1)) as pool:
         return pool.starmap(oracle_run, jobs)
+
+
+FLOOR_ORDERS = (2, 61)
+
+
+def oracle_floor_runs(specs, dt, steps, orders=FLOOR_ORDERS):
+    """The oracle at the reference's own tolerances on each deck spec, with the reference's
+    left-to-right dot products and with each interleaved summation order in `orders` (spawned
+    processes).  Returns, per spec, {order: oracle_run output}; the spread over the orders is the
+    reference algorithm's rounding floor on that deck."""
+    jobs = [(spec, dt, steps, False, m) for spec in specs for m in (0, *orders)]
+    res = oracle_runs_parallel(jobs)
+    out, k = [], 0
+    for _ in specs:
+        d = {}
+        for m in (0, *orders):
+            d[m] = res[k]
+            k += 1
+        out.append(d)
+    return out
