@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "rf_fiber.hpp"
@@ -193,8 +194,10 @@ void run_fibers(BatchGroup& g, void (*fn)(void*), void* const* args, int count, 
     if (all_done) break;
     if (ran) continue;
     if (oldest) {
-      // nothing runnable: block on the wait filed first (the group's stream completes in order)
-      cudaEventSynchronize(oldest->ev);
+      // nothing runnable: wait for the wait filed first (the group's stream completes in order),
+      // yielding the core meanwhile (many group threads share the host's cores, and the driver's
+      // own wait spins)
+      while (cudaEventQuery(oldest->ev) == cudaErrorNotReady) std::this_thread::yield();
       continue;
     }
     // every unfinished fiber waits for a batched launch
