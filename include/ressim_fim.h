@@ -243,7 +243,8 @@ int32_t rf_set_cluster_size(RfCtx* ctx, int32_t ctas);
  * cluster of rf_set_cluster_size; RF_PRESSURE_SOLVER_LEVEL runs each as one thread block with its
  * vectors in level order and the sweeps' dependencies in shared memory (`threads` threads,
  * 32..512 in steps of 32, 0 automatic); RF_PRESSURE_SOLVER_AUTO (default) takes the level-order
- * kernels whenever their level window fits shared memory.  Both compute the same preconditioner;
+ * kernels, where their level window fits shared memory, for decks of up to 32,768 cells and for
+ * every variant of an ensemble stepped in RF_BATCH_GROUPS mode, and the cluster kernels otherwise.  Both compute the same preconditioner;
  * the solves differ only in the summation order of their dot products.  Takes effect at the next
  * linear solve; RF_ERR_UNSUPPORTED when the level-order kernels cannot run this deck.  No
  * counterpart in the reference. */

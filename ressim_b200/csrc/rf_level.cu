@@ -901,15 +901,25 @@ void level_plan_reshape(Ctx& c) {
   choose_block_shape<float>(c, 1);
 }
 
+// Automatic choice: the one-block level-order kernels for decks of up to kLevelAutoCells cells and
+// for every variant of a batched ensemble (their launches join the group's batched launches); the
+// cluster kernels for larger single decks, where a level holds more rows than one SM issues
+// quickly (measured crossover between 19k and 40k cells).
+constexpr int kLevelAutoCells = 32768;
+
+static bool level_chosen(const Ctx& c) {
+  if (c.pressure_solver == 2) return true;
+  return c.pressure_solver == 0 && (c.batched || c.n <= kLevelAutoCells);
+}
+
 bool level_solver_active(const Ctx& c) {
   const int f = c.precision == 1 ? 1 : 0;
-  if (!c.lvl.built || !c.lvl.fits[f]) return false;
-  return c.pressure_solver == 2 || c.pressure_solver == 0;
+  return c.lvl.built && c.lvl.fits[f] && level_chosen(c);
 }
 
 bool level_block_sweep_active(const Ctx& c) {
   const int f = c.precision == 1 ? 1 : 0;
-  return c.lvl.built && c.lvl.blk_fits[f] && (c.pressure_solver == 2 || c.pressure_solver == 0);
+  return c.lvl.built && c.lvl.blk_fits[f] && level_chosen(c);
 }
 
 void level_pack(Ctx& c) {
