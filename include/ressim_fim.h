@@ -274,6 +274,17 @@ int32_t rf_profile(RfCtx* ctx, int32_t enable, int32_t reset, double* out, int32
  * the inputs, which finite-difference checks of the adjoint need.  Defaults: 0, 0, 0. */
 int32_t rf_set_controller_options(RfCtx* ctx, int32_t one_substep_per_report_step, double cnv_tol, double mb_tol);
 
+/* Linear refinement; no counterpart in the reference (whose Newton systems get one CPR-FGMRES
+ * solve to 1e-12 + 5e-3 |b|, fim/linear/mod.rs:252-372).  rtol > 0 refines every CPR-FGMRES solve
+ * of the well-eliminated system: x += solve(b - A x), the CPR factors of the first pass reused,
+ * until |b - A x| <= rtol |b| or max_passes solves (0: 12).  With a tight rtol the Newton iterates
+ * no longer depend on the preconditioner's rounding, so two implementations take the same Newton
+ * path; with tight CNV / MB tolerances (rf_set_controller_options) this is the matched profile
+ * used to compare against other implementations at 1e-6.  The direct route for systems of at most
+ * 512 rows is unchanged.  rtol = 0 (default) restores the reference's single solve.  The first
+ * call with rtol > 0 allocates two vectors of 3 x cells doubles. */
+int32_t rf_set_linear_refinement(RfCtx* ctx, double rtol, int32_t max_passes);
+
 /* ---- Discrete adjoint (no counterpart in the reference, which has no adjoint).
  * rf_adjoint_record(ctx, 1) clears the tape and starts recording: every later rf_step checkpoints
  * the simulator state at its start (p, Sw; So, Sg, Rs in three-phase mode; device copies) and

@@ -50,6 +50,7 @@ def lib():
         L.orc_rate_history_len.argtypes = [C.c_void_p]
         L.orc_rate_history_get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(_abi.RfTimePointRates)]
         L.orc_set_controller_options.argtypes = [C.c_int32, C.c_double, C.c_double]
+        L.orc_set_linear_refinement.argtypes = [C.c_double, C.c_int32]
         L.orc_assemble_current.argtypes = [C.c_void_p, C.c_double, _ip, _ip, _dp, _ip, _ip, _dp]
         L.orc_initial_well_state.argtypes = [C.c_void_p, _dp, _dp]
         L.orc_linear_solve_csr.argtypes = [C.c_int32, _ip, _ip, _dp, _dp, C.c_int32, _dp,

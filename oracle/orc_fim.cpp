@@ -707,10 +707,38 @@ static LinReport fgmres(const Csr& m, const std::vector<double>& rhs, const Cpr&
   return rep;
 }
 
+// Test-only refinement of every CPR-FGMRES solve, mirroring the device path's
+// rf_set_linear_refinement (no counterpart in the reference): x += fgmres(b - A x) with the CPR of
+// the first pass until |b - A x| <= g_lin_refine_rtol |b|, at most g_lin_refine_passes solves;
+// 0 keeps the reference's single solve.
+static double g_lin_refine_rtol = 0.0;
+static int g_lin_refine_passes = 12;
+
 static LinReport solve_tail_free(const Csr& m, const std::vector<double>& rhs) {
   Cpr pc;
   pc.build(m);
-  return fgmres(m, rhs, pc);
+  if (g_lin_refine_rtol <= 0.0) return fgmres(m, rhs, pc);
+  const int n = m.n;
+  LinReport rep;
+  rep.rhs_norm = vnorm(rhs);
+  std::vector<double> x(n, 0.0), ax, r(n);
+  for (int pass = 0;; ++pass) {
+    csr_matvec(m, x, ax);
+    for (int i = 0; i < n; ++i) r[i] = rhs[i] - ax[i];
+    const double rn = vnorm(r);
+    rep.final_residual_norm = rn;
+    if (!std::isfinite(rn)) break;
+    if (rn <= g_lin_refine_rtol * rep.rhs_norm || rep.rhs_norm == 0.0) {
+      rep.converged = true;
+      break;
+    }
+    if (pass == g_lin_refine_passes) break;
+    const LinReport in = fgmres(m, r, pc);
+    rep.iterations += in.iterations;
+    for (int i = 0; i < n; ++i) x[i] += in.x[i];
+  }
+  rep.x = x;
+  return rep;
 }
 
 // solve_with_well_elimination (well_schur.rs:70-238, 382-471)

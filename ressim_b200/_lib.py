@@ -52,6 +52,7 @@ def load():
     L.rf_dense_solve_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
                                          C.c_size_t]
     L.rf_set_controller_options.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double]
+    L.rf_set_linear_refinement.argtypes = [C.c_void_p, C.c_double, C.c_int32]
     L.rf_adjoint_record.argtypes = [C.c_void_p, C.c_int32]
     L.rf_backward.argtypes = [C.c_void_p, C.POINTER(_abi.RfObjective), _dp, _dp, _dp, C.c_int32]
     L.rf_well_count.argtypes = [C.c_void_p]
@@ -71,6 +72,7 @@ EXPORTED_SYMBOLS = (
     "rf_profile", "rf_set_linear_precision", "rf_set_cluster_size", "rf_batch_create", "rf_batch_destroy", "rf_batch_size",
     "rf_batch_context", "rf_batch_step", "rf_dense_solve_noalloc", "rf_set_controller_options", "rf_adjoint_record",
     "rf_backward", "rf_well_count", "rf_set_pressure_solver", "rf_batch_set_mode", "rf_batch_profile",
+    "rf_set_linear_refinement",
 )
 
 PHASES = ("assembly", "well_elimination", "cpr_build", "pressure_stage", "block_ilu_smoother", "krylov", "update",

@@ -1186,6 +1186,8 @@ static void free_ctx(Ctx& c) {
   c.dir_rows = 0;
   free_level_plan(c);
   for (auto* b : {&c.d_tri_ptr, &c.d_tri_up, &c.d_tri_ip, &c.d_pt_ptr, &c.d_pt_lp, &c.d_pt_ue}) b->free();
+  c.d_ref_b.free();
+  c.d_ref_x.free();
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);
   if (c.levels.d_long_rows) cudaFree(c.levels.d_long_rows);
@@ -1361,6 +1363,20 @@ int32_t rf_set_controller_options(RfCtx* ctx, int32_t one_substep_per_report_ste
   ctx->c.ctl_cnv = cnv_tol;
   ctx->c.ctl_mb = mb_tol;
   return RF_OK;
+}
+
+int32_t rf_set_linear_refinement(RfCtx* ctx, double rtol, int32_t max_passes) {
+  if (!ctx || !(rtol >= 0.0) || !(rtol < 1.0) || max_passes < 0) return RF_ERR_INVALID;
+  return guarded(ctx, [&]() -> int32_t {
+    rf::Ctx& c = ctx->c;
+    if (rtol > 0.0 && !c.d_ref_b.p) {
+      c.d_ref_b.alloc(size_t(3) * c.n);
+      c.d_ref_x.alloc(size_t(3) * c.n);
+    }
+    c.lin_refine_rtol = rtol;
+    c.lin_refine_passes = max_passes > 0 ? max_passes : 12;
+    return RF_OK;
+  });
 }
 
 int32_t rf_adjoint_record(RfCtx* ctx, int32_t enable) {

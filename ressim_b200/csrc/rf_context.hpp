@@ -201,6 +201,12 @@ struct Ctx {
   // transpose of the forward coarse correction (rf_linear.cu, k_cpr_weights_t)
   int cpr_transposed = 0;
   double ctl_cnv = 0.0, ctl_mb = 0.0;
+  // refinement of each CPR-FGMRES solve of the Newton systems (rf_set_linear_refinement):
+  // x += solve(b - A x) until |b - A x| <= lin_refine_rtol |b|, at most lin_refine_passes solves;
+  // 0 keeps the reference's single solve.  d_ref_b / d_ref_x hold b and x meanwhile.
+  double lin_refine_rtol = 0.0;
+  int lin_refine_passes = 0;
+  DBuf<double> d_ref_b, d_ref_x;
   // discrete adjoint tape (rf_adjoint.cu); null until recording starts
   struct AdjointTape* tape = nullptr;
   int cluster_size = 0;  // CTAs in the one cluster that runs the level-scheduled kernels

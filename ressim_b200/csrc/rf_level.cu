@@ -235,46 +235,79 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
       rstride = RB;
     }
     T* cur = S + size_t(l & 1) * W;
-    for (int off = t; off < w; off += NT) {
-      const int q = lst + off;
+    // A thread's rows of one level read only earlier levels (the window of the previous level and
+    // the far cache), never each other, so its rows are taken in pairs (offsets off and off + NT):
+    // both rows' loads first, then both rows' arithmetic, then the stores, so the two dependency
+    // chains overlap.  Per row the operations and their order are those of a single row, and the
+    // rows keep their order in the thread's sum.
+    struct Row {
+      unsigned long long word;
+      T v0, v1, v2, v3, pre, s;
+      int q;
+    };
+    auto load_row = [&](int off, Row& R) {
+      R.q = lst + off;
       const unsigned char* rp = rbase + size_t(off) * rstride;
-      const unsigned long long word = *reinterpret_cast<const unsigned long long*>(rp);
+      R.word = *reinterpret_cast<const unsigned long long*>(rp);
       const T* v = reinterpret_cast<const T*>(rp + 8);
-      const T x0 = inp ? inp[off] : in0[q];
-      T s;
+      R.v0 = v[0];
+      R.v1 = v[1];
+      R.v2 = v[2];
+      R.v3 = MODE == 2 ? v[3] : T(0);
+      const T x0 = inp ? inp[off] : in0[R.q];
       if (MODE == 0) {
-        const T x1 = inp ? inp[W + off] : in1[q];
-        const T x2 = inp ? inp[2 * W + off] : in2[q];
-        s = first ? x0 : T(double(x0) + beta * (double(x2) - omega * double(x1)));
-        a.p[q] = s;
+        const T x1 = inp ? inp[W + off] : in1[R.q];
+        const T x2 = inp ? inp[2 * W + off] : in2[R.q];
+        R.pre = first ? x0 : T(double(x0) + beta * (double(x2) - omega * double(x1)));
       } else if (MODE == 1) {
-        const T x1 = inp ? inp[W + off] : in1[q];
-        s = T(double(x0) - alpha * double(x1));
-        a.s[q] = s;
-        acc += double(s) * double(s);
+        const T x1 = inp ? inp[W + off] : in1[R.q];
+        R.pre = T(double(x0) - alpha * double(x1));
       } else {
-        s = x0;
+        R.pre = x0;
       }
-      const unsigned meta = unsigned(word >> 48);
+    };
+    auto solve_row = [&](Row& R) {
+      T s = R.pre;
+      const unsigned meta = unsigned(R.word >> 48);
       if ((meta & 7u) != kLongCnt) {
         // absent entries point at the zero slot with a zero value: exact no-ops
-        const T d0 = S[unsigned(word) & 0xffffu], d1 = S[unsigned(word >> 16) & 0xffffu],
-                d2 = S[unsigned(word >> 32) & 0xffffu];
-        s -= v[0] * d0;
-        s -= v[1] * d1;
-        s -= v[2] * d2;
+        const T d0 = S[unsigned(R.word) & 0xffffu], d1 = S[unsigned(R.word >> 16) & 0xffffu],
+                d2 = S[unsigned(R.word >> 32) & 0xffffu];
+        s -= R.v0 * d0;
+        s -= R.v1 * d1;
+        s -= R.v2 * d2;
       } else {
-        const int li = int(word & 0xffffu);
+        const int li = int(R.word & 0xffffu);
         for (int e = lptr[li]; e < lptr[li + 1]; ++e) s -= lval[e] * S[lidx[e]];
       }
-      if (MODE == 2) {
-        const T d = v[3];
-        s = fabs(double(d)) > kEpsL ? s / d : s;
+      if (MODE == 2) s = fabs(double(R.v3)) > kEpsL ? s / R.v3 : s;
+      R.s = s;
+    };
+    auto store_row = [&](int off, const Row& R) {
+      if (MODE == 0) a.p[R.q] = R.pre;
+      if (MODE == 1) {
+        a.s[R.q] = R.pre;
+        acc += double(R.pre) * double(R.pre);
       }
-      cur[off] = s;
-      out[q] = s;
-      const unsigned fs = meta >> 3;
-      if (fs) far[fs - 1] = s;
+      cur[off] = R.s;
+      out[R.q] = R.s;
+      const unsigned fs = unsigned(R.word >> 48) >> 3;
+      if (fs) far[fs - 1] = R.s;
+    };
+    for (int off = t; off < w; off += 2 * NT) {
+      const int offb = off + NT;
+      Row A, B;
+      load_row(off, A);
+      if (offb < w) {
+        load_row(offb, B);
+        solve_row(A);
+        solve_row(B);
+        store_row(off, A);
+        store_row(offb, B);
+      } else {
+        solve_row(A);
+        store_row(off, A);
+      }
     }
     __syncthreads();
   }
@@ -299,22 +332,35 @@ template <class T, int MODE>
 __device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0, double& acc1) {
   const int NT = a.threads, n = a.n;
   const int t0 = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);
-  for (int q = t0; q < n; q += NT) {
-    int c[kSpK];
-    T v[kSpK], x[kSpK];
+  // rows q and q + NT together: both rows' loads are issued before either's stores; each row's sum
+  // and the thread's dot-product order are those of one row at a time
+  for (int q = t0; q < n; q += 2 * NT) {
+    const int nr = q + NT < n ? 2 : 1;
+    int c[2][kSpK];
+    T v[2][kSpK];
 #pragma unroll
-    for (int j = 0; j < kSpK; ++j) {
-      c[j] = a.sp_col[size_t(j) * n + q];
-      v[j] = a.spval[size_t(j) * n + q];
-    }
-    if (c[0] == -2) continue;  // a longer row: below
+    for (int r = 0; r < 2; ++r)
+      if (r < nr) {
 #pragma unroll
-    for (int j = 0; j < kSpK; ++j) x[j] = c[j] >= 0 ? in[c[j]] : T(0);
-    T s = T(0);
+        for (int j = 0; j < kSpK; ++j) {
+          c[r][j] = a.sp_col[size_t(j) * n + q + r * NT];
+          v[r][j] = a.spval[size_t(j) * n + q + r * NT];
+        }
+      }
+    T s[2] = {T(0), T(0)};
 #pragma unroll
-    for (int j = 0; j < kSpK; ++j)
-      if (c[j] >= 0) s += v[j] * x[j];
-    spmv_row_done<T, MODE>(a, q, s, out, acc0, acc1);
+    for (int r = 0; r < 2; ++r)
+      if (r < nr && c[r][0] != -2) {  // -2: a longer row, below
+        T x[kSpK];
+#pragma unroll
+        for (int j = 0; j < kSpK; ++j) x[j] = c[r][j] >= 0 ? in[c[r][j]] : T(0);
+#pragma unroll
+        for (int j = 0; j < kSpK; ++j)
+          if (c[r][j] >= 0) s[r] += v[r][j] * x[j];
+      }
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+      if (r < nr && c[r][0] != -2) spmv_row_done<T, MODE>(a, q + r * NT, s[r], out, acc0, acc1);
   }
   for (int e = t0; e < a.n_splong; e += NT) {
     const int q = a.splong_row[e];
@@ -385,12 +431,31 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     if (!isfinite(omega) || fabs(omega) < kEpsL) break;
     d0 = 0.0;
     d1 = 0.0;
-    for (int q = t; q < n; q += NT) {
-      a.xq[q] += alpha * double(a.ph[q]) + omega * double(a.sh[q]);
-      const T ri = T(double(a.s[q]) - omega * double(a.t[q]));
-      a.r[q] = ri;
-      d0 += double(ri) * double(ri);
-      d1 += double(a.rh[q]) * double(ri);
+    // positions q and q + NT together (all loads before the stores), sums in position order
+    for (int q = t; q < n; q += 2 * NT) {
+      const int nr = q + NT < n ? 2 : 1;
+      double xv[2], pv[2], sv[2], s0[2], tv[2], hv[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+        if (r < nr) {
+          const int k = q + r * NT;
+          xv[r] = a.xq[k];
+          pv[r] = double(a.ph[k]);
+          sv[r] = double(a.sh[k]);
+          s0[r] = double(a.s[k]);
+          tv[r] = double(a.t[k]);
+          hv[r] = double(a.rh[k]);
+        }
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+        if (r < nr) {
+          const int k = q + r * NT;
+          a.xq[k] = xv[r] + (alpha * pv[r] + omega * sv[r]);
+          const T ri = T(s0[r] - omega * tv[r]);
+          a.r[k] = ri;
+          d0 += double(ri) * double(ri);
+          d1 += hv[r] * double(ri);
+        }
     }
     block_sum2(d0, d1, red);
     if (sqrt(d0) <= tol) break;

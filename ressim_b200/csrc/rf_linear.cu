@@ -2340,9 +2340,11 @@ void schur_eliminate(Ctx& c) {
   }
 }
 
-LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol, int max_passes) {
-  // iterative refinement over the path's own inner solve (direct LU for small systems, else
-  // CPR-FGMRES at its 5e-3 relative tolerance): x += solve(b - A x) until |b - A x| <= rtol |b|
+LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol, int max_passes,
+                                 bool allow_direct) {
+  // iterative refinement over the path's own inner solve (direct LU for small systems when
+  // allowed, else CPR-FGMRES at its 5e-3 relative tolerance): x += solve(b - A x) until
+  // |b - A x| <= rtol |b|
   const long long n3 = 3ll * c.n;
   LinResult out;
   dot_dev(c, n3, b, nullptr, c.d_scal.p + 26, true);
@@ -2351,7 +2353,7 @@ LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol
   d2h_wait(c);
   out.rhs_norm = bn;
   RF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n3, c.stream));
-  const bool direct = direct_rows(c, false) <= kDirectSolveRows;
+  const bool direct = allow_direct && direct_rows(c, false) <= kDirectSolveRows;
   for (int pass = 0; pass <= max_passes; ++pass) {
     spmv_res(c, x, b, c.d_rhs_red.p);
     dot_dev(c, n3, c.d_rhs_red.p, nullptr, c.d_scal.p + 27, true);
@@ -2390,7 +2392,19 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
   const long long n3 = 3ll * n;
   schur_eliminate(c);
   const int W = c.topo.n_wells;
-  LinResult lin = linear_solve_reduced(c);
+  LinResult lin;
+  if (c.lin_refine_rtol > 0.0) {
+    // refined solve (rf_set_linear_refinement): the reduced system's b and x kept aside while
+    // the passes use the solver's own buffers; d_cres ends as the reduced residual of x
+    const size_t bytes = sizeof(double) * size_t(n3);
+    RF_CUDA(cudaMemcpyAsync(c.d_ref_b.p, c.d_rhs_red.p, bytes, cudaMemcpyDeviceToDevice, c.stream));
+    lin = solve_reduced_accurate(c, c.d_ref_b.p, c.d_ref_x.p, c.lin_refine_rtol, c.lin_refine_passes, false);
+    RF_CUDA(cudaMemcpyAsync(c.d_x.p, c.d_ref_x.p, bytes, cudaMemcpyDeviceToDevice, c.stream));
+    RF_CUDA(cudaMemcpyAsync(c.d_rhs_red.p, c.d_ref_b.p, bytes, cudaMemcpyDeviceToDevice, c.stream));
+    spmv_res(c, c.d_x.p, c.d_rhs_red.p, c.d_cres.p);
+  } else {
+    lin = linear_solve_reduced(c);
+  }
   h_dx_tail.assign(size_t(W) + c.topo.n_perfs, 0.0);
   // full-system residual: reduced residual for unperforated rows, direct rows elsewhere
   k_copy<<<reduce_blocks(c, n3), kBlock, 0, c.stream>>>(n3, c.d_cres.p, c.d_full.p);

@@ -39,9 +39,11 @@ void schur_eliminate(Ctx& c);
 LinResult linear_solve_reduced(Ctx& c, bool rebuild = true);
 
 // Accurate solve of the tail-free system in d_val: x = A^-1 b to |b - A x| <= rtol |b| by
-// iterative refinement over the inner solve (at most max_passes inner solves).  b and x are
-// device vectors of 3N (not d_rhs_red / d_x, which the inner solves use).
-LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol, int max_passes);
+// iterative refinement over the inner solve (at most max_passes inner solves; the direct LU for
+// systems of at most 512 rows when allow_direct, else CPR-FGMRES).  b and x are device vectors of
+// 3N (not d_rhs_red / d_x, which the inner solves use).
+LinResult solve_reduced_accurate(Ctx& c, const double* b, double* x, double rtol, int max_passes,
+                                 bool allow_direct = true);
 
 // Discrete adjoint kernels (rf_adjoint.cu)
 void adj_transpose(Ctx& c, const int* d_tpos);

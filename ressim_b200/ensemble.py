@@ -114,6 +114,14 @@ class Ensemble:
             if rc != _abi.RF_OK:
                 raise DeviceError(f"rf_set_controller_options failed for variant {i}: {_lib.last_error(c)}")
 
+    def set_linear_refinement(self, rtol: float = 0.0, max_passes: int = 0) -> None:
+        """rf_set_linear_refinement on every variant (see ReservoirSimulator.set_linear_refinement)."""
+        L = _lib.load()
+        for i, c in enumerate(self._ctx):
+            rc = L.rf_set_linear_refinement(c, float(rtol), int(max_passes))
+            if rc != _abi.RF_OK:
+                raise DeviceError(f"rf_set_linear_refinement failed for variant {i}: {_lib.last_error(c)}")
+
     def well_bhp(self, i: int) -> np.ndarray:
         n = len(self.decks[i].wells)
         out = np.zeros(n)

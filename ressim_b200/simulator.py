@@ -187,6 +187,15 @@ class ReservoirSimulator(Deck):
         if rc != _abi.RF_OK:
             raise DeviceError(f"rf_set_controller_options failed ({rc}): {_lib.last_error(self._context())}")
 
+    def set_linear_refinement(self, rtol: float = 0.0, max_passes: int = 0) -> None:
+        """Refine every CPR-FGMRES solve of the Newton systems to |b - A x| <= rtol |b| (at most
+        max_passes solves, 0: 12); no counterpart in the reference.  With tight CNV / MB tolerances
+        this is the matched profile for comparisons at 1e-6.  rtol = 0 restores the reference's
+        single solve."""
+        rc = _lib.load().rf_set_linear_refinement(self._context(), float(rtol), int(max_passes))
+        if rc != _abi.RF_OK:
+            raise DeviceError(f"rf_set_linear_refinement failed ({rc}): {_lib.last_error(self._context())}")
+
     def adjoint_record(self, enable: bool = True) -> None:
         """Start (clearing the tape) or stop recording report-step checkpoints for `backward`."""
         rc = _lib.load().rf_adjoint_record(self._context(), int(bool(enable)))

@@ -2,34 +2,33 @@
 
 Two bars.
 
-The matched tight-tolerance profile (tests/_matched.py) keeps the reference's controller and
-tightens only the Newton acceptance to CNV 1e-9 / MB 1e-11 on both the device and the oracle, so a
-substep whose Newton path (substep sizes, retries) is the same on both converges to the same
-discrete solution: pressure, water saturation and well BHP within 1e-6 relative (scale
-max(|x|, 1)), every rate-history record within 1e-6, Newton counts within one.  A Newton attempt
-that stops at the 20-iteration limit on one side and converges on the other changes the substep
-sequence; that happens at these tolerances because the linear solver keeps the reference's
-absolute floor (1e-12 + 5e-3 |b|) and its BiCGStab cap, so near convergence a solve can miss its
-tolerance.  Where the substep sequences differ, the fields differ by the time-discretisation of
-different substeps; the test then checks the Newton-tolerance bound (1e-4 pressure, 2e-3
-saturation) and reports the case.
+The matched tight-tolerance profile (tests/_matched.py) keeps the reference's controller, accepts
+a Newton attempt only at CNV 1e-9 / MB 1e-11 and refines every CPR-FGMRES solve to a relative
+residual of 1e-10, on both the device and the oracle.  Then the Newton path (every substep size,
+Newton count and retry) does not depend on rounding: the oracle run with reordered dot-product
+summations takes the same path and lands within 1e-14 of itself.  So the device must take the
+oracle's path exactly (same Newton iterations, substeps and retries per report step) and end each
+report step with pressure, water saturation (and Sg, Rs in three-phase mode) and well BHP within
+1e-6 relative (scale max(|x|, 1)), every rate-history record within 1e-6.
 
-At the reference's own tolerances, where the pressure BiCGStab stops at its 50-iteration cap, the
-bar is the reference algorithm's rounding floor: the oracle stepped with reordered dot-product
-summations moves by that much against itself, and the device stays within three times that spread
-plus 1e-6 (tests/_parity.py), with Newton counts inside the oracle's own range plus or minus one.
+At the reference's own tolerances, where the pressure BiCGStab stops at its 50-iteration cap and
+the Newton systems get one solve to 5e-3, the bar is the reference algorithm's rounding floor: the
+oracle stepped with reordered dot-product summations moves by that much against itself, and the
+device stays within three times that spread plus 1e-6 (tests/_parity.py), with Newton counts
+inside the oracle's own range plus or minus one.
 
   configuration 1: the 200-cell 1D waterflood, all 100 report steps (matched and default)
   configuration 2: the 60x60x20 three-phase black-oil deck (72,000 cells), 3 report steps of 10 d
+                   (matched and at the rounding floor)
   configuration 4: one ensemble variant from each size quartile, 3 report steps of 10 d, stepped
-                   together through the batch API
+                   together through the batch API (matched and at the rounding floor)
 
 The oracle runs in spawned processes (its controller options and summation order are
 process-wide).
 """
 import pytest
 
-from _matched import MATCHED_CNV, MATCHED_MB, make_deck, oracle_floor_runs, oracle_runs_parallel
+from _matched import apply_matched, make_deck, oracle_floor_runs, oracle_runs_parallel
 from _parity import NEWTON_TOL_P, NEWTON_TOL_SW, rel_err
 from ressim_b200 import Ensemble, ReservoirSimulator, decks
 
@@ -47,23 +46,16 @@ def _errs(gs, gbhp, cs, cbhp, three):
     return e
 
 
-def _check_step(tag, s, gs, gbhp, gnewton, gsub, gret, ref, three, state):
-    """Matched-profile bar for one report step; returns whether the substep sequences agreed."""
+def _check_step(tag, s, gs, gbhp, gnewton, gsub, gret, ref, three):
+    """Matched-profile bar for one report step: the oracle's Newton path, fields within 1e-6."""
     cs, cbhp, cnewton, csub, crc, cret = ref
     assert crc == 0, (tag, s, "oracle warning")
     e = _errs(gs, gbhp, cs, cbhp, three)
-    same = gsub == csub and gret == cret and not state.get("diverged")
     print(f"{tag} step {s}: " + ", ".join(f"{k} {v:.1e}" for k, v in e.items()) +
-          f", newton {gnewton}/{cnewton}, substeps {gsub}/{csub}, retries {gret}/{cret}" +
-          ("" if same else "  [substep sequences differ: Newton-tolerance bound]"))
-    if same:
-        for k, v in e.items():
-            assert v <= RTOL, (tag, s, k, v)
-        assert abs(gnewton - cnewton) <= 1, (tag, s, gnewton, cnewton)
-    else:
-        state["diverged"] = True
-        assert e["pressure"] <= NEWTON_TOL_P and e["sat_water"] <= NEWTON_TOL_SW, (tag, s, e)
-    return same
+          f", newton {gnewton}/{cnewton}, substeps {gsub}/{csub}, retries {gret}/{cret}")
+    assert (gnewton, gsub, gret) == (cnewton, csub, cret), (tag, s, "Newton path differs")
+    for k, v in e.items():
+        assert v <= RTOL, (tag, s, k, v)
 
 
 def _check_rates(tag, hg, hc):
@@ -81,13 +73,12 @@ def test_config1_waterflood_1d_all_100_report_steps_matched():
     deck, dt, steps = decks.waterflood_1d()
     refs, hist = oracle_runs_parallel([(("1d",), dt, steps)])[0]
     g = ReservoirSimulator.from_deck(deck)
-    g.set_controller_options(False, MATCHED_CNV, MATCHED_MB)
-    state = {}
+    apply_matched(g)
     for s in range(steps):
         r = g.step(dt)
         assert r["warning"] == 0
-        assert _check_step("config 1", s, g.state(), g.get_well_bhp(), r["newton_iterations"], r["substeps"],
-                           r["retries"], refs[s], False, state)
+        _check_step("config 1", s, g.state(), g.get_well_bhp(), r["newton_iterations"], r["substeps"],
+                    r["retries"], refs[s], False)
     _check_rates("config 1", g.get_rate_history(), hist)
 
 
@@ -97,11 +88,10 @@ def test_config1_waterflood_1d_all_100_report_steps_default_profile():
     deck, dt, steps = decks.waterflood_1d()
     refs, hist = oracle_runs_parallel([(("1d",), dt, steps, False)])[0]
     g = ReservoirSimulator.from_deck(deck)
-    state = {}
     for s in range(steps):
         r = g.step(dt)
-        assert _check_step("config 1 default", s, g.state(), g.get_well_bhp(), r["newton_iterations"],
-                           r["substeps"], r["retries"], refs[s], False, state)
+        _check_step("config 1 default", s, g.state(), g.get_well_bhp(), r["newton_iterations"], r["substeps"],
+                    r["retries"], refs[s], False)
     _check_rates("config 1 default", g.get_rate_history(), hist)
 
 
@@ -115,10 +105,12 @@ def _floor_check(tag, s, gs, newton, runs, three, state):
         floor = max(rel_err(runs[m][0][s][0][k], ref[k]) for m in runs if m != 0)
         err = rel_err(gs[k], ref[k])
         line.append(f"{k} {err:.1e} (floor {floor:.1e})")
+        bar = 3 * floor + RTOL
         if state.get("diverged"):
-            assert err <= (NEWTON_TOL_P if k == "pressure" else NEWTON_TOL_SW), (tag, s, k, err)
-        else:
-            assert err <= 3 * floor + RTOL, (tag, s, k, err, floor)
+            # a Newton count off the unreordered oracle's changed the substep sizes: the
+            # Newton-tolerance bound, or the floor where the oracle's own orders spread wider
+            bar = max(bar, NEWTON_TOL_P if k == "pressure" else NEWTON_TOL_SW)
+        assert err <= bar, (tag, s, k, err, floor)
     print(f"{tag} step {s}: " + ", ".join(line) + f", newton {newton} (oracle {min(counts)}..{max(counts)})")
     assert min(counts) - 1 <= newton <= max(counts) + 1, (tag, s, newton, counts)
     if newton != runs[0][0][s][2]:
@@ -134,6 +126,18 @@ def test_config2_blackoil_72k_three_report_steps_at_rounding_floor():
         r = g.step(dt)
         assert r["warning"] == 0
         _floor_check("config 2", s, g.state(), r["newton_iterations"], runs, True, state)
+
+
+def test_config2_blackoil_72k_three_report_steps_matched():
+    spec, dt, steps = ("bo", (60, 60, 20)), 10.0, 3
+    refs, _ = oracle_runs_parallel([(spec, dt, steps)])[0]
+    g = ReservoirSimulator.from_deck(make_deck(spec))
+    apply_matched(g)
+    for s in range(steps):
+        r = g.step(dt)
+        assert r["warning"] == 0
+        _check_step("config 2", s, g.state(), g.get_well_bhp(), r["newton_iterations"], r["substeps"],
+                    r["retries"], refs[s], True)
 
 
 def quartile_variants(n_variants=256):
@@ -164,18 +168,14 @@ def test_config4_ensemble_quartile_variants_matched():
     dt, steps = 10.0, 3
     refs = oracle_runs_parallel([(("variant", i), dt, steps) for i in picks])
     ens = Ensemble([decks.ensemble_variant(i) for i in picks])
-    ens.set_controller_options(False, MATCHED_CNV, MATCHED_MB)
-    states = [{} for _ in picks]
+    apply_matched(ens)
     for s in range(steps):
         reps = ens.step(dt)
         for j, i in enumerate(picks):
             r = reps[j]
             assert r["warning"] == 0
             _check_step(f"variant {i} ({sizes[i]} cells)", s, ens.state(j), ens.well_bhp(j), r["newton_iterations"],
-                        r["substeps"], r["retries"], refs[j][0][s], False, states[j])
+                        r["substeps"], r["retries"], refs[j][0][s], False)
     for j, i in enumerate(picks):
-        if not states[j].get("diverged"):
-            _check_rates(f"variant {i}", ens.rate_history(j), refs[j][1])
-    # the profile matches where the paths agree: the smallest quartile's variant does (8,096 cells)
-    assert not states[0].get("diverged")
+        _check_rates(f"variant {i}", ens.rate_history(j), refs[j][1])
     ens.close()
