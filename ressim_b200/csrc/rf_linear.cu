@@ -20,6 +20,7 @@
 // fill.  Pressure-matrix entries with |v| <= 1e-14 are dropped, as the reference does.
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <cstdio>
@@ -756,31 +757,6 @@ __device__ __forceinline__ const int* stage_levels(const LevelSched& L, int* s_p
   return L.lvl_ptr;
 }
 
-__global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(LevelSched L, const double* __restrict__ val,
-                                                                const unsigned char* __restrict__ mask, double* lu,
-                                                                double* dinv, const double* __restrict__ pval,
-                                                                double* plu, double* pdiag) {
-  __shared__ int s_ptr[kSmemLevels];
-  const int* lp = stage_levels(L, s_ptr);
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  const int warp = tid >> 5, nwarps = nth >> 5;
-  for (int l = 0; l < L.n_levels; ++l) {
-    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) {
-      const int r = L.lvl_rows[q];
-      if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
-      block_ilu_row(r, L.rp, L.col, L.diag, val, mask, lu, dinv);
-      pressure_ilu_row(r, L.rp, L.col, L.diag, pval, plu, pdiag);
-    }
-    __syncwarp();
-    for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps)
-      ilu_rows_warp(L.long_rows[q], L.rp, L.col, L.diag, val, mask, lu, dinv, pval, plu, pdiag);
-    cluster_barrier();
-  }
-}
-
-// The same factorisation for many contexts in one launch (the ensemble's batched stepping):
-// thread block b factors item b's matrices alone, level by level, with block barriers.  Every row
-// gets the operations of k_factor_cluster, so the factors do not depend on the launch.
 // Precomputed update lists of the factorisation (built once per pattern): for each lower entry kp
 // of a row, the pairs (up, ip) of the U-row of col[kp] whose column the row also holds (the
 // merge block_ilu_row performs); for each entry k of a row, the terms (lp, ue) of the pressure ILU
@@ -864,6 +840,168 @@ __device__ void ilu_row_recipe(int i, const FacArgs& a) {
     a.plu[up] = terms(up, a.pval[up]);
   }
 }
+// Both ILU0 rows of a row of at most 32 blocks (a perforated cell's row with its well's fill) by
+// one warp, from the update lists: lane j holds entry b0 + j of the row in registers, so the
+// sequential walk over the row's lower entries costs shuffles instead of global round trips.
+// Every element gets the operations of block_ilu_row / pressure_ilu_row in their order:
+//  - block: for each present lower entry kp in turn, every lane forms L_ik = lu_kp Dinv_col[kp]
+//    (both shuffled from lane kp); lane e takes the e-th pair (up, ip) of kp's list and forms
+//    L_ik U_up; lane ip - b0 subtracts it from its block (each pair updates a different block);
+//    lane kp's block becomes L_ik;
+//  - pressure: each lower entry in turn, its terms plu[lp] U(col[lp], c) formed by one lane each
+//    and summed in list order; then the diagonal; the upper entries each by their own lane.
+// s_src and s_pl are this warp's 32-entry shared-memory scratch.
+__device__ void ilu_rows_lanes(int i, const FacArgs& a, int* s_src, double* s_pl) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int* rp = a.L.rp;
+  const int* col = a.L.col;
+  const FacRecipes& R = a.R;
+  const int b0 = rp[i], dp = a.L.diag[i], b1 = rp[i + 1];
+  const int len = b1 - b0, nl = dp - b0;
+  const int k = b0 + lane;
+  const bool own = lane < len;
+  const bool m = own && a.mask[k];
+  double blk[9], dv[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) blk[e] = m ? a.val[size_t(k) * 9 + e] : 0.0;
+  const int ck = own ? col[k] : 0;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) dv[e] = lane < nl ? a.dinv[size_t(ck) * 9 + e] : 0.0;
+  const unsigned present = __ballot_sync(kAll, m);
+  for (int kp = 0; kp < nl; ++kp) {
+    if (!((present >> kp) & 1u)) continue;  // uniform over the warp
+    double lk[9], dk[9], lik[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      lk[e] = __shfl_sync(kAll, blk[e], kp);
+      dk[e] = __shfl_sync(kAll, dv[e], kp);
+    }
+    mat3_mul(lk, dk, lik);
+    const int e0 = R.tri_ptr[b0 + kp], np = R.tri_ptr[b0 + kp + 1] - e0;
+    int tgt = -1;
+    double prod[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) prod[e] = 0.0;
+    if (lane < np) {
+      const int up = R.tri_up[e0 + lane], ip = R.tri_ip[e0 + lane];
+      if (a.mask[up] && a.mask[ip]) {
+        double u[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) u[e] = a.lu[size_t(up) * 9 + e];
+        mat3_mul(lik, u, prod);
+        tgt = ip - b0;
+      }
+    }
+    s_src[lane] = -1;
+    __syncwarp();
+    if (tgt >= 0) s_src[tgt] = lane;
+    __syncwarp();
+    const int src = s_src[lane];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      const double v = __shfl_sync(kAll, prod[e], src >= 0 ? src : lane);
+      if (src >= 0) blk[e] -= v;
+    }
+    if (lane == kp) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) blk[e] = lik[e];
+    }
+  }
+  if (lane == nl) mat3_inverse_or_diag(blk, a.dinv + size_t(i) * 9);
+  if (own) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) a.lu[size_t(k) * 9 + e] = blk[e];
+  }
+  // pressure ILU0
+  const double pv = own ? a.pval[k] : 0.0;
+  const double pdg = lane < nl ? a.pdiag[ck] : 0.0;
+  const unsigned pnz = __ballot_sync(kAll, own && pv != 0.0);
+  double pl = 0.0;
+  // s0 minus the terms of entry kk in list order (entries whose lp has a zero value skipped)
+  auto terms = [&](int kk, double s0) {
+    const int e0 = R.pt_ptr[kk], nt = R.pt_ptr[kk + 1] - e0;
+    int lpl = lane;
+    double ue = 0.0;
+    if (lane < nt) {
+      lpl = R.pt_lp[e0 + lane] - b0;
+      ue = a.plu[R.pt_ue[e0 + lane]];
+    }
+    const double plp = __shfl_sync(kAll, pl, lpl);
+    const bool valid = lane < nt && ((pnz >> lpl) & 1u);
+    const double term = valid ? plp * ue : 0.0;
+    double s = s0;
+    for (int q = 0; q < nt; ++q) {
+      const double tq = __shfl_sync(kAll, term, q);
+      if (__shfl_sync(kAll, int(valid), q)) s -= tq;
+    }
+    return s;
+  };
+  for (int kp = 0; kp < nl; ++kp) {
+    if (!((pnz >> kp) & 1u)) continue;  // plu stays 0
+    const double s = terms(b0 + kp, __shfl_sync(kAll, pv, kp));
+    const double d = __shfl_sync(kAll, pdg, kp);
+    if (lane == kp) pl = fabs(d) > kEps ? s / d : 0.0;
+  }
+  {
+    const double de = __shfl_sync(kAll, pv, nl);
+    double ud = terms(dp, de);
+    if (fabs(ud) <= kEps) ud = fabs(de) > kEps ? de : 1.0;
+    if (lane == 0) a.pdiag[i] = ud;
+  }
+  // upper entries: each lane its own, reading the row's lower values from shared memory
+  s_pl[lane] = pl;
+  __syncwarp();
+  if (own && lane > nl && pv != 0.0) {
+    double s = pv;
+    for (int e = R.pt_ptr[k]; e < R.pt_ptr[k + 1]; ++e) {
+      const int lpl = R.pt_lp[e] - b0;
+      if (!((pnz >> lpl) & 1u)) continue;
+      s -= s_pl[lpl] * a.plu[R.pt_ue[e]];
+    }
+    pl = s;
+  }
+  if (own) a.plu[k] = lane == nl ? 0.0 : pl;
+  __syncwarp();
+}
+
+// One factorisation on one thread-block cluster: each level's short rows spread over all CTAs'
+// threads, the rows with a well's fill over their warps, one cluster barrier per level.
+__global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(const __grid_constant__ FacArgs a) {
+  __shared__ int s_ptr[kSmemLevels];
+  __shared__ int s_src[kFBlock];
+  __shared__ double s_pl[kFBlock];
+  const LevelSched& L = a.L;
+  const int* lp = stage_levels(L, s_ptr);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int warp = tid >> 5, nwarps = nth >> 5, lw = threadIdx.x >> 5;
+  for (int l = 0; l < L.n_levels; ++l) {
+    for (int q = lp[l] + tid; q < lp[l + 1]; q += nth) {
+      const int r = L.lvl_rows[q];
+      if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
+      if (a.R.tri_ptr) {
+        ilu_row_recipe(r, a);
+      } else {
+        block_ilu_row(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv);
+        pressure_ilu_row(r, L.rp, L.col, L.diag, a.pval, a.plu, a.pdiag);
+      }
+    }
+    __syncwarp();
+    for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps) {
+      const int r = L.long_rows[q];
+      if (a.R.tri_ptr && L.rp[r + 1] - L.rp[r] <= 32)
+        ilu_rows_lanes(r, a, s_src + 32 * lw, s_pl + 32 * lw);
+      else
+        ilu_rows_warp(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv, a.pval, a.plu, a.pdiag);
+    }
+    cluster_barrier();
+  }
+}
+
+// The same factorisation for many contexts in one launch (the ensemble's batched stepping, and
+// the level-order path with one item): thread block b factors item b's matrices alone, level by
+// level, with block barriers.  Every row gets the operations of k_factor_cluster, so the factors
+// do not depend on the launch.
 struct FacBatch {
   int count;
   FacArgs item[kBatchItems];
@@ -874,6 +1012,8 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_batch(const __grid_consta
   const LevelSched& L = a.L;
   __shared__ int s_ptr[kSmemLevels];
   const int* lp = stage_levels(L, s_ptr);
+  __shared__ int s_src[kFBlock];
+  __shared__ double s_pl[kFBlock];
   const int tid = threadIdx.x, nth = blockDim.x;
   const int warp = tid >> 5, nwarps = nth >> 5;
   for (int l = 0; l < L.n_levels; ++l) {
@@ -888,8 +1028,13 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_batch(const __grid_consta
       }
     }
     __syncwarp();
-    for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps)
-      ilu_rows_warp(L.long_rows[q], L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv, a.pval, a.plu, a.pdiag);
+    for (int q = L.long_ptr[l] + warp; q < L.long_ptr[l + 1]; q += nwarps) {
+      const int r = L.long_rows[q];
+      if (a.R.tri_ptr && L.rp[r + 1] - L.rp[r] <= 32)
+        ilu_rows_lanes(r, a, s_src + 32 * warp, s_pl + 32 * warp);
+      else
+        ilu_rows_warp(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv, a.pval, a.plu, a.pdiag);
+    }
     __syncthreads();
   }
 }
@@ -1987,7 +2132,7 @@ static void cpr_build(Ctx& c) {
     k_factor_batch<<<1, kFBlock, 0, c.stream>>>(fb);
     c.launches++;
   } else {
-    void* args[] = {&L, (void*)&val, (void*)&mask, &lu, &dinv, (void*)&pval, &plu, &pdiag};
+    void* args[] = {(void*)&fa};
     cluster_launch(c, (const void*)k_factor_cluster, kFBlock, args);
   }
   c.lvl.packed = -1;
@@ -2480,6 +2625,10 @@ LinResult linear_solve_full(Ctx& c, std::vector<double>& h_dx_tail) {
 // ---- one-time setup ----
 // Update lists of the factorisation (FacRecipes) for the current pattern.
 void build_factor_recipes(Ctx& c) {
+  // RESSIM_FACTOR_RECIPES=0 (read when a context is set up) keeps the searching forms of the
+  // factorisation instead; the two give identical factors, which the tests check through it
+  const char* env = std::getenv("RESSIM_FACTOR_RECIPES");
+  if (env && std::strcmp(env, "0") == 0) return;
   const int n = c.n, nnzb = c.nnzb;
   std::vector<int> tri_ptr(nnzb + 1, 0), tri_up, tri_ip, pt_ptr(nnzb + 1, 0), pt_lp, pt_ue;
   auto find_in_row_upper = [&](int row, int colj) -> int {

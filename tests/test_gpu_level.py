@@ -129,3 +129,26 @@ def test_level_kernel_is_deterministic_and_validates_arguments():
             g.set_pressure_solver("warp")
         g.close()
     assert np.array_equal(runs[0], runs[1])
+
+
+@pytest.mark.parametrize("kind", ["level", "cluster"])
+def test_factorisation_update_lists_equal_searching_form(kind, monkeypatch):
+    """The factorisation from update lists (short rows by one thread each; a perforated cell's row
+    with its well's fill, here 7 + 11 blocks, by a warp holding the row in registers) gives the
+    factors of the searching form bit for bit: a deck whose wells perforate 12 layers, stepped with
+    each form (RESSIM_FACTOR_RECIPES=0 keeps the searching one), ends with identical states and
+    Newton counts, on both kernel families."""
+    deck = decks.waterflood_3d(14, 12, 12, seed=5, rate_per_perf=30.0)
+    runs = []
+    for recipes in ("1", "0"):
+        monkeypatch.setenv("RESSIM_FACTOR_RECIPES", recipes)
+        g = ReservoirSimulator.from_deck(deck)
+        g.set_pressure_solver(kind)
+        newton = [g.step(5.0)["newton_iterations"] for _ in range(2)]
+        runs.append((g.state(), g.get_well_bhp().copy(), newton))
+        g.close()
+    (s1, b1, n1), (s0, b0, n0) = runs
+    assert n1 == n0, (n1, n0)
+    for k in ("pressure", "sat_water"):
+        assert np.array_equal(s1[k], s0[k]), k
+    assert np.array_equal(b1, b0)
