@@ -29,8 +29,8 @@ Legs of the `--impl ours` run:
             -march=native on this host) on the same deck (ensemble: variant 0) and the same report
             steps after the same warm-up, in a spawned process beside the GPU legs;
   matched_comparison  (ensemble) the batched mixed form over all variants against the plain FP64
-            path one variant at a time, both with Newton accepted at CNV 1e-9 / MB 1e-11, and the
-            field error between them.
+            path one variant at a time, both with Newton accepted at CNV 1e-8 / MB 1e-10 and every
+            CPR-FGMRES solve refined to 1e-10 relative, and the field error between them.
 
 The reference arm (`--impl reference`) times the CPU restatement on the host cores: the single
 deck on one core (the reference is single-threaded), the ensemble as one single-threaded process
@@ -402,7 +402,7 @@ def run_reference(args):
     return 0
 
 
-MATCHED_CNV, MATCHED_MB = 1e-9, 1e-11
+MATCHED_CNV, MATCHED_MB = 1e-8, 1e-10
 MATCHED_LIN_RTOL, MATCHED_LIN_PASSES = 1e-10, 12
 
 
@@ -436,8 +436,8 @@ def ensemble_roofline(ds, profs, peak, peak_kind, batch=None):
 
 
 def matched_comparison(ds, dt, sample):
-    """The north-star comparison on the ensemble at the matched profile (Newton accepted at CNV 1e-9
-    / MB 1e-11 and every CPR-FGMRES solve refined to 1e-10 relative on both paths, the reference's
+    """The north-star comparison on the ensemble at the matched profile (Newton accepted at CNV 1e-8
+    / MB 1e-10 and every CPR-FGMRES solve refined to 1e-10 relative on both paths, the reference's
     controller otherwise): the batched mixed form over all
     variants against the plain FP64 path stepping variants one at a time through rf_step.  One
     untimed and one timed report step each; the plain path runs on `sample` (variants spread over
@@ -481,7 +481,7 @@ def matched_comparison(ds, dt, sample):
     cells = sum(d.n_cells for d in ds)
     v_batch = cells / (batch_ms / 1e3)
     v_seq = seq_cells / (seq_ms / 1e3)
-    return {"profile": "matched: reference controller, Newton accepted at CNV 1e-9 / MB 1e-11, every CPR-FGMRES "
+    return {"profile": "matched: reference controller, Newton accepted at CNV 1e-8 / MB 1e-10, every CPR-FGMRES "
                        "solve refined to 1e-10 relative, on both paths",
             "batched_mixed": v_batch, "plain_fp64_one_at_a_time": v_seq, "ratio": v_batch / v_seq,
             "plain_sample_variants": list(sample), "report_step": "the second report step (one untimed before it)",

@@ -2,15 +2,16 @@
 in spawned worker processes (the oracle's controller options are process-wide).
 
 Profile: the reference's controller unchanged (PID substep sizes, 0.33 retry factor, iteration-count
-growth; timestep.rs:989-1848), with every Newton attempt accepted only at CNV <= 1e-9 and MB <= 1e-11
+growth; timestep.rs:989-1848), with every Newton attempt accepted only at CNV <= 1e-8 and MB <= 1e-10
 on each component (no relaxed tiers, no pore-volume relaxation) instead of the reference's
 CNV 1e-2 / MB 1e-7 tiers, and every CPR-FGMRES solve of a Newton system refined to a relative
 residual of 1e-10 (x += solve(b - A x), the reference's solver inside each pass) instead of the
 reference's single solve to 5e-3.  The reference's single solve leaves each Newton update
 uncertain at the 5e-3 level, so the preconditioner's rounding moves Newton counts and, through
 the iteration-count dt rule, the substep sizes; refined, a Newton update is determined to about
-1e-10 and a state that meets CNV 1e-9 to about that level, whatever the summation order or the
-precision of the preconditioner.  Both sides then take the same Newton path and converge to the
+1e-10 and a state that meets CNV 1e-8 to about that level, whatever the summation order or the
+precision of the preconditioner.  (At CNV 1e-9 / MB 1e-11 some decks' Newton iterations stall near
+the residual's rounding level, so acceptance there, and with it the retries, turns on rounding.)  Both sides then take the same Newton path and converge to the
 same discrete solution, and the report-step fields can be compared at 1e-6.  This deviates from
 the reference's default tolerances; it is used for parity and for the matched-error comparison
 of the mixed form.
@@ -22,7 +23,7 @@ import os
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-MATCHED_CNV, MATCHED_MB = 1e-9, 1e-11
+MATCHED_CNV, MATCHED_MB = 1e-8, 1e-10
 MATCHED_LIN_RTOL, MATCHED_LIN_PASSES = 1e-10, 12
 
 

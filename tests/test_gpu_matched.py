@@ -3,7 +3,7 @@
 Two bars.
 
 The matched tight-tolerance profile (tests/_matched.py) keeps the reference's controller, accepts
-a Newton attempt only at CNV 1e-9 / MB 1e-11 and refines every CPR-FGMRES solve to a relative
+a Newton attempt only at CNV 1e-8 / MB 1e-10 and refines every CPR-FGMRES solve to a relative
 residual of 1e-10, on both the device and the oracle.  Then the Newton path (every substep size,
 Newton count and retry) does not depend on rounding: the oracle run with reordered dot-product
 summations takes the same path and lands within 1e-14 of itself.  So the device must take the
