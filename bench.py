@@ -406,6 +406,18 @@ MATCHED_CNV, MATCHED_MB = 1e-8, 1e-10
 MATCHED_LIN_RTOL, MATCHED_LIN_PASSES = 1e-10, 12
 
 
+# DRAM bytes (read + write) per algorithmic byte of one batched level-order pressure launch, from
+# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass, caches flushed before the
+# launch) of the first k_bicgstab_level_batch launch of `bench.py --variants 2 --host-threads 1
+# --steps 1 --warmup 0`: variants 0 and 1 (18,705 and 39,480 cells), 50 iterations each, 11.03 MB
+# of DRAM traffic against 1,901 MB of algorithmic bytes.  The solves' working set is read from
+# DRAM about once and every later pass hits L2.
+LEVEL_BATCH_DRAM_PER_ALG_BYTE = 11.03e6 / 1901.47e6
+# DRAM bytes per launch of the one-cluster pressure BiCGStab on the 60x60x20 black-oil deck
+# (k_bicgstab_dsmem, ncu dram__bytes_read.sum + dram__bytes_write.sum, caches flushed).
+CLUSTER_DRAM_PER_LAUNCH = {"72k-bo": 15.71e6}
+
+
 def ensemble_roofline(ds, profs, peak, peak_kind, batch=None):
     """Roofline of the dominant kernel (the pressure BiCGStab): algorithmic bytes of one launch / its
     duration (CUDA events on the launching stream), averaged over the launches (bytes and time
@@ -429,8 +441,11 @@ def ensemble_roofline(ds, profs, peak, peak_kind, batch=None):
         return None
     phase_ms = sum(sum(p[k] for k in _lib.PHASES if k != "bicgstab_kernel") for p in profs)
     achieved = (byts / nl) / (kms / nl / 1e3) / 1e9
+    traffic = LEVEL_BATCH_DRAM_PER_ALG_BYTE * byts / nl
     return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-            "unit": "GB/s", "frac": achieved / peak, "traffic": None, "bytes_per_launch": byts / nl,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "traffic_basis": "ncu DRAM bytes per algorithmic byte of one batched launch (caches flushed), "
+                             "scaled to this run's bytes per launch", "bytes_per_launch": byts / nl,
             "ms_per_launch": kms / nl, "launches": nl, "solves": solves, "iterations_per_solve": it / max(solves, 1),
             "share_of_phase_time": sum(p["bicgstab_kernel"] for p in profs) / max(phase_ms, 1e-9)}
 
@@ -975,8 +990,10 @@ def main():
         achieved = bytes_launch / (ms_launch / 1e3) / 1e9
         kname = ("k_bicgstab_level (one thread block, level order)" if prof.get("level_kernels")
                  else "k_bicgstab_dsmem / k_bicgstab_cluster (one thread-block cluster)")
+        traffic = (None if prof.get("level_kernels") or args.precision != "fp64"
+                   else CLUSTER_DRAM_PER_LAUNCH.get(args.workload))
         roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "bytes_per_launch": bytes_launch, "ms_per_launch": ms_launch,
                 "iterations_per_launch": iters / launches_b,
                 "share_of_step": kernel_ms / max(dev_ms, 1e-9)}

@@ -1187,6 +1187,7 @@ static void free_ctx(Ctx& c) {
   free_level_plan(c);
   for (auto* b : {&c.d_tri_ptr, &c.d_tri_up, &c.d_tri_ip, &c.d_pt_ptr, &c.d_pt_lp, &c.d_pt_ue}) b->free();
   c.d_ref_b.free();
+  c.d_fac_simple.free();
   c.d_ref_x.free();
   if (c.levels.d_rows) cudaFree(c.levels.d_rows);
   if (c.levels.d_ptr) cudaFree(c.levels.d_ptr);

@@ -226,6 +226,7 @@ struct Ctx {
   DBuf<int> d_flag_dense;
   // update lists of the factorisation (rf_linear.cu, FacRecipes)
   DBuf<int> d_tri_ptr, d_tri_up, d_tri_ip, d_pt_ptr, d_pt_lp, d_pt_ue;
+  DBuf<unsigned char> d_fac_simple;  // [n] rows of the simple shape (rf_linear.cu, ilu_row_simple)
   // pressure-stage solver: 0 automatic, 1 the cluster kernels, 2 the single-CTA level-order kernels
   int pressure_solver = 0;
   int level_threads = 0;  // threads of the level-order kernels (0: automatic)

@@ -769,6 +769,7 @@ struct FacRecipes {
   const int* pt_ptr;   // [nnzb + 1]
   const int* pt_lp;
   const int* pt_ue;
+  const unsigned char* simple;  // [n] 1: the row takes ilu_row_simple
 };
 
 struct FacArgs {
@@ -840,6 +841,117 @@ __device__ void ilu_row_recipe(int i, const FacArgs& a) {
     a.plu[up] = terms(up, a.pval[up]);
   }
 }
+// Both ILU0 rows of a "simple" row, the shape of every 7-point stencil row: at most kSimpleLower
+// lower entries, each updating only the diagonal block (at most one pair per lower entry, its
+// target the diagonal), and pressure terms only on the diagonal.  Then no lower entry changes
+// before it is used, so the row's inputs (its own values, the lower columns' inverse diagonal
+// blocks and pivots, the U blocks and pressure factors the updates read) are all loaded first, in
+// a few independent rounds, instead of the chain of dependent loads the general walk takes.  The
+// arithmetic is ilu_row_recipe's, in its order: L_ik = lu_kp Dinv_col[kp], the diagonal minus
+// L_ik U_up in kp order, the pressure lower entries s / d, the diagonal's terms in list order.
+constexpr int kSimpleLower = 4;
+__device__ void ilu_row_simple(int i, const FacArgs& a) {
+  const int* rp = a.L.rp;
+  const int* col = a.L.col;
+  const FacRecipes& R = a.R;
+  const int b0 = __ldg(rp + i), dp = __ldg(a.L.diag + i), b1 = __ldg(rp + i + 1);
+  const int nl = dp - b0;
+  // structure (read-only in this kernel)
+  int ck[kSimpleLower], up[kSimpleLower];
+  bool mk[kSimpleLower];
+  double pv[kSimpleLower];
+#pragma unroll
+  for (int j = 0; j < kSimpleLower; ++j) {
+    ck[j] = 0;
+    up[j] = -1;
+    mk[j] = false;
+    pv[j] = 0.0;
+    if (j < nl) {
+      const int k = b0 + j;
+      ck[j] = __ldg(col + k);
+      mk[j] = __ldg(a.mask + k) != 0;
+      pv[j] = __ldg(a.pval + k);
+      const int e0 = __ldg(R.tri_ptr + k), e1 = __ldg(R.tri_ptr + k + 1);
+      if (e1 > e0) up[j] = __ldg(R.tri_up + e0);
+    }
+  }
+  const bool md = __ldg(a.mask + dp) != 0;
+  double D[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) D[e] = md ? __ldg(a.val + size_t(dp) * 9 + e) : 0.0;
+  // block ILU0: each present lower entry's L_ik, and its update of the diagonal in kp order; the
+  // row's stores wait until all its loads are issued
+  double lik[kSimpleLower][9];
+#pragma unroll
+  for (int j = 0; j < kSimpleLower; ++j) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) lik[j][e] = 0.0;
+    if (j >= nl || !mk[j]) continue;
+    const int k = b0 + j;
+    double lk[9], dk[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      lk[e] = __ldg(a.val + size_t(k) * 9 + e);
+      dk[e] = a.dinv[size_t(ck[j]) * 9 + e];
+    }
+    mat3_mul(lk, dk, lik[j]);
+    if (up[j] >= 0 && md && __ldg(a.mask + up[j])) {
+      double u[9], prod[9];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) u[e] = a.lu[size_t(up[j]) * 9 + e];
+      mat3_mul(lik[j], u, prod);
+#pragma unroll
+      for (int e = 0; e < 9; ++e) D[e] -= prod[e];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kSimpleLower; ++j)
+    if (j < nl) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) a.lu[size_t(b0 + j) * 9 + e] = lik[j][e];
+    }
+  for (int k = dp + 1; k < b1; ++k) {
+    const bool m = __ldg(a.mask + k) != 0;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) a.lu[size_t(k) * 9 + e] = m ? __ldg(a.val + size_t(k) * 9 + e) : 0.0;
+  }
+#pragma unroll
+  for (int e = 0; e < 9; ++e) a.lu[size_t(dp) * 9 + e] = D[e];
+  mat3_inverse_or_diag(D, a.dinv + size_t(i) * 9);
+  // pressure ILU0: lower entries (no terms), the diagonal's terms in list order, upper entries
+  double pl[kSimpleLower];
+#pragma unroll
+  for (int j = 0; j < kSimpleLower; ++j) {
+    pl[j] = 0.0;
+    if (j < nl && pv[j] != 0.0) {
+      const double d = a.pdiag[ck[j]];
+      pl[j] = fabs(d) > kEps ? pv[j] / d : 0.0;
+    }
+    if (j < nl) a.plu[b0 + j] = pl[j];
+  }
+  const double de = __ldg(a.pval + dp);
+  double ud = de;
+  for (int e = __ldg(R.pt_ptr + dp); e < __ldg(R.pt_ptr + dp + 1); ++e) {
+    const int jl = __ldg(R.pt_lp + e) - b0;
+    double plp = 0.0, pvl = 0.0;
+#pragma unroll
+    for (int j = 0; j < kSimpleLower; ++j)
+      if (j == jl) {
+        plp = pl[j];
+        pvl = pv[j];
+      }
+    if (pvl == 0.0) continue;
+    ud -= plp * a.plu[__ldg(R.pt_ue + e)];
+  }
+  if (fabs(ud) <= kEps) ud = fabs(de) > kEps ? de : 1.0;
+  a.pdiag[i] = ud;
+  a.plu[dp] = 0.0;
+  for (int k = dp + 1; k < b1; ++k) {
+    const double v = __ldg(a.pval + k);
+    a.plu[k] = v == 0.0 ? 0.0 : v;
+  }
+}
+
 // Both ILU0 rows of a row of at most 32 blocks (a perforated cell's row with its well's fill) by
 // one warp, from the update lists: lane j holds entry b0 + j of the row in registers, so the
 // sequential walk over the row's lower entries costs shuffles instead of global round trips.
@@ -980,7 +1092,10 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_cluster(const __grid_cons
       const int r = L.lvl_rows[q];
       if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
       if (a.R.tri_ptr) {
-        ilu_row_recipe(r, a);
+        if (a.R.simple[r])
+          ilu_row_simple(r, a);
+        else
+          ilu_row_recipe(r, a);
       } else {
         block_ilu_row(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv);
         pressure_ilu_row(r, L.rp, L.col, L.diag, a.pval, a.plu, a.pdiag);
@@ -1021,7 +1136,10 @@ __global__ void __launch_bounds__(kFBlock, 1) k_factor_batch(const __grid_consta
       const int r = L.lvl_rows[q];
       if (L.rp[r + 1] - L.rp[r] > kLongRowBlocks) continue;  // a warp takes it below
       if (a.R.tri_ptr) {
-        ilu_row_recipe(r, a);
+        if (a.R.simple[r])
+          ilu_row_simple(r, a);
+        else
+          ilu_row_recipe(r, a);
       } else {
         block_ilu_row(r, L.rp, L.col, L.diag, a.val, a.mask, a.lu, a.dinv);
         pressure_ilu_row(r, L.rp, L.col, L.diag, a.pval, a.plu, a.pdiag);
@@ -2120,7 +2238,7 @@ static void cpr_build(Ctx& c) {
   const double* pval = c.d_pval.p;
   double* plu = c.d_plu.p;
   double* pdiag = c.d_pdiag.p;
-  FacRecipes rec{c.d_tri_ptr.p, c.d_tri_up.p, c.d_tri_ip.p, c.d_pt_ptr.p, c.d_pt_lp.p, c.d_pt_ue.p};
+  FacRecipes rec{c.d_tri_ptr.p, c.d_tri_up.p, c.d_tri_ip.p, c.d_pt_ptr.p, c.d_pt_lp.p, c.d_pt_ue.p, c.d_fac_simple.p};
   const FacArgs fa{L, val, mask, lu, dinv, pval, plu, pdiag, rec};
   if (c.batched && fiber_file(kBatchFactor, 0, &fa, sizeof(fa), kFBlock, 0)) {
     // filed with the group's batched launch
@@ -2669,6 +2787,23 @@ void build_factor_recipes(Ctx& c) {
     b.alloc(h.size());
     if (!h.empty()) RF_CUDA(cudaMemcpy(b.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
   };
+  // rows of the simple shape (ilu_row_simple): few lower entries, each updating only the
+  // diagonal, and pressure terms only on the diagonal
+  std::vector<unsigned char> simple(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const int b0 = c.h_row_ptr[i], dp = c.h_diag[i], b1 = c.h_row_ptr[i + 1];
+    bool ok = dp - b0 <= 4 && b1 - b0 <= kLongRowBlocks;  // kSimpleLower
+    for (int k = b0; ok && k < dp; ++k) {
+      const int cnt = tri_ptr[k + 1] - tri_ptr[k];
+      if (cnt > 1 || (cnt == 1 && tri_ip[tri_ptr[k]] != dp)) ok = false;
+    }
+    for (int k = b0; ok && k < b1; ++k)
+      if (k != dp && pt_ptr[k + 1] != pt_ptr[k]) ok = false;
+    simple[i] = ok ? 1 : 0;
+  }
+  c.d_fac_simple.free();
+  c.d_fac_simple.alloc(size_t(n));
+  RF_CUDA(cudaMemcpy(c.d_fac_simple.p, simple.data(), size_t(n), cudaMemcpyHostToDevice));
   up(c.d_tri_ptr, tri_ptr);
   up(c.d_tri_up, tri_up);
   up(c.d_tri_ip, tri_ip);
