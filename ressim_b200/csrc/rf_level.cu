@@ -11,10 +11,11 @@
 //   - a row of level l reads its dependencies from a shared-memory window holding the values of
 //     the level processed just before (l-1 forward, l+1 backward); the few rows a dependency
 //     reaches from further away (the wells' fill) are kept in a shared-memory cache;
-//   - the pressure solve copies the per-row data of the levels ahead (16-byte records of factor
-//     values, pivot and the dependencies' shared-memory indices, plus the input vectors) into
-//     shared memory with cp.async, `stages - 1` levels ahead of use, so a level step is a block
-//     barrier, shared-memory reads and the row arithmetic, with no branch per dependency;
+//   - the pressure solve copies the per-row data of the levels ahead (16-byte-aligned records of
+//     factor values, pivot and the dependencies' shared-memory indices, plus the input vectors)
+//     into shared memory with bulk copies that one thread issues per level, `stages - 1` levels
+//     ahead of use, so a level step is an mbarrier wait, a block barrier, shared-memory reads and
+//     the row arithmetic, with no branch per dependency;
 //   - the BiCGStab updates are fused into the sweeps that read them (the search direction p into
 //     the first forward sweep, s = r - alpha v and its norm into the second).
 // Every row is computed with the same operations in the same order as the natural-order
@@ -42,29 +43,8 @@ constexpr int kSpK = 7;  // pressure-matrix entries per row held in the fixed-wi
 __device__ __forceinline__ unsigned smem_u32a(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void cp_async(void* dst, const double* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async(void* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-// wait until at most `pending` of this thread's newest copy groups are still in flight
-__device__ __forceinline__ void cp_wait_dyn(int pending) {
-  switch (pending) {
-    case 0: cp_wait<0>(); break;
-    case 1: cp_wait<1>(); break;
-    case 2: cp_wait<2>(); break;
-    default: cp_wait<3>(); break;
-  }
-}
-
 // Per-position records of the pressure sweeps (rebuilt after each factorisation), copied into
-// shared memory with 16-byte cp.async: a 64-bit word with three dependency indices into the
+// shared memory a level at a time: a 64-bit word with three dependency indices into the
 // shared-memory array S (the two level windows, the far cache and a zero slot that absent entries
 // point at, their factor value being 0) and a meta field (bits 0-2 entry count, 7 = long row whose
 // index is the word's low 16 bits; bits 3-15 own far slot + 1), then the factor values in column
@@ -123,6 +103,7 @@ struct LvlArgs {
   T* sh;
   int max_iters;
   long long* iter_counter;
+  int* status;  // set to 3 when a wait for staged data gave up (may be null)
 };
 
 // Sums of two per-thread values over the block with a fixed tree; every thread gets both totals.
@@ -155,29 +136,69 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* red) {
   b = red[65];
 }
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32a(dst)), "l"(src) : "memory");
+// Staging of a level's records and inputs: one bulk copy per array (cp.async.bulk, global to
+// shared memory, completion counted in bytes on the stage's mbarrier), issued by one thread.
+// Both addresses must be 16-byte aligned and the size a multiple of 16 bytes: record arrays have
+// 16-byte-multiple records, and input vectors are copied from their 16-byte boundary below the
+// level's first position to the one above its last (the vectors are padded to that boundary).
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32a(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32a(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32a(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the phase of parity `parity` to complete; false when it gave up
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (int i = 0; i < (1 << 20); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32a(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32a(bar))
+               : "memory");
 }
 
-// Bytes of one staging slot: the level's records (the larger record type) and up to three input
-// vectors, rounded to 16 bytes.
+// Bytes of one staged input vector: a level's W values plus the alignment slack at both ends
+// (the copy runs from the 16-byte boundary below the level to the one above it), rounded to 16.
+template <class T>
+__host__ __device__ constexpr size_t lvl_in_bytes(int W) {
+  return ((size_t(W) + 2 * (16 / sizeof(T))) * sizeof(T) + 15) / 16 * 16;
+}
+// Bytes of one staging slot: the level's records (room for the larger record type) and up to three
+// input vectors.
 template <class T>
 __host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
-  return (size_t(W) * (sizeof(BRec<T>) + 3 * sizeof(T)) + 15) / 16 * 16;
+  return size_t(W) * sizeof(BRec<T>) + 3 * lvl_in_bytes<T>(W);
 }
 
 // One triangular sweep over all levels.  MODE 0: forward sweep of p = r + beta (p - omega v)
 // (p = r on the first iteration), p stored; MODE 1: forward sweep of s = r - alpha v, s stored and
 // its squares summed into acc; MODE 2: backward sweep of y.  The result goes to `out` (position
-// order).  Each thread handles the offsets t, t + NT, ... of every level and stages exactly those
-// offsets' data, so the staging needs no barrier of its own.  S holds the window of level l at
-// S[(l & 1) W ..], the far cache at S[2W ..] and the zero slot after it; sl is the level pointers.
+// order).  With D > 0 stages, thread 0 copies each level's records and inputs `D - 1` levels ahead
+// into a ring of D slots (bulk copies completing on the slot's mbarrier), and every thread waits
+// on the mbarrier before the level; a slot is refilled only after the block barrier that ends the
+// level that read it.  `phase` holds each slot's mbarrier parity across sweeps.  S holds the window
+// of level l at S[(l & 1) W ..], the far cache at S[2W ..] and the zero slot after it; sl is the
+// level pointers.
 template <class T, int MODE>
-__device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const int* sl, T* out, double& acc,
-                          double beta, double omega, double alpha, bool first) {
+__device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, unsigned long long* mbar, unsigned& phase,
+                          T* S, const int* sl, T* out, double& acc, double beta, double omega, double alpha,
+                          bool first) {
   constexpr bool FWD = MODE != 2;
   constexpr size_t RB = FWD ? sizeof(FRec<T>) : sizeof(BRec<T>);
-  constexpr size_t RMAX = sizeof(BRec<T>);
+  constexpr int E = 16 / int(sizeof(T));  // values per 16 bytes
   const int NT = a.threads, L = a.L, W = a.width, D = a.stages;
   const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   const unsigned char* recs = FWD ? reinterpret_cast<const unsigned char*>(a.frec)
@@ -189,51 +210,48 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
   const T* in1 = a.v;
   const T* in2 = a.p;
   const size_t slot_bytes = lvl_slot_bytes<T>(W);
+  const size_t in_off = size_t(W) * sizeof(BRec<T>), in_bytes = lvl_in_bytes<T>(W);
   auto level_at = [&](int k) { return FWD ? k : L - 1 - k; };
   auto issue = [&](int k, int slot) {
-    if (k >= L) return;
+    if (k >= L || threadIdx.x != 0) return;
     const int l = level_at(k), lst = sl[l], w = sl[l + 1] - lst;
     unsigned char* base = stage + size_t(slot) * slot_bytes;
-    T* inp = reinterpret_cast<T*>(base + size_t(W) * RMAX);
-    for (int off = t; off < w; off += NT) {
-      const int q = lst + off;
-      const unsigned char* src = recs + size_t(q) * RB;
-      unsigned char* dst = base + size_t(off) * RMAX;
-#pragma unroll
-      for (int b = 0; b < int(RB / 16); ++b) cp_async16(dst + 16 * b, src + 16 * b);
-      cp_async(inp + off, in0 + q);
-      if (MODE != 2) cp_async(inp + W + off, in1 + q);
-      if (MODE == 0) cp_async(inp + 2 * W + off, in2 + q);
-    }
+    const int a0 = lst & ~(E - 1), a1 = (lst + w + E - 1) & ~(E - 1);
+    const unsigned rb = unsigned(size_t(w) * RB), ib = unsigned(size_t(a1 - a0) * sizeof(T));
+    constexpr int nin = MODE == 0 ? 3 : MODE == 1 ? 2 : 1;
+    // the slot was last read by the level before this one, finished at the block barrier
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(mbar + slot, rb + nin * ib);
+    bulk_g2s(base, recs + size_t(lst) * RB, rb, mbar + slot);
+    bulk_g2s(base + in_off, in0 + a0, ib, mbar + slot);
+    if (MODE != 2) bulk_g2s(base + in_off + in_bytes, in1 + a0, ib, mbar + slot);
+    if (MODE == 0) bulk_g2s(base + in_off + 2 * in_bytes, in2 + a0, ib, mbar + slot);
   };
   int s_iss = 0, s_cur = 0;
   if (D > 0) {
-    for (int k = 0; k < D - 1; ++k) {
-      issue(k, k);
-      cp_commit();
-    }
+    for (int k = 0; k < D - 1; ++k) issue(k, k);
     s_iss = D - 1;
   }
   T* far = S + 2 * size_t(W);
   for (int k = 0; k < L; ++k) {
     const int l = level_at(k), lst = sl[l], w = sl[l + 1] - lst;
     const unsigned char* rbase;
-    const T* inp;
-    size_t rstride;
+    const T *inp0 = nullptr, *inp1 = nullptr, *inp2 = nullptr;
     if (D > 0) {
       issue(k + D - 1, s_iss);
-      cp_commit();
-      cp_wait_dyn(D - 1);
       s_iss = s_iss + 1 == D ? 0 : s_iss + 1;
+      if (!mbar_wait(mbar + s_cur, (phase >> s_cur) & 1u) && a.status) atomicExch(a.status, 3);
+      phase ^= 1u << s_cur;
       rbase = stage + size_t(s_cur) * slot_bytes;
-      inp = reinterpret_cast<const T*>(rbase + size_t(W) * RMAX);
-      rstride = RMAX;
+      const int sh = lst & (E - 1);
+      inp0 = reinterpret_cast<const T*>(rbase + in_off) + sh;
+      inp1 = reinterpret_cast<const T*>(rbase + in_off + in_bytes) + sh;
+      inp2 = reinterpret_cast<const T*>(rbase + in_off + 2 * in_bytes) + sh;
       s_cur = s_cur + 1 == D ? 0 : s_cur + 1;
     } else {
       rbase = recs + size_t(lst) * RB;
-      inp = nullptr;
-      rstride = RB;
     }
+    const size_t rstride = RB;
     T* cur = S + size_t(l & 1) * W;
     // A thread's rows of one level read only earlier levels (the window of the previous level and
     // the far cache), never each other, so its rows are taken in pairs (offsets off and off + NT):
@@ -254,13 +272,13 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
       R.v1 = v[1];
       R.v2 = v[2];
       R.v3 = MODE == 2 ? v[3] : T(0);
-      const T x0 = inp ? inp[off] : in0[R.q];
+      const T x0 = inp0 ? inp0[off] : in0[R.q];
       if (MODE == 0) {
-        const T x1 = inp ? inp[W + off] : in1[R.q];
-        const T x2 = inp ? inp[2 * W + off] : in2[R.q];
+        const T x1 = inp1 ? inp1[off] : in1[R.q];
+        const T x2 = inp2 ? inp2[off] : in2[R.q];
         R.pre = first ? x0 : T(double(x0) + beta * (double(x2) - omega * double(x1)));
       } else if (MODE == 1) {
-        const T x1 = inp ? inp[W + off] : in1[R.q];
+        const T x1 = inp1 ? inp1[off] : in1[R.q];
         R.pre = T(double(x0) - alpha * double(x1));
       } else {
         R.pre = x0;
@@ -311,7 +329,6 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, T* S, const
     }
     __syncthreads();
   }
-  if (D > 0) cp_wait<0>();
 }
 
 // out = A in (pressure matrix, position space), with the dot products the solve needs next:
@@ -374,14 +391,20 @@ __device__ void lvl_spmv(const LvlArgs<T>& a, const T* in, T* out, double& acc0,
 // thread block.  Dot products accumulate in double and the iterate is kept in double for either
 // storage type T, as in the cluster kernels.
 template <class T>
-__device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem, double* red) {
+__device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem, double* red,
+                                    unsigned long long* mbar) {
   const int W = a.width, n = a.n, NT = a.threads;
   const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   unsigned char* stage = lvl_smem;
   T* S = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * lvl_slot_bytes<T>(W));
   int* sl = reinterpret_cast<int*>(S + 2 * size_t(W) + a.nfar + 1);
   for (int l = threadIdx.x; l <= a.L; l += blockDim.x) sl[l] = a.lstart[l];
-  if (threadIdx.x == 0) S[2 * size_t(W) + a.nfar] = T(0);  // the zero slot
+  if (threadIdx.x == 0) {
+    S[2 * size_t(W) + a.nfar] = T(0);  // the zero slot
+    for (int k = 0; k < a.stages; ++k) mbar_init(mbar + k, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  unsigned phase = 0;  // parity of each staging slot's mbarrier
   double d0 = 0.0, d1 = 0.0;
   for (int q = t; q < n; q += NT) {
     const double ri = a.rhs[a.pos_row[q]] - 0.0;
@@ -405,8 +428,8 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     const double beta = it == 0 ? 0.0 : (rho / rho_prev) * (alpha / omega);
     d0 = 0.0;
     d1 = 0.0;
-    lvl_sweep<T, 0>(a, stage, S, sl, a.y, d0, beta, omega, 0.0, it == 0);
-    lvl_sweep<T, 2>(a, stage, S, sl, a.ph, d0, 0.0, 0.0, 0.0, false);
+    lvl_sweep<T, 0>(a, stage, mbar, phase, S, sl, a.y, d0, beta, omega, 0.0, it == 0);
+    lvl_sweep<T, 2>(a, stage, mbar, phase, S, sl, a.ph, d0, 0.0, 0.0, 0.0, false);
     lvl_spmv<T, 0>(a, a.ph, a.v, d0, d1);
     block_sum2(d0, d1, red);
     const double vd = d0;
@@ -414,13 +437,13 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     alpha = rho / vd;
     d0 = 0.0;
     d1 = 0.0;
-    lvl_sweep<T, 1>(a, stage, S, sl, a.y, d0, 0.0, 0.0, alpha, false);
+    lvl_sweep<T, 1>(a, stage, mbar, phase, S, sl, a.y, d0, 0.0, 0.0, alpha, false);
     block_sum2(d0, d1, red);
     if (sqrt(d0) <= tol) {
       for (int q = t; q < n; q += NT) a.xq[q] += alpha * double(a.ph[q]);
       break;
     }
-    lvl_sweep<T, 2>(a, stage, S, sl, a.sh, d0, 0.0, 0.0, 0.0, false);
+    lvl_sweep<T, 2>(a, stage, mbar, phase, S, sl, a.sh, d0, 0.0, 0.0, 0.0, false);
     d0 = 0.0;
     d1 = 0.0;
     lvl_spmv<T, 1>(a, a.sh, a.t, d0, d1);
@@ -471,7 +494,8 @@ template <class T>
 __global__ void __launch_bounds__(kLvlMaxThreads, 1) k_bicgstab_level(const __grid_constant__ LvlArgs<T> a) {
   extern __shared__ __align__(16) unsigned char lvl_smem[];
   __shared__ double red[72];
-  bicgstab_level_body(a, lvl_smem, red);
+  __shared__ unsigned long long mbar[kLvlMaxStages];
+  bicgstab_level_body(a, lvl_smem, red, mbar);
 }
 
 // Many independent pressure solves in one launch: thread block b solves item b (every item lays
@@ -485,7 +509,8 @@ template <class T>
 __global__ void __launch_bounds__(kLvlMaxThreads, 1) k_bicgstab_level_batch(const __grid_constant__ LvlBatch<T> b) {
   extern __shared__ __align__(16) unsigned char lvl_smem[];
   __shared__ double red[72];
-  if (blockIdx.x < unsigned(b.count)) bicgstab_level_body(b.item[blockIdx.x], lvl_smem, red);
+  __shared__ unsigned long long mbar[kLvlMaxStages];
+  if (blockIdx.x < unsigned(b.count)) bicgstab_level_body(b.item[blockIdx.x], lvl_smem, red, mbar);
 }
 
 // ============================================================================================
@@ -667,6 +692,9 @@ __global__ void k_lvl_pack_rec(int n, const unsigned long long* __restrict__ fwo
   frec[q] = f;
   brec[q] = b;
 }
+
+// values per position-order vector of the solve's scratch: n rounded up to a multiple of 4
+inline size_t lvl_work_pad(int n) { return (size_t(n) + 3) / 4 * 4; }
 
 template <class T>
 size_t lvl_smem_bytes(int W, int stages, int nfar, int L) {
@@ -923,7 +951,10 @@ void build_level_plan(Ctx& c) {
   P.d_vals64.free();
   P.d_vals32.free();
   P.d_work.free();
-  P.work_bytes = size_t(n) * (9 * sizeof(double) + sizeof(double));
+  // ten position-order vectors (the iterate in double, nine of the solve's type), each padded to
+  // a multiple of four values so every vector starts on a 16-byte boundary and the staging's bulk
+  // copies, rounded out to 16-byte boundaries, stay inside the buffer
+  P.work_bytes = lvl_work_pad(n) * (9 * sizeof(double) + sizeof(double)) + 64;
   P.d_work.alloc(P.work_bytes);
   P.d_blk_y.free();
   P.d_blk_y.alloc(3 * size_t(n) * sizeof(double));
@@ -1098,20 +1129,22 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.splongval = vals + g.splong;
   a.rhs = rhs;
   a.x = x;
+  const size_t np = lvl_work_pad(n);
   double* xq = reinterpret_cast<double*>(P.d_work.p);
-  T* vb = reinterpret_cast<T*>(P.d_work.p + sizeof(double) * size_t(n));
+  T* vb = reinterpret_cast<T*>(P.d_work.p + sizeof(double) * np);
   a.xq = xq;
   a.r = vb;
-  a.rh = vb + size_t(n);
-  a.p = vb + 2 * size_t(n);
-  a.v = vb + 3 * size_t(n);
-  a.s = vb + 4 * size_t(n);
-  a.t = vb + 5 * size_t(n);
-  a.y = vb + 6 * size_t(n);
-  a.ph = vb + 7 * size_t(n);
-  a.sh = vb + 8 * size_t(n);
+  a.rh = vb + np;
+  a.p = vb + 2 * np;
+  a.v = vb + 3 * np;
+  a.s = vb + 4 * np;
+  a.t = vb + 5 * np;
+  a.y = vb + 6 * np;
+  a.ph = vb + 7 * np;
+  a.sh = vb + 8 * np;
   a.max_iters = 50;
   a.iter_counter = c.d_bicg_iters;
+  a.status = c.d_pipe_status.p;
   a.threads = P.threads[f];
   if (c.batched && submit_item(kBatchPressure, f, &a, sizeof(a), P.threads[f], P.smem[f])) return;
   c.launches++;
