@@ -934,6 +934,29 @@ def main():
         pg.barrier()
     value = world * n * args.steps / (dev_ms_max / 1e3)
 
+    # ---- mixed form: the plain FP64 path on the same report steps, and the field error ----
+    fp64_cmp = None
+    if args.precision == "mixed":
+        ref = ReservoirSimulator.from_deck(deck)
+        for _ in range(args.warmup):
+            ref.step(dt)
+        ref_ms = 0.0
+        ref_newton = 0
+        for _ in range(args.steps):
+            l2_flush()
+            r = ref.step(dt)
+            ref_ms += r["device_ms"]
+            ref_newton += r["newton_iterations"]
+        a, b = sim.state(), ref.state()
+        ref.close()
+        fp64_cmp = {"fp64_value": n * args.steps / (ref_ms / 1e3), "mixed_over_fp64": (n * args.steps / (dev_ms / 1e3))
+                    / (n * args.steps / (ref_ms / 1e3)), "fp64_newton_iterations": ref_newton,
+                    "field_error_mixed_vs_fp64": {
+                        "pressure_rel": float(np.max(np.abs(a["pressure"] - b["pressure"]) /
+                                                     np.maximum(np.abs(b["pressure"]), 1.0))),
+                        "sat_water_abs": float(np.max(np.abs(a["sat_water"] - b["sat_water"])))},
+                    "profile": "the reference's tolerances on both; the same warm-up and timed report steps"}
+
     # ---- end-to-end leg: host buffers, copies inside the timed region ----
     # A second simulator of the same deck takes the same warm-up steps (the path is deterministic),
     # so the timed steps here are the same report steps as in the device-resident leg.
@@ -1035,6 +1058,7 @@ def main():
                     "d2h_bytes_per_step": len(keys) * 8 * n},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
             "phase_ms": phases, "precision": args.precision, "field_error_vs_oracle": field_err,
+            "mixed_vs_fp64": fp64_cmp,
         }
         print(json.dumps(line), flush=True)
     sim.close()
