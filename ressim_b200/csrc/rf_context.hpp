@@ -64,6 +64,7 @@ struct DBuf {
 struct LevelPlan {
   int built = 0;          // structure present
   int n_levels = 0, width = 0, nfar_f = 0, nfar_b = 0, n_flong = 0, n_blong = 0, nnz = 0;
+  int n_flong_rows = 0, n_blong_rows = 0;  // rows behind the n_flong / n_blong long entries
   DBuf<int> d_lstart, d_pos_row;
   DBuf<unsigned long long> d_fcode, d_bcode;
   DBuf<int> d_flong_ptr, d_blong_ptr;                  // long rows: entry ranges

@@ -68,12 +68,11 @@ struct LvlArgs {
                 // take part in the barriers, so the solve is the same as its own launch's)
   const int* lstart;   // [L + 1] first position of each level
   const int* pos_row;  // [n] natural row of each position
-  const unsigned long long* fcode;  // [n] forward (lower part) code words
-  const unsigned long long* bcode;  // [n] backward (upper part) code words
-  const int* flong_ptr;
-  const unsigned short* flong_code;
-  const int* blong_ptr;
-  const unsigned short* blong_code;
+  // rows with more than three entries in a sweep direction (the wells' fill): entry ranges,
+  // copied into shared memory with their indices and values at the start of a solve
+  int n_flong_rows, n_blong_rows, n_flong, n_blong;  // rows and entries, forward and backward
+  const int* flong_ptr;  // [n_flong_rows + 1]
+  const int* blong_ptr;  // [n_blong_rows + 1]
   // pressure matrix in position space: rows of at most kSpK entries as [kSpK][n] column positions
   // (-1: no entry; -2 in slot 0: a longer row, listed separately) and values, in column order
   const int* sp_col;
@@ -182,6 +181,50 @@ template <class T>
 __host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
   return size_t(W) * sizeof(BRec<T>) + 3 * lvl_in_bytes<T>(W);
 }
+__host__ __device__ constexpr size_t lvl_up16(size_t x) { return (x + 15) / 16 * 16; }
+// Bytes of the two level windows, the far cache and the zero slot.
+template <class T>
+__host__ __device__ constexpr size_t lvl_win_bytes(int W, int nfar) {
+  return lvl_up16((2 * size_t(W) + size_t(nfar) + 1) * sizeof(T));
+}
+// Counts of the long rows (rows and entries, forward and backward) and the byte offsets of their
+// shared-memory copy: values, entry ranges, dependency indices.
+struct LvlArgsLong {
+  int fr, br, fe, be;
+};
+struct LvlLongLayout {
+  size_t fval, bval, fptr, bptr, fidx, bidx, total;
+};
+template <class T>
+__host__ __device__ inline LvlLongLayout lvl_long_layout(const LvlArgsLong& g) {
+  LvlLongLayout o;
+  size_t p = 0;
+  o.fval = p;
+  p += lvl_up16(size_t(g.fe) * sizeof(T));
+  o.bval = p;
+  p += lvl_up16(size_t(g.be) * sizeof(T));
+  o.fptr = p;
+  p += lvl_up16((size_t(g.fr) + 1) * sizeof(int));
+  o.bptr = p;
+  p += lvl_up16((size_t(g.br) + 1) * sizeof(int));
+  o.fidx = p;
+  p += lvl_up16(size_t(g.fe) * sizeof(unsigned short));
+  o.bidx = p;
+  p += lvl_up16(size_t(g.be) * sizeof(unsigned short));
+  o.total = p;
+  return o;
+}
+
+// The long rows' entry ranges, dependency indices and values in shared memory.
+template <class T>
+struct LvlLongSm {
+  const int* fptr;
+  const int* bptr;
+  const unsigned short* fidx;
+  const unsigned short* bidx;
+  const T* fval;
+  const T* bval;
+};
 
 // One triangular sweep over all levels.  MODE 0: forward sweep of p = r + beta (p - omega v)
 // (p = r on the first iteration), p stored; MODE 1: forward sweep of s = r - alpha v, s stored and
@@ -194,8 +237,8 @@ __host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
 // level pointers.
 template <class T, int MODE>
 __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, unsigned long long* mbar, unsigned& phase,
-                          T* S, const int* sl, T* out, double& acc, double beta, double omega, double alpha,
-                          bool first) {
+                          T* S, const int* sl, const LvlLongSm<T>& lg, T* out, double& acc, double beta,
+                          double omega, double alpha, bool first) {
   constexpr bool FWD = MODE != 2;
   constexpr size_t RB = FWD ? sizeof(FRec<T>) : sizeof(BRec<T>);
   constexpr int E = 16 / int(sizeof(T));  // values per 16 bytes
@@ -203,9 +246,9 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, unsigned lo
   const int t = int(threadIdx.x) < NT ? int(threadIdx.x) : (1 << 30);  // idle threads: barriers only
   const unsigned char* recs = FWD ? reinterpret_cast<const unsigned char*>(a.frec)
                                   : reinterpret_cast<const unsigned char*>(a.brec);
-  const int* lptr = FWD ? a.flong_ptr : a.blong_ptr;
-  const unsigned short* lidx = FWD ? a.flong_abs : a.blong_abs;
-  const T* lval = FWD ? a.flong_val : a.blong_val;
+  const int* lptr = FWD ? lg.fptr : lg.bptr;
+  const unsigned short* lidx = FWD ? lg.fidx : lg.bidx;
+  const T* lval = FWD ? lg.fval : lg.bval;
   const T* in0 = MODE == 2 ? a.y : a.r;
   const T* in1 = a.v;
   const T* in2 = a.p;
@@ -399,6 +442,30 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
   T* S = reinterpret_cast<T*>(lvl_smem + size_t(a.stages) * lvl_slot_bytes<T>(W));
   int* sl = reinterpret_cast<int*>(S + 2 * size_t(W) + a.nfar + 1);
   for (int l = threadIdx.x; l <= a.L; l += blockDim.x) sl[l] = a.lstart[l];
+  // the long rows, copied once per solve (their values change with every factorisation)
+  const LvlLongLayout lo = lvl_long_layout<T>(LvlArgsLong{a.n_flong_rows, a.n_blong_rows, a.n_flong, a.n_blong});
+  unsigned char* lbase = reinterpret_cast<unsigned char*>(S) + lvl_win_bytes<T>(W, a.nfar) +
+                         lvl_up16(sizeof(int) * (size_t(a.L) + 1));
+  LvlLongSm<T> lg;
+  {
+    T* fv = reinterpret_cast<T*>(lbase + lo.fval);
+    T* bv = reinterpret_cast<T*>(lbase + lo.bval);
+    int* fp = reinterpret_cast<int*>(lbase + lo.fptr);
+    int* bp = reinterpret_cast<int*>(lbase + lo.bptr);
+    unsigned short* fi = reinterpret_cast<unsigned short*>(lbase + lo.fidx);
+    unsigned short* bi = reinterpret_cast<unsigned short*>(lbase + lo.bidx);
+    for (int e = threadIdx.x; e < a.n_flong; e += blockDim.x) {
+      fv[e] = a.flong_val[e];
+      fi[e] = a.flong_abs[e];
+    }
+    for (int e = threadIdx.x; e < a.n_blong; e += blockDim.x) {
+      bv[e] = a.blong_val[e];
+      bi[e] = a.blong_abs[e];
+    }
+    for (int r = threadIdx.x; r <= a.n_flong_rows; r += blockDim.x) fp[r] = a.flong_ptr[r];
+    for (int r = threadIdx.x; r <= a.n_blong_rows; r += blockDim.x) bp[r] = a.blong_ptr[r];
+    lg = LvlLongSm<T>{fp, bp, fi, bi, fv, bv};
+  }
   if (threadIdx.x == 0) {
     S[2 * size_t(W) + a.nfar] = T(0);  // the zero slot
     for (int k = 0; k < a.stages; ++k) mbar_init(mbar + k, 1);
@@ -428,8 +495,8 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     const double beta = it == 0 ? 0.0 : (rho / rho_prev) * (alpha / omega);
     d0 = 0.0;
     d1 = 0.0;
-    lvl_sweep<T, 0>(a, stage, mbar, phase, S, sl, a.y, d0, beta, omega, 0.0, it == 0);
-    lvl_sweep<T, 2>(a, stage, mbar, phase, S, sl, a.ph, d0, 0.0, 0.0, 0.0, false);
+    lvl_sweep<T, 0>(a, stage, mbar, phase, S, sl, lg, a.y, d0, beta, omega, 0.0, it == 0);
+    lvl_sweep<T, 2>(a, stage, mbar, phase, S, sl, lg, a.ph, d0, 0.0, 0.0, 0.0, false);
     lvl_spmv<T, 0>(a, a.ph, a.v, d0, d1);
     block_sum2(d0, d1, red);
     const double vd = d0;
@@ -437,13 +504,13 @@ __device__ void bicgstab_level_body(const LvlArgs<T>& a, unsigned char* lvl_smem
     alpha = rho / vd;
     d0 = 0.0;
     d1 = 0.0;
-    lvl_sweep<T, 1>(a, stage, mbar, phase, S, sl, a.y, d0, 0.0, 0.0, alpha, false);
+    lvl_sweep<T, 1>(a, stage, mbar, phase, S, sl, lg, a.y, d0, 0.0, 0.0, alpha, false);
     block_sum2(d0, d1, red);
     if (sqrt(d0) <= tol) {
       for (int q = t; q < n; q += NT) a.xq[q] += alpha * double(a.ph[q]);
       break;
     }
-    lvl_sweep<T, 2>(a, stage, mbar, phase, S, sl, a.sh, d0, 0.0, 0.0, 0.0, false);
+    lvl_sweep<T, 2>(a, stage, mbar, phase, S, sl, lg, a.sh, d0, 0.0, 0.0, 0.0, false);
     d0 = 0.0;
     d1 = 0.0;
     lvl_spmv<T, 1>(a, a.sh, a.t, d0, d1);
@@ -697,9 +764,9 @@ __global__ void k_lvl_pack_rec(int n, const unsigned long long* __restrict__ fwo
 inline size_t lvl_work_pad(int n) { return (size_t(n) + 3) / 4 * 4; }
 
 template <class T>
-size_t lvl_smem_bytes(int W, int stages, int nfar, int L) {
-  const size_t win = ((2 * size_t(W) + size_t(nfar) + 1) * sizeof(T) + 15) / 16 * 16;
-  return size_t(stages) * lvl_slot_bytes<T>(W) + win + sizeof(int) * (size_t(L) + 1);
+size_t lvl_smem_bytes(int W, int stages, int nfar, int L, const LvlArgsLong& lg) {
+  return size_t(stages) * lvl_slot_bytes<T>(W) + lvl_win_bytes<T>(W, nfar) + lvl_up16(sizeof(int) * (size_t(L) + 1)) +
+         lvl_long_layout<T>(lg).total;
 }
 
 // offsets of the packed value segments (elements)
@@ -750,12 +817,13 @@ void choose_shape(Ctx& c, int f) {
   const size_t budget = size_t(optin) > fa.sharedSizeBytes + 1024 ? size_t(optin) - fa.sharedSizeBytes - 1024 : 0;
   const int nfar = std::max(P.nfar_f, P.nfar_b);
   P.fits[f] = 0;
-  if (lvl_smem_bytes<T>(P.width, 0, nfar, P.n_levels) > budget) return;
+  const LvlArgsLong lg{P.n_flong_rows, P.n_blong_rows, P.n_flong, P.n_blong};
+  if (lvl_smem_bytes<T>(P.width, 0, nfar, P.n_levels, lg) > budget) return;
   int st = kLvlMaxStages;
-  while (st > 0 && lvl_smem_bytes<T>(P.width, st, nfar, P.n_levels) > budget) --st;
+  while (st > 0 && lvl_smem_bytes<T>(P.width, st, nfar, P.n_levels, lg) > budget) --st;
   if (st == 1) st = 0;  // one stage only re-reads what it just copied: direct loads do the same
   P.stages[f] = st;
-  P.smem[f] = lvl_smem_bytes<T>(P.width, st, nfar, P.n_levels);
+  P.smem[f] = lvl_smem_bytes<T>(P.width, st, nfar, P.n_levels, lg);
   P.threads[f] = auto_threads(c);
   raise_dynamic_smem((const void*)k_bicgstab_level<T>, P.smem[f]);
   raise_dynamic_smem((const void*)k_bicgstab_level_batch<T>, P.smem[f]);
@@ -879,6 +947,8 @@ void build_level_plan(Ctx& c) {
   P.nfar_b = nfb;
   P.n_flong = int(flong_map.size());
   P.n_blong = int(blong_map.size());
+  P.n_flong_rows = int(flong_ptr.size()) - 1;
+  P.n_blong_rows = int(blong_ptr.size()) - 1;
   P.nnz = c.h_row_ptr[n];
   fmap.insert(fmap.end(), flong_map.begin(), flong_map.end());
   fmap.insert(fmap.end(), blong_map.begin(), blong_map.end());
@@ -1107,12 +1177,12 @@ static void launch_level(Ctx& c, const double* rhs, double* x) {
   a.stages = P.stages[f];
   a.lstart = P.d_lstart.p;
   a.pos_row = P.d_pos_row.p;
-  a.fcode = P.d_fcode.p;
-  a.bcode = P.d_bcode.p;
+  a.n_flong_rows = P.n_flong_rows;
+  a.n_blong_rows = P.n_blong_rows;
+  a.n_flong = P.n_flong;
+  a.n_blong = P.n_blong;
   a.flong_ptr = P.d_flong_ptr.p;
-  a.flong_code = P.d_flong_code.p;
   a.blong_ptr = P.d_blong_ptr.p;
-  a.blong_code = P.d_blong_code.p;
   a.sp_col = P.d_sp_col.p;
   a.n_splong = P.n_splong;
   a.splong_row = P.d_splong_row.p;
