@@ -2075,11 +2075,23 @@ __global__ void __launch_bounds__(1024) k_dense_lu(int n, double* a, int* perm, 
   }
   __syncthreads();
   for (int c = 0; c < n; ++c) {
-    // every thread reduces the warps' partials in warp order: the same pivot everywhere
+    // every warp reduces the warps' partials (lane w takes warp w's) by the same butterfly and
+    // takes lane 0's result: the same pivot everywhere.  piv_better is a total order (largest
+    // value, then smallest row), so the order of the reduction does not change the pivot.
     double bv = 0.0;
     int piv = -1;
-    for (int w = 0; w < nwarps; ++w)
-      if (s_row[w] >= 0) piv_better(s_val[w], s_row[w], bv, piv);
+    if (lane < nwarps && s_row[lane] >= 0) {
+      bv = s_val[lane];
+      piv = s_row[lane];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int orr = __shfl_xor_sync(0xffffffffu, piv, o);
+      if (orr >= 0) piv_better(ov, orr, bv, piv);
+    }
+    bv = __shfl_sync(0xffffffffu, bv, 0);
+    piv = __shfl_sync(0xffffffffu, piv, 0);
     if (piv < 0 || bv == 0.0) {  // |a_piv,c| of the partials: an exactly zero pivot
       if (t == 0) ok[0] = 0;
       return;  // uniform: every thread saw the same partials
