@@ -451,10 +451,10 @@ def ensemble_roofline(ds, profs, peak, peak_kind, batch=None):
 
 
 def matched_comparison(ds, dt, sample):
-    """The north-star comparison on the ensemble at the matched profile (Newton accepted at CNV 1e-8
-    / MB 1e-10 and every CPR-FGMRES solve refined to 1e-10 relative on both paths, the reference's
-    controller otherwise): the batched mixed form over all
-    variants against the plain FP64 path stepping variants one at a time through rf_step.  One
+    """Batched mixed against plain FP64 on the ensemble at the matched profile (Newton accepted at
+    CNV 1e-8 / MB 1e-10 and every CPR-FGMRES solve refined to 1e-10 relative on both paths, the
+    reference's controller otherwise): the batched mixed form over all variants against the plain
+    FP64 path stepping variants one at a time through rf_step.  One
     untimed and one timed report step each; the plain path runs on `sample` (variants spread over
     the size range), the batched path on all of them; field error of the batched mixed states
     against the plain FP64 ones on the sample."""
