@@ -27,6 +27,7 @@
 #include <mutex>
 
 #include "rf_fiber.hpp"
+#include "rf_level_layout.hpp"
 #include "rf_ops.hpp"
 
 namespace rf {
@@ -43,24 +44,6 @@ constexpr int kSpK = 7;  // pressure-matrix entries per row held in the fixed-wi
 __device__ __forceinline__ unsigned smem_u32a(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
-// Per-position records of the pressure sweeps (rebuilt after each factorisation), copied into
-// shared memory a level at a time: a 64-bit word with three dependency indices into the
-// shared-memory array S (the two level windows, the far cache and a zero slot that absent entries
-// point at, their factor value being 0) and a meta field (bits 0-2 entry count, 7 = long row whose
-// index is the word's low 16 bits; bits 3-15 own far slot + 1), then the factor values in column
-// order (and the pivot for the backward sweep).
-template <class T>
-struct alignas(16) FRec {
-  unsigned long long word;
-  T v[3];
-};
-template <class T>
-struct alignas(16) BRec {
-  unsigned long long word;
-  T v[3];
-  T piv;
-};
-
 template <class T>
 struct LvlArgs {
   int n, L, width, stages, nfar;
@@ -169,52 +152,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-// Bytes of one staged input vector: a level's W values plus the alignment slack at both ends
-// (the copy runs from the 16-byte boundary below the level to the one above it), rounded to 16.
-template <class T>
-__host__ __device__ constexpr size_t lvl_in_bytes(int W) {
-  return ((size_t(W) + 2 * (16 / sizeof(T))) * sizeof(T) + 15) / 16 * 16;
-}
-// Bytes of one staging slot: the level's records (room for the larger record type) and up to three
-// input vectors.
-template <class T>
-__host__ __device__ constexpr size_t lvl_slot_bytes(int W) {
-  return size_t(W) * sizeof(BRec<T>) + 3 * lvl_in_bytes<T>(W);
-}
-__host__ __device__ constexpr size_t lvl_up16(size_t x) { return (x + 15) / 16 * 16; }
-// Bytes of the two level windows, the far cache and the zero slot.
-template <class T>
-__host__ __device__ constexpr size_t lvl_win_bytes(int W, int nfar) {
-  return lvl_up16((2 * size_t(W) + size_t(nfar) + 1) * sizeof(T));
-}
-// Counts of the long rows (rows and entries, forward and backward) and the byte offsets of their
-// shared-memory copy: values, entry ranges, dependency indices.
-struct LvlArgsLong {
-  int fr, br, fe, be;
-};
-struct LvlLongLayout {
-  size_t fval, bval, fptr, bptr, fidx, bidx, total;
-};
-template <class T>
-__host__ __device__ inline LvlLongLayout lvl_long_layout(const LvlArgsLong& g) {
-  LvlLongLayout o;
-  size_t p = 0;
-  o.fval = p;
-  p += lvl_up16(size_t(g.fe) * sizeof(T));
-  o.bval = p;
-  p += lvl_up16(size_t(g.be) * sizeof(T));
-  o.fptr = p;
-  p += lvl_up16((size_t(g.fr) + 1) * sizeof(int));
-  o.bptr = p;
-  p += lvl_up16((size_t(g.br) + 1) * sizeof(int));
-  o.fidx = p;
-  p += lvl_up16(size_t(g.fe) * sizeof(unsigned short));
-  o.bidx = p;
-  p += lvl_up16(size_t(g.be) * sizeof(unsigned short));
-  o.total = p;
-  return o;
-}
-
 // The long rows' entry ranges, dependency indices and values in shared memory.
 template <class T>
 struct LvlLongSm {
@@ -259,7 +196,8 @@ __device__ void lvl_sweep(const LvlArgs<T>& a, unsigned char* stage, unsigned lo
     if (k >= L || threadIdx.x != 0) return;
     const int l = level_at(k), lst = sl[l], w = sl[l + 1] - lst;
     unsigned char* base = stage + size_t(slot) * slot_bytes;
-    const int a0 = lst & ~(E - 1), a1 = (lst + w + E - 1) & ~(E - 1);
+    int a0, a1;
+    lvl_input_span(lst, w, E, a0, a1);
     const unsigned rb = unsigned(size_t(w) * RB), ib = unsigned(size_t(a1 - a0) * sizeof(T));
     constexpr int nin = MODE == 0 ? 3 : MODE == 1 ? 2 : 1;
     // the slot was last read by the level before this one, finished at the block barrier
@@ -759,9 +697,6 @@ __global__ void k_lvl_pack_rec(int n, const unsigned long long* __restrict__ fwo
   frec[q] = f;
   brec[q] = b;
 }
-
-// values per position-order vector of the solve's scratch: n rounded up to a multiple of 4
-inline size_t lvl_work_pad(int n) { return (size_t(n) + 3) / 4 * 4; }
 
 template <class T>
 size_t lvl_smem_bytes(int W, int stages, int nfar, int L, const LvlArgsLong& lg) {
